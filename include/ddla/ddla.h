@@ -1,0 +1,105 @@
+// ddla C++ API for the Cholesky path on B200.
+//
+// The five reference templates keep their exact signatures, argument meaning,
+// info and exception behaviour (reference include/ddla/ddla.h):
+//   ppotrf       1064-1070     ppotrs      1148-1155     pposv   1183-1190
+//   potrf        2159-2160     diag_logdet 2900-2902
+// Instantiated for float, double, std::complex<float>, std::complex<double>.
+// A handle's matrices are device memory; the process grid is 1x1, so the
+// descriptor supplies the leading dimension (LLD_) and is validated exactly as
+// the reference validates it (src/ddla_desc.cpp:9-59).
+//
+// Additions beside the reference path (no reference counterpart):
+//   pposv_mixed     FP64-accurate solve from a low-precision tensor-core factor
+//                   plus iterative refinement / GMRES-IR (LAPACK ?sposv shape);
+//   potrf_batched_solve_logdet / gp_nll_batched: see ddla_batched.h.
+#ifndef DDLA_H
+#define DDLA_H
+
+#include <complex>
+
+#include <ddla/ddla_desc.h>
+#include <ddla/ddla_handle_t.h>
+
+namespace ddla {
+
+template <typename T> struct real_type { using type = T; };
+template <typename U> struct real_type<std::complex<U>> { using type = U; };
+template <typename T> using real_type_t = typename real_type<T>::type;
+
+// A = L*L^H (uplo 'L') or U^H*U ('U') of the leading n x n, in place.  info is
+// 0 or the order of the first leading minor that is not positive definite.
+// Returns with the handle's stream synchronised.
+template <typename T>
+void ppotrf(const DdlaHandle_t& handle, char uplo, int n, T* A, int ia, int ja, const int* descA, int& info);
+
+// A*X = B (side 'L', B n x nrhs) or X*A = B (side 'R', B nrhs x n) with the
+// factor from ppotrf; trans 'N' and 'C' are equivalent, 'T' is rejected.
+template <typename T>
+void ppotrs(const DdlaHandle_t& handle, char side, char uplo, char trans, int n, int nrhs, const T* A,
+            const int* descA, T* B, const int* descB);
+
+// ppotrf then, if info == 0, ppotrs.  B is untouched when info != 0.
+template <typename T>
+void pposv(const DdlaHandle_t& handle, char side, char uplo, char trans, int n, int nrhs, T* A, int ia, int ja,
+           const int* descA, T* B, int ib, int jb, const int* descB, int& info);
+
+// LAPACK-style factorization with a DEVICE info pointer; asynchronous.
+template <typename T>
+void potrf(const DdlaHandle_t& handle, char uplo, int n, T* A, int lda, int* info);
+
+// Principal log of prod(A(i,i)), i < n, as (log magnitude, phase in (-pi, pi]).
+// Zero diagonal -> (-inf, 0); nonfinite diagonal throws std::domain_error and
+// leaves result unchanged.  Completes before returning.
+template <typename T>
+void diag_logdet(const DdlaHandle_t& handle, int n, const T* A, int lda, std::complex<real_type_t<T>>& result);
+
+// Workspace split of the reference's check / size / run components
+// (src/Cholesky/cholesky_workspace.h:133-154, 207-222, 239-249; plan_util.h).
+// The *_workspace_size functions report device bytes; *_run performs the
+// routine on caller scratch (no validation, no allocation).
+namespace cholesky_impl {
+template <typename T>
+void ppotrf_workspace_size(const DdlaHandle_t& handle, char uplo, int n, const T* A, const int* descA,
+                           std::size_t* backend_bytes, std::size_t* host_bytes);
+template <typename T>
+void ppotrf_run(const DdlaHandle_t& handle, char uplo, int n, T* A, int ia, int ja, const int* descA, int& info,
+                void* backend_work, std::size_t backend_bytes, void* host_work, std::size_t host_bytes);
+template <typename T>
+void ppotrs_workspace_size(const DdlaHandle_t& handle, char side, int n, int nrhs, const int* descA,
+                           const int* descB, std::size_t* backend_bytes, std::size_t* host_bytes);
+template <typename T>
+void ppotrs_run(const DdlaHandle_t& handle, char side, char uplo, char trans, int n, int nrhs, const T* A,
+                const int* descA, T* B, const int* descB, void* backend_work, std::size_t backend_bytes,
+                void* host_work, std::size_t host_bytes);
+}  // namespace cholesky_impl
+
+// ---------------------------------------------------------------------------
+// Mixed precision (new): solve A*X = B for a Hermitian positive-definite FP64
+// A to FP64 accuracy.  A low-precision Cholesky factor of A is computed with
+// the trailing updates on the tensor cores (precision 'B': BF16 operands,
+// 'T': TF32 operands; FP32 accumulation and FP32 storage, FP64 diagonal
+// blocks), then X is refined in FP64 (residuals against the untouched FP64 A)
+// with classical iterative refinement, switching to GMRES-IR preconditioned by
+// the low-precision factor when refinement stagnates.  precision 'D' factors
+// in FP64 directly.  uplo 'L' only.
+//   On success A is unchanged, X holds the solution and iter > 0 is the number
+//   of refinement sweeps (GMRES iterations count one each).  If neither scheme
+//   reaches the LAPACK ?sposv stopping test (||r|| <= ||x|| ||A|| eps sqrt(n))
+//   within the iteration budget, the routine falls back to ppotrf/ppotrs in
+//   FP64 (A then holds the FP64 factor) and sets iter = -(sweeps + 1).
+//   info is ppotrf's info of whichever factorization produced X.
+// ---------------------------------------------------------------------------
+struct MixedReport {
+    int iter = 0;            // refinement sweeps (> 0), or -(sweeps+1) after FP64 fallback
+    int gmres = 0;           // 1 if GMRES-IR was used
+    double shift = 0;        // diagonal shift applied to the low-precision factor (relative)
+    double backward_error = 0;  // final max_j ||b_j - A x_j||_inf / (||A||_inf ||x_j||_inf)
+};
+void pposv_mixed(const DdlaHandle_t& handle, char uplo, char precision, int n, int nrhs, double* A,
+                 const int* descA, const double* B, const int* descB, double* X, const int* descX, int& info,
+                 MixedReport* report = nullptr);
+
+}  // namespace ddla
+
+#endif

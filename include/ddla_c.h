@@ -1,0 +1,155 @@
+/*
+ * ddla_c.h -- C ABI of the B200 Cholesky-path library (libddla_c.so).
+ *
+ * This is the drop-in boundary: the same exported names, argument order and
+ * status convention as the reference's generated C ABI
+ * (fortran/ddla_c_api.cpp), which python/ddla/_c_api.py binds with ctypes.
+ * Each declaration cites the reference export it replaces.
+ *
+ * Conventions (ddla_c_api.cpp:1-27, 44-52): every call returns an int status
+ * 0 success, 1 invalid handle, 2 invalid value, 3 alloc failed,
+ * 4 backend unavailable, 5 internal (device) error, 6 a C++ exception escaped
+ * (its text via ddla_c_error_string(6), kept per thread).  The handle travels
+ * as void*; matrices are device pointers of a GPU handle; descriptors are the
+ * ScaLAPACK int[9] arrays; info is a host int* except for ddla_?_potrf, whose
+ * info is a device int* (asynchronous, like the reference's GPU potrf).
+ * Only the 1x1 process grid is served and only the GPU backend exists.
+ */
+#ifndef DDLA_C_H
+#define DDLA_C_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- lifecycle, grid and memory -------------------------------------- */
+const char* ddla_c_error_string(int status);                                  /* ddla_c_api.cpp:91 */
+int ddla_c_init_backend(void** handle, int backend);                          /* ddla_c_api.cpp:100 */
+int ddla_c_set(void* handle, int f_comm, int nprows, int npcols, char major); /* ddla_c_api.cpp:115 */
+int ddla_c_set_communication(void* handle, int communication);                /* ddla_c_api.cpp:134 */
+int ddla_c_get_communication(void* handle, int* communication);               /* ddla_c_api.cpp:144 */
+int ddla_c_communication_available(void* handle, int communication);          /* ddla_c_api.cpp:156 */
+int ddla_c_destroy(void** handle);                                            /* ddla_c_api.cpp:165 */
+int ddla_c_backend_available(int backend);                                    /* ddla_c_api.cpp:178 */
+int ddla_c_get_backend(void* handle);                                         /* ddla_c_api.cpp:184 */
+int ddla_c_grid_dims(void* handle, int* nprows, int* npcols);                 /* ddla_c_api.cpp:190 */
+int ddla_c_grid_coords(void* handle, int* myprow, int* mypcol);               /* ddla_c_api.cpp:197 */
+int ddla_c_rank(void* handle);                                                /* ddla_c_api.cpp:204 */
+int ddla_c_size(void* handle);                                                /* ddla_c_api.cpp:210 */
+int ddla_c_descinit(int* desc, void* handle, int m, int n, int mb, int nb, int irsrc, int icsrc,
+                    int lld);                                                 /* ddla_c_api.cpp:216 */
+int ddla_c_numloc(int n, int nb, int iproc, int srcproc, int nprocs);         /* ddla_c_api.cpp:224 */
+int ddla_c_malloc(void* handle, void** ptr, long long bytes);                 /* ddla_c_api.cpp:229 */
+int ddla_c_free(void* handle, void* ptr);                                     /* ddla_c_api.cpp:236 */
+int ddla_c_memcpy(void* handle, void* dst, const void* src, long long bytes); /* ddla_c_api.cpp:242 */
+int ddla_c_memcpy2d(void* handle, void* dst, long long dpitch, const void* src, long long spitch, long long width,
+                    long long height);                                        /* ddla_c_api.cpp:249 */
+int ddla_c_memset(void* handle, void* ptr, int value, long long bytes);       /* ddla_c_api.cpp:260 */
+int ddla_c_synchronize(void* handle);                                         /* ddla_c_api.cpp:267 */
+int ddla_c_default_comm(void);                                                /* ddla_c_api.cpp:304 */
+int ddla_c_comm_rank(int f_comm);                                             /* ddla_c_api.cpp:310 */
+int ddla_c_comm_size(int f_comm);                                             /* ddla_c_api.cpp:319 */
+void ddla_c_finalize(void);                                                   /* ddla_c_api.cpp:328 */
+int ddla_c_bcast_dims(int f_comm, int* m, int* n, int* type_char, int root);  /* ddla_c_api.cpp:339 */
+
+/* ---- 1x1-grid gather / scatter (host global <-> device local) ---------- */
+int ddla_s_gather(void* h, int m, int n, const void* A, int ia, int ja, const int* descA, int root, void* dst,
+                  int lddst); /* ddla_c_api.cpp:515 (ddla_c_gather and its s/d/z siblings) */
+int ddla_d_gather(void* h, int m, int n, const void* A, int ia, int ja, const int* descA, int root, void* dst,
+                  int lddst);
+int ddla_c_gather(void* h, int m, int n, const void* A, int ia, int ja, const int* descA, int root, void* dst,
+                  int lddst);
+int ddla_z_gather(void* h, int m, int n, const void* A, int ia, int ja, const int* descA, int root, void* dst,
+                  int lddst);
+int ddla_s_scatter(void* h, int m, int n, void* A, int ia, int ja, const int* descA, int root, const void* src,
+                   int ldsrc); /* ddla_c_api.cpp:551 (ddla_c_scatter and its s/d/z siblings) */
+int ddla_d_scatter(void* h, int m, int n, void* A, int ia, int ja, const int* descA, int root, const void* src,
+                   int ldsrc);
+int ddla_c_scatter(void* h, int m, int n, void* A, int ia, int ja, const int* descA, int root, const void* src,
+                   int ldsrc);
+int ddla_z_scatter(void* h, int m, int n, void* A, int ia, int ja, const int* descA, int root, const void* src,
+                   int ldsrc);
+
+/* ---- the Cholesky path ------------------------------------------------- */
+/* ddla_c_api.cpp:1155-1189 */
+int ddla_s_ppotrf(void* handle, char uplo, int n, void* A, int ia, int ja, const int* descA, int* info);
+int ddla_d_ppotrf(void* handle, char uplo, int n, void* A, int ia, int ja, const int* descA, int* info);
+int ddla_c_ppotrf(void* handle, char uplo, int n, void* A, int ia, int ja, const int* descA, int* info);
+int ddla_z_ppotrf(void* handle, char uplo, int n, void* A, int ia, int ja, const int* descA, int* info);
+/* ddla_c_api.cpp:1263-1297 */
+int ddla_s_ppotrs(void* handle, char side, char uplo, char trans, int n, int nrhs, const void* A, const int* descA,
+                  void* B, const int* descB);
+int ddla_d_ppotrs(void* handle, char side, char uplo, char trans, int n, int nrhs, const void* A, const int* descA,
+                  void* B, const int* descB);
+int ddla_c_ppotrs(void* handle, char side, char uplo, char trans, int n, int nrhs, const void* A, const int* descA,
+                  void* B, const int* descB);
+int ddla_z_ppotrs(void* handle, char side, char uplo, char trans, int n, int nrhs, const void* A, const int* descA,
+                  void* B, const int* descB);
+/* ddla_c_api.cpp:1299-1333 */
+int ddla_s_pposv(void* handle, char side, char uplo, char trans, int n, int nrhs, void* A, int ia, int ja,
+                 const int* descA, void* B, int ib, int jb, const int* descB, int* info);
+int ddla_d_pposv(void* handle, char side, char uplo, char trans, int n, int nrhs, void* A, int ia, int ja,
+                 const int* descA, void* B, int ib, int jb, const int* descB, int* info);
+int ddla_c_pposv(void* handle, char side, char uplo, char trans, int n, int nrhs, void* A, int ia, int ja,
+                 const int* descA, void* B, int ib, int jb, const int* descB, int* info);
+int ddla_z_pposv(void* handle, char side, char uplo, char trans, int n, int nrhs, void* A, int ia, int ja,
+                 const int* descA, void* B, int ib, int jb, const int* descB, int* info);
+/* ddla_c_api.cpp:2150-2180 (info is a DEVICE int*) */
+int ddla_s_potrf(void* handle, char uplo, int n, void* A, int lda, void* info);
+int ddla_d_potrf(void* handle, char uplo, int n, void* A, int lda, void* info);
+int ddla_c_potrf(void* handle, char uplo, int n, void* A, int lda, void* info);
+int ddla_z_potrf(void* handle, char uplo, int n, void* A, int lda, void* info);
+
+/* diag_logdet has no C export in the reference (its C++ template is
+ * include/ddla/ddla.h:2900-2902); these add one.  result receives two reals
+ * of the matrix's real type: log magnitude, phase in (-pi, pi]. */
+int ddla_s_diag_logdet(void* handle, int n, const void* A, int lda, void* result);
+int ddla_d_diag_logdet(void* handle, int n, const void* A, int lda, void* result);
+int ddla_c_diag_logdet(void* handle, int n, const void* A, int lda, void* result);
+int ddla_z_diag_logdet(void* handle, int n, const void* A, int lda, void* result);
+
+/* The reference's internal check / size / run split of ppotrf and ppotrs
+ * (src/Cholesky/cholesky_workspace.h:133-154, 207-222) exported so a caller can
+ * own the device scratch: *_workspace_size reports bytes, *_run computes on
+ * the caller's scratch without allocating. */
+int ddla_s_ppotrf_workspace_size(void* handle, char uplo, int n, const int* descA, long long* bytes);
+int ddla_d_ppotrf_workspace_size(void* handle, char uplo, int n, const int* descA, long long* bytes);
+int ddla_c_ppotrf_workspace_size(void* handle, char uplo, int n, const int* descA, long long* bytes);
+int ddla_z_ppotrf_workspace_size(void* handle, char uplo, int n, const int* descA, long long* bytes);
+int ddla_s_ppotrf_run(void* handle, char uplo, int n, void* A, const int* descA, int* info, void* work, long long bytes);
+int ddla_d_ppotrf_run(void* handle, char uplo, int n, void* A, const int* descA, int* info, void* work, long long bytes);
+int ddla_c_ppotrf_run(void* handle, char uplo, int n, void* A, const int* descA, int* info, void* work, long long bytes);
+int ddla_z_ppotrf_run(void* handle, char uplo, int n, void* A, const int* descA, int* info, void* work, long long bytes);
+int ddla_s_ppotrs_workspace_size(void* handle, char side, int n, int nrhs, const int* descA, const int* descB,
+                                 long long* bytes);
+int ddla_d_ppotrs_workspace_size(void* handle, char side, int n, int nrhs, const int* descA, const int* descB,
+                                 long long* bytes);
+int ddla_c_ppotrs_workspace_size(void* handle, char side, int n, int nrhs, const int* descA, const int* descB,
+                                 long long* bytes);
+int ddla_z_ppotrs_workspace_size(void* handle, char side, int n, int nrhs, const int* descA, const int* descB,
+                                 long long* bytes);
+
+/* Mixed-precision solve (no reference counterpart; LAPACK dsposv semantics,
+ * see ddla::pposv_mixed in include/ddla/ddla.h).  precision: 'B' BF16 or 'T'
+ * TF32 tensor-core factor, 'D' plain FP64.  report (may be NULL) receives
+ * {double iter, double gmres, double shift, double backward_error}. */
+int ddla_d_pposv_mixed(void* handle, char uplo, char precision, int n, int nrhs, void* A, const int* descA,
+                       const void* B, const int* descB, void* X, const int* descX, int* info, double* report);
+
+/* Diagnostics (no reference counterpart: the reference has no tracing).
+ * ddla_c_get_stream returns the handle's CUDA stream (ddlaGetStream of
+ * include/ddla/ddla_handle_t.h:337, which the reference's C ABI does not
+ * export).  ddla_c_launch_count is the number of kernels this library has
+ * launched in the process.  ddla_c_profile_enable / ddla_c_profile_read switch
+ * per-kernel CUDA-event timing on and read it back per kernel kind (see
+ * ddlak_profile_read in ddla_kernels.h). */
+int ddla_c_get_stream(void* handle, void** stream);
+long long ddla_c_launch_count(void);
+void ddla_c_profile_enable(int on);
+int ddla_c_profile_read(int kind, double* ms, long long* launches, double* flops, double* bytes, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

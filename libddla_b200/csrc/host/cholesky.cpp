@@ -1,0 +1,260 @@
+// ddla::ppotrf / ppotrs / pposv / potrf / diag_logdet on a GPU handle (1x1 grid).
+//
+// Argument checks, exception types and messages follow the reference's
+// check components (src/Cholesky/ppotrf.cpp:21-29, ppotrs.cpp:14-30,
+// pposv.cpp:15-21, potrf.cpp:122-135, src/diag_logdet.cpp:42-55); the run
+// components replace the vendor calls with the kernels of include/ddla_kernels.h.
+// ppotrf/ppotrs/pposv return with the handle's stream synchronised and info
+// on the host (ppotrf.cpp:49-52, ppotrs.cpp:84, pposv.cpp:62); potrf is
+// asynchronous with a device info (ddla.h:2150-2160).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <stdexcept>
+#include <string>
+
+#include <ddla/ddla.h>
+#include <ddla_kernels.h>
+
+#include "ddla_stream.h"
+
+namespace ddla {
+
+namespace {
+
+template <class T> constexpr char tcode();
+template <> constexpr char tcode<float>() { return 's'; }
+template <> constexpr char tcode<double>() { return 'd'; }
+template <> constexpr char tcode<std::complex<float>>() { return 'c'; }
+template <> constexpr char tcode<std::complex<double>>() { return 'z'; }
+
+void ppotrf_check(const DdlaHandle_t& h, char uplo, int n, const void* A, int ia, int ja, const int* d)
+{
+    detail::check_desc(d, h);
+    detail::require_gpu(h, "ppotrf");
+    if ((uplo != 'L' && uplo != 'U') || n < 0 || n > d[DDLA_M_] || n > d[DDLA_N_] || d[DDLA_MB_] != d[DDLA_NB_] ||
+        ia != 1 || ja != 1)
+        throw std::invalid_argument("ppotrf: invalid triangle, dimensions, blocks or offsets");
+    if (n && !A) throw std::invalid_argument("ppotrf: null local matrix");
+}
+
+void ppotrs_check(const DdlaHandle_t& h, char side, char uplo, char trans, int n, int nrhs, const void* A,
+                  const int* da, const void* B, const int* db)
+{
+    detail::check_desc(da, h);
+    detail::check_desc(db, h);
+    detail::require_gpu(h, "ppotrs");
+    if ((side != 'L' && side != 'R') || (uplo != 'L' && uplo != 'U') || (trans != 'N' && trans != 'C') || n < 0 ||
+        nrhs < 0 || n > da[DDLA_M_] || n > da[DDLA_N_] || da[DDLA_MB_] != da[DDLA_NB_])
+        throw std::invalid_argument("ppotrs: invalid flags, dimensions or factor blocks");
+    if (db[DDLA_MB_] != da[DDLA_MB_] || (side == 'L' && db[DDLA_RSRC_] != da[DDLA_RSRC_]) ||
+        (side == 'R' && (db[DDLA_NB_] != da[DDLA_NB_] || db[DDLA_CSRC_] != da[DDLA_CSRC_])))
+        throw std::invalid_argument("ppotrs: B must be distributed like A along the solved dimension");
+    const int rows = side == 'L' ? n : nrhs, cols = side == 'L' ? nrhs : n;
+    if (rows > db[DDLA_M_] || cols > db[DDLA_N_]) throw std::invalid_argument("ppotrs: invalid right-hand side");
+    if (n && !A) throw std::invalid_argument("ppotrs: null local factor");
+    if (rows && cols && !B) throw std::invalid_argument("ppotrs: null local right-hand side");
+}
+
+void pposv_check(const DdlaHandle_t& h, char side, char uplo, char trans, int n, int nrhs, const void* A, int ia,
+                 int ja, const int* da, const void* B, int ib, int jb, const int* db)
+{
+    ppotrf_check(h, uplo, n, A, ia, ja, da);
+    ppotrs_check(h, side, uplo, trans, n, nrhs, A, da, B, db);
+    if (ib != 1 || jb != 1) throw std::invalid_argument("pposv: offsets must be one");
+}
+
+int read_device_int(const DdlaHandle_t& h, const int* dptr)
+{
+    detail::cuda_check(cudaMemcpyAsync(h->host_word, dptr, sizeof(int), cudaMemcpyDeviceToHost, h->stream),
+                       "info read-back");
+    detail::cuda_check(cudaStreamSynchronize(h->stream), "stream synchronisation");
+    return *h->host_word;
+}
+
+}  // namespace
+
+namespace cholesky_impl {
+
+template <typename T>
+void ppotrf_workspace_size(const DdlaHandle_t&, char, int n, const T*, const int*, std::size_t* backend_bytes,
+                           std::size_t* host_bytes)
+{
+    *backend_bytes = n > 0 ? detail::padded_bytes<int>(1) : 0;  // the device info word
+    *host_bytes = 0;
+}
+
+template <typename T>
+void ppotrf_run(const DdlaHandle_t& h, char uplo, int n, T* A, int, int, const int* descA, int& info,
+                void* backend_work, std::size_t backend_bytes, void*, std::size_t)
+{
+    if (n == 0) {
+        info = 0;
+        return;
+    }
+    if (backend_bytes < detail::padded_bytes<int>(1) || backend_work == nullptr)
+        throw std::invalid_argument("ppotrf: workspace smaller than ppotrf_workspace_size");
+    char* w = static_cast<char*>(backend_work);
+    int* dinfo = detail::take<int>(w, 1);
+    detail::kernel_check(ddlak_potrf(tcode<T>(), uplo, n, A, descA[DDLA_LLD_], dinfo, h->stream), "potrf kernels");
+    info = read_device_int(h, dinfo);
+}
+
+template <typename T>
+void ppotrs_workspace_size(const DdlaHandle_t&, char side, int n, int nrhs, const int*, const int*,
+                           std::size_t* backend_bytes, std::size_t* host_bytes)
+{
+    (void)side;
+    *host_bytes = 0;
+    *backend_bytes = (n > 0 && nrhs > 0) ? static_cast<std::size_t>(ddlak_potrs_workspace(n, nrhs)) : 0;
+}
+
+template <typename T>
+void ppotrs_run(const DdlaHandle_t& h, char side, char uplo, char, int n, int nrhs, const T* A, const int* descA,
+                T* B, const int* descB, void* backend_work, std::size_t backend_bytes, void*, std::size_t)
+{
+    if (n == 0 || nrhs == 0) return;
+    const unsigned long long need = ddlak_potrs_workspace(n, nrhs);
+    if (backend_bytes < need || backend_work == nullptr)
+        throw std::invalid_argument("ppotrs: workspace smaller than ppotrs_workspace_size");
+    detail::kernel_check(ddlak_potrs(tcode<T>(), uplo, side, n, nrhs, A, descA[DDLA_LLD_], B, descB[DDLA_LLD_],
+                                     backend_work, need, h->stream),
+                         "potrs kernel");
+    const int status = read_device_int(h, static_cast<const int*>(backend_work));
+    if (status != 0) throw std::runtime_error("ppotrs: a device wait in the fused solve timed out");
+}
+
+}  // namespace cholesky_impl
+
+template <typename T>
+void ppotrf(const DdlaHandle_t& handle, char uplo, int n, T* A, int ia, int ja, const int* descA, int& info)
+{
+    ppotrf_check(handle, uplo, n, A, ia, ja, descA);
+    info = 0;
+    if (n == 0) return;
+    std::size_t bb = 0, hb = 0;
+    cholesky_impl::ppotrf_workspace_size<T>(handle, uplo, n, A, descA, &bb, &hb);
+    detail::DeviceScratch work(handle, bb);
+    cholesky_impl::ppotrf_run<T>(handle, uplo, n, A, ia, ja, descA, info, work.data(), bb, nullptr, 0);
+}
+
+template <typename T>
+void ppotrs(const DdlaHandle_t& h, char side, char uplo, char trans, int n, int nrhs, const T* A, const int* da, T* B,
+            const int* db)
+{
+    ppotrs_check(h, side, uplo, trans, n, nrhs, A, da, B, db);
+    if (n == 0 || nrhs == 0) return;
+    std::size_t bb = 0, hb = 0;
+    cholesky_impl::ppotrs_workspace_size<T>(h, side, n, nrhs, da, db, &bb, &hb);
+    detail::DeviceScratch work(h, bb);
+    cholesky_impl::ppotrs_run<T>(h, side, uplo, trans, n, nrhs, A, da, B, db, work.data(), bb, nullptr, 0);
+    detail::cuda_check(cudaStreamSynchronize(h->stream), "stream synchronisation");
+}
+
+template <typename T>
+void pposv(const DdlaHandle_t& h, char side, char uplo, char trans, int n, int nrhs, T* A, int ia, int ja,
+           const int* da, T* B, int ib, int jb, const int* db, int& info)
+{
+    pposv_check(h, side, uplo, trans, n, nrhs, A, ia, ja, da, B, ib, jb, db);
+    if (n == 0) {
+        info = 0;
+        return;
+    }
+    std::size_t fb = 0, fh = 0, sb = 0, sh = 0;
+    cholesky_impl::ppotrf_workspace_size<T>(h, uplo, n, A, da, &fb, &fh);
+    cholesky_impl::ppotrs_workspace_size<T>(h, side, n, nrhs, da, db, &sb, &sh);
+    const std::size_t bb = std::max(fb, sb);
+    detail::DeviceScratch work(h, bb);
+    cholesky_impl::ppotrf_run<T>(h, uplo, n, A, ia, ja, da, info, work.data(), bb, nullptr, 0);
+    if (info == 0) cholesky_impl::ppotrs_run<T>(h, side, uplo, trans, n, nrhs, A, da, B, db, work.data(), bb, nullptr, 0);
+    detail::cuda_check(cudaStreamSynchronize(h->stream), "stream synchronisation");
+}
+
+template <typename T>
+void potrf(const DdlaHandle_t& h, char uplo, int n, T* A, int lda, int* info)
+{
+    detail::require_gpu(h, "potrf");
+    char u;
+    if (uplo == 'U' || uplo == 'u') u = 'U';
+    else if (uplo == 'L' || uplo == 'l') u = 'L';
+    else throw std::runtime_error("ddla: invalid uplo flag (expected 'U' or 'L')");
+    if (n < 0) throw std::runtime_error("potrf: negative matrix size");
+    if (info == nullptr) throw std::runtime_error("potrf: null info");
+    if (n > 0) {
+        if (A == nullptr) throw std::runtime_error("potrf: null A");
+        if (lda < std::max(1, n)) throw std::runtime_error("potrf: lda too small");
+    }
+    detail::kernel_check(ddlak_potrf(tcode<T>(), u, n, A, lda, info, h->stream), "potrf kernels");
+}
+
+template <typename T>
+void diag_logdet(const DdlaHandle_t& h, int n, const T* a, int lda, std::complex<real_type_t<T>>& result)
+{
+    using R = real_type_t<T>;
+    detail::require_gpu(h, "diag_logdet");
+    if (n < 0 || lda < std::max(1, n) || (n > 0 && !a))
+        throw std::invalid_argument("diag_logdet: invalid order, leading dimension or pointer");
+    if (n > 0) {
+        // the reference's check_diag_span (src/diag_logdet_impl.h:33-40)
+        const auto last = std::uint64_t(n - 1) * std::uint64_t(lda) + std::uint64_t(n) - 1;
+        if (last > std::uint64_t(std::numeric_limits<std::ptrdiff_t>::max()) / sizeof(T))
+            throw std::overflow_error("diag_logdet: matrix address span is not representable");
+    }
+    double magnitude = 0, phase = 0;
+    int flags = 0;
+    if (n > 0) {
+        detail::DeviceScratch work(h, static_cast<std::size_t>(ddlak_logdet_workspace()));
+        detail::kernel_check(ddlak_diag_logsum(tcode<T>(), n, a, lda, work.data(), h->stream), "diag_logdet kernels");
+        struct {
+            double mag, phase;
+            int flags, pad;
+        } st{};
+        static_assert(sizeof(st) == 24, "state layout");
+        detail::cuda_check(cudaMemcpyAsync(h->host_word, work.data(), sizeof(st), cudaMemcpyDeviceToHost, h->stream),
+                           "logdet read-back");
+        detail::cuda_check(cudaStreamSynchronize(h->stream), "stream synchronisation");
+        std::memcpy(&st, h->host_word, sizeof(st));
+        magnitude = st.mag;
+        phase = st.phase;
+        flags = st.flags;
+    }
+    if (flags & 1) throw std::domain_error("diag_logdet: nonfinite diagonal");
+    // finish_diagonal_log (src/diag_logdet_impl.h:104-113)
+    if (flags & 2) {
+        result = {-std::numeric_limits<R>::infinity(), R(0)};
+        return;
+    }
+    const double pi = std::acos(-1.0);
+    phase = std::remainder(phase + ((flags >> 2) & 1) * pi, 2 * pi);
+    if (phase <= -pi) phase = pi;
+    result = {static_cast<R>(magnitude), static_cast<R>(phase)};
+}
+
+#define DDLA_INSTANTIATE(T)                                                                                          \
+    template void ppotrf<T>(const DdlaHandle_t&, char, int, T*, int, int, const int*, int&);                         \
+    template void ppotrs<T>(const DdlaHandle_t&, char, char, char, int, int, const T*, const int*, T*, const int*); \
+    template void pposv<T>(const DdlaHandle_t&, char, char, char, int, int, T*, int, int, const int*, T*, int, int, \
+                           const int*, int&);                                                                        \
+    template void potrf<T>(const DdlaHandle_t&, char, int, T*, int, int*);                                          \
+    template void diag_logdet<T>(const DdlaHandle_t&, int, const T*, int, std::complex<real_type_t<T>>&);           \
+    template void cholesky_impl::ppotrf_workspace_size<T>(const DdlaHandle_t&, char, int, const T*, const int*,      \
+                                                          std::size_t*, std::size_t*);                               \
+    template void cholesky_impl::ppotrf_run<T>(const DdlaHandle_t&, char, int, T*, int, int, const int*, int&,       \
+                                               void*, std::size_t, void*, std::size_t);                              \
+    template void cholesky_impl::ppotrs_workspace_size<T>(const DdlaHandle_t&, char, int, int, const int*,           \
+                                                          const int*, std::size_t*, std::size_t*);                   \
+    template void cholesky_impl::ppotrs_run<T>(const DdlaHandle_t&, char, char, char, int, int, const T*,           \
+                                               const int*, T*, const int*, void*, std::size_t, void*, std::size_t);
+
+DDLA_INSTANTIATE(float)
+DDLA_INSTANTIATE(double)
+DDLA_INSTANTIATE(std::complex<float>)
+DDLA_INSTANTIATE(std::complex<double>)
+#undef DDLA_INSTANTIATE
+
+}  // namespace ddla

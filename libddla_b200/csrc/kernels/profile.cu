@@ -1,0 +1,104 @@
+// Launch accounting and per-kernel CUDA-event timing for the kernel layer.
+//
+// Every launcher bumps a process-wide launch counter.  When profiling is
+// switched on, launchers also bracket their kernels with CUDA events on the
+// launching stream and record the algorithmic flops and bytes of that launch;
+// ddlak_profile_read folds the records of one kernel kind into total device
+// time, launch count, flops and bytes.  The reference has no tracing of its
+// own; this is what bench.py uses for the live roofline numbers.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <mutex>
+#include <vector>
+
+#include "profile.h"
+
+namespace ddlak {
+
+namespace {
+std::atomic<long long> g_launches{0};
+std::atomic<bool> g_on{false};
+std::mutex g_mu;
+struct Rec {
+    int kind;
+    cudaEvent_t a, b;
+    double flops, bytes;
+};
+std::vector<Rec> g_recs;
+std::vector<cudaEvent_t> g_free;
+
+cudaEvent_t get_event()
+{
+    if (!g_free.empty()) {
+        cudaEvent_t e = g_free.back();
+        g_free.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+}  // namespace
+
+void note_launches(int count) { g_launches.fetch_add(count, std::memory_order_relaxed); }
+
+bool profiling() { return g_on.load(std::memory_order_relaxed); }
+
+ProfScope::ProfScope(int kind, cudaStream_t st, double flops, double bytes) : st_(st), active_(profiling())
+{
+    if (!active_) return;
+    std::lock_guard<std::mutex> lk(g_mu);
+    Rec r{kind, get_event(), get_event(), flops, bytes};
+    cudaEventRecord(r.a, st);
+    idx_ = g_recs.size();
+    g_recs.push_back(r);
+}
+
+ProfScope::~ProfScope()
+{
+    if (!active_) return;
+    std::lock_guard<std::mutex> lk(g_mu);
+    cudaEventRecord(g_recs[idx_].b, st_);
+}
+
+}  // namespace ddlak
+
+extern "C" long long ddlak_launch_count(void) { return ddlak::g_launches.load(); }
+
+extern "C" void ddlak_profile_enable(int on) { ddlak::g_on.store(on != 0); }
+
+extern "C" int ddlak_profile_read(int kind, double* ms, long long* launches, double* flops, double* bytes, int reset)
+{
+    using namespace ddlak;
+    std::lock_guard<std::mutex> lk(g_mu);
+    double t = 0, f = 0, b = 0;
+    long long c = 0;
+    std::vector<Rec> keep;
+    for (auto& r : g_recs) {
+        if (kind >= 0 && r.kind != kind) {
+            keep.push_back(r);
+            continue;
+        }
+        const cudaError_t e = cudaEventSynchronize(r.b);
+        if (e != cudaSuccess) return (int)e;
+        float x = 0;
+        cudaEventElapsedTime(&x, r.a, r.b);
+        t += x;
+        f += r.flops;
+        b += r.bytes;
+        ++c;
+        if (reset) {
+            g_free.push_back(r.a);
+            g_free.push_back(r.b);
+        } else {
+            keep.push_back(r);
+        }
+    }
+    g_recs.swap(keep);
+    if (ms) *ms = t;
+    if (launches) *launches = c;
+    if (flops) *flops = f;
+    if (bytes) *bytes = b;
+    return 0;
+}

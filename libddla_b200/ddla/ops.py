@@ -1,0 +1,89 @@
+"""Cholesky-path routines -- mirror of ppotrf / ppotrs / pposv in the reference's
+python/ddla/ops.py:113-143, plus potrf, diag_logdet and pposv_mixed."""
+from __future__ import annotations
+
+import ctypes
+from typing import Tuple, Union
+
+import numpy as np
+
+from . import _c_api as C
+from .matrix import DistributedMatrix
+
+
+def _ch(c: Union[str, bytes]) -> bytes:
+    if isinstance(c, bytes):
+        return c.upper()
+    return c.upper().encode("ascii")
+
+
+def ppotrf(A: DistributedMatrix, uplo: str = "L") -> Tuple[DistributedMatrix, int]:
+    """Cholesky factorization in place; returns (A, info)."""
+    info = ctypes.c_int(0)
+    f = getattr(C.lib, f"ddla_{A.type_char}_ppotrf")
+    C.check_status(f(A.handle.ptr, _ch(uplo), A.n, A.data_ptr, 1, 1, A.desc.ctypes.data, ctypes.byref(info)),
+                   f"ddla_{A.type_char}_ppotrf")
+    return A, info.value
+
+
+def ppotrs(A: DistributedMatrix, B: DistributedMatrix, uplo: str = "L", side: str = "L",
+           trans: str = "N") -> DistributedMatrix:
+    """Solve A X = B (side 'L') or X A = B (side 'R') with the factor from ppotrf; X overwrites B."""
+    s = _ch(side)
+    nrhs = B.n if s == b"L" else B.m
+    f = getattr(C.lib, f"ddla_{A.type_char}_ppotrs")
+    C.check_status(f(A.handle.ptr, s, _ch(uplo), _ch(trans), A.n, nrhs, A.data_ptr, A.desc.ctypes.data,
+                     B.data_ptr, B.desc.ctypes.data), f"ddla_{A.type_char}_ppotrs")
+    return B
+
+
+def pposv(A: DistributedMatrix, B: DistributedMatrix, uplo: str = "L", side: str = "L",
+          trans: str = "N") -> Tuple[DistributedMatrix, int]:
+    """Factor and solve in one native call (ddla::pposv); returns (B, info), B untouched when info != 0."""
+    s = _ch(side)
+    nrhs = B.n if s == b"L" else B.m
+    info = ctypes.c_int(0)
+    f = getattr(C.lib, f"ddla_{A.type_char}_pposv")
+    C.check_status(f(A.handle.ptr, s, _ch(uplo), _ch(trans), A.n, nrhs, A.data_ptr, 1, 1, A.desc.ctypes.data,
+                     B.data_ptr, 1, 1, B.desc.ctypes.data, ctypes.byref(info)), f"ddla_{A.type_char}_pposv")
+    return B, info.value
+
+
+def potrf(handle, type_char: str, uplo: str, n: int, A_ptr: int, lda: int, dinfo_ptr: int) -> None:
+    """LAPACK-style potrf with a DEVICE info pointer (asynchronous on the handle's stream)."""
+    f = getattr(C.lib, f"ddla_{type_char}_potrf")
+    C.check_status(f(handle.ptr, _ch(uplo), int(n), A_ptr, int(lda), dinfo_ptr), f"ddla_{type_char}_potrf")
+
+
+def diag_logdet(A: DistributedMatrix, n: int = -1) -> complex:
+    """Principal log of the product of the diagonal of the leading n x n of A."""
+    n = A.n if n < 0 else n
+    out = np.zeros(2, dtype=np.float32 if A.type_char in "sc" else np.float64)
+    f = getattr(C.lib, f"ddla_{A.type_char}_diag_logdet")
+    C.check_status(f(A.handle.ptr, int(n), A.data_ptr, A.lld, out.ctypes.data), f"ddla_{A.type_char}_diag_logdet")
+    return complex(float(out[0]), float(out[1]))
+
+
+def pposv_mixed(A: DistributedMatrix, B: DistributedMatrix, X: DistributedMatrix, precision: str = "B",
+                uplo: str = "L"):
+    """FP64-accurate solve from a low-precision tensor-core factor plus refinement.
+
+    Returns (X, info, report) with report = {iter, gmres, shift, backward_error}; A is left
+    unchanged unless the routine fell back to the FP64 factorization (iter < 0)."""
+    if A.type_char != "d":
+        raise TypeError("pposv_mixed takes float64 matrices")
+    info = ctypes.c_int(0)
+    rep = (ctypes.c_double * 4)()
+    C.check_status(C.ddla_d_pposv_mixed(A.handle.ptr, _ch(uplo), _ch(precision), A.n, B.n, A.data_ptr,
+                                        A.desc.ctypes.data, B.data_ptr, B.desc.ctypes.data, X.data_ptr,
+                                        X.desc.ctypes.data, ctypes.byref(info), rep), "ddla_d_pposv_mixed")
+    report = {"iter": int(rep[0]), "gmres": int(rep[1]), "shift": float(rep[2]), "backward_error": float(rep[3])}
+    return X, info.value, report
+
+
+def gather(A: DistributedMatrix, root: int = 0):
+    return A.to_global_matrix(root)
+
+
+def scatter(handle, arr, mb: int = 64, nb: int = 64, root: int = 0):
+    return DistributedMatrix.from_global_matrix(handle, arr, mb=mb, nb=nb, root=root)

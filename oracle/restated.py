@@ -1,0 +1,86 @@
+"""ctypes wrapper of oracle/ddla_oracle.c (TEST INFRASTRUCTURE ONLY).
+
+Every function takes NumPy arrays and works on Fortran-ordered copies; the
+C code it calls restates the reference's CPU arm (see ddla_oracle.c for the
+reference file:line each routine follows).
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+_LIB = None
+
+_TC = {np.dtype(np.float32): "s", np.dtype(np.float64): "d", np.dtype(np.complex64): "c",
+       np.dtype(np.complex128): "z"}
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        from .build import build
+
+        path = build()
+        L = ctypes.CDLL(str(path))
+        vp, i, c = ctypes.c_void_p, ctypes.c_int, ctypes.c_char
+        for p in "sdcz":
+            getattr(L, f"oracle_{p}_potrf").argtypes = [c, i, vp, i]
+            getattr(L, f"oracle_{p}_potrf").restype = i
+            getattr(L, f"oracle_{p}_trsm").argtypes = [c, c, c, i, i, vp, i, vp, i]
+            getattr(L, f"oracle_{p}_trsm").restype = None
+            getattr(L, f"oracle_{p}_ppotrs").argtypes = [c, c, i, i, vp, i, vp, i]
+            getattr(L, f"oracle_{p}_ppotrs").restype = None
+            getattr(L, f"oracle_{p}_pposv").argtypes = [c, c, i, i, vp, i, vp, i]
+            getattr(L, f"oracle_{p}_pposv").restype = i
+            getattr(L, f"oracle_{p}_diag_logdet").argtypes = [i, vp, i, vp]
+            getattr(L, f"oracle_{p}_diag_logdet").restype = i
+        _LIB = L
+    return _LIB
+
+
+def _f(a: np.ndarray) -> np.ndarray:
+    return np.array(a, order="F", copy=True)
+
+
+def potrf(a: np.ndarray, uplo: str = "L", n: int | None = None):
+    """Return (factor array, info).  Only the uplo triangle of the leading n x n is touched."""
+    A = _f(a)
+    n = A.shape[1] if n is None else n
+    info = getattr(_lib(), f"oracle_{_TC[A.dtype]}_potrf")(uplo.encode(), n, A.ctypes.data, max(1, A.shape[0]))
+    return A, int(info)
+
+
+def ppotrs(factor: np.ndarray, b: np.ndarray, uplo: str = "L", side: str = "L", n: int | None = None):
+    A = np.asfortranarray(factor)
+    B = _f(b.astype(A.dtype))
+    n = A.shape[1] if n is None else n
+    nrhs = B.shape[1] if side == "L" else B.shape[0]
+    getattr(_lib(), f"oracle_{_TC[A.dtype]}_ppotrs")(side.encode(), uplo.encode(), n, nrhs, A.ctypes.data,
+                                                     max(1, A.shape[0]), B.ctypes.data, max(1, B.shape[0]))
+    return B
+
+
+def pposv(a: np.ndarray, b: np.ndarray, uplo: str = "L", side: str = "L"):
+    """Return (factor, X, info); X is b unchanged when info != 0 (pposv.cpp:36-38)."""
+    A = _f(a)
+    B = _f(b.astype(A.dtype))
+    n = A.shape[1]
+    nrhs = B.shape[1] if side == "L" else B.shape[0]
+    info = getattr(_lib(), f"oracle_{_TC[A.dtype]}_pposv")(side.encode(), uplo.encode(), n, nrhs, A.ctypes.data,
+                                                           max(1, A.shape[0]), B.ctypes.data, max(1, B.shape[0]))
+    return A, B, int(info)
+
+
+def diag_logdet(a: np.ndarray, n: int | None = None, lda: int | None = None):
+    """Return complex(log magnitude, phase), or raise ValueError for a nonfinite diagonal."""
+    A = np.asfortranarray(a)
+    n = A.shape[1] if n is None else n
+    lda = max(1, A.shape[0]) if lda is None else lda
+    out = np.zeros(2, dtype=np.float64)
+    st = getattr(_lib(), f"oracle_{_TC[A.dtype]}_diag_logdet")(n, A.ctypes.data, lda, out.ctypes.data)
+    if st != 0:
+        raise ValueError("diag_logdet: nonfinite diagonal")
+    return complex(out[0], out[1])
