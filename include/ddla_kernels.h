@@ -46,6 +46,45 @@ unsigned long long ddlak_logdet_workspace(void);
  * {double magnitude; double phase; int flags} at the start of work. */
 int ddlak_diag_logsum(char type, int n, const void* A, long long lda, void* work, void* stream);
 
+/* ---- mixed precision (ddla::pposv_mixed; no reference counterpart) ------ */
+
+/* Bytes of one K-contiguous panel operand copy for an order-n factorization. */
+unsigned long long ddlak_mixed_panel_bytes(int n);
+
+/* W = fl32(A) on the lower triangle (diagonal times diag_scale, a relative
+ * shift), colsum[j] = sum_i |A(i,j)| of the full symmetric A, *anrm = max_j
+ * colsum[j] (= ||A||_inf), all on the stream.  ldw must be a multiple of 4. */
+int ddlak_convert_lower(int n, const void* A, long long lda, void* W, long long ldw, double diag_scale, void* colsum,
+                        void* anrm, void* stream);
+
+/* Cholesky of the FP32 matrix W (lower) with tensor-core trailing updates:
+ * precision 'B' (BF16 operands) or 'T' (TF32 operands), FP32 accumulation,
+ * FP64 diagonal blocks.  P0/P1: two buffers of ddlak_mixed_panel_bytes(n).
+ * *dinfo as ddlak_potrf; *status nonzero if a tensor-core pipeline wait gave up. */
+int ddlak_potrf_mixed(char precision, int n, void* W, long long ldw, void* P0, void* P1, int* dinfo, int* status,
+                      void* stream);
+
+/* In-place solve L L^T X = B with an FP32 factor (lower, ldl) and FP64 B;
+ * scratch as ddlak_potrs_workspace(n, nrhs). */
+int ddlak_potrs_mixed(int n, int nrhs, const void* L32, long long ldl, void* B, long long ldb, void* work,
+                      unsigned long long work_bytes, void* stream);
+
+/* R = B - A X, A symmetric FP64 stored in its lower triangle; deterministic. */
+int ddlak_symm_residual(int n, int nrhs, const void* A, long long lda, const void* X, long long ldx, const void* B,
+                        long long ldb, void* R, long long ldr, void* stream);
+
+/* out[j] = max_i |M(i,j)|;  Y += alpha X  (FP64, column-major). */
+int ddlak_colmax(int n, int ncol, const void* M, long long ld, void* out, void* stream);
+int ddlak_axpy(int n, int ncol, double alpha, const void* X, long long ldx, void* Y, long long ldy, void* stream);
+
+/* GMRES helpers on n x ncol column blocks (ld = n), vectors vstride apart:
+ * out[i*ncol+c] = <V_i(:,c), w(:,c)>;  w(:,c) -= sum_i coef[i*ncol+c] V_i(:,c);
+ * y(:,c) = alpha x(:,c) / sqrt(nrm2[c]) (nrm2 NULL: alpha x). */
+int ddlak_multidot(const void* V, long long vstride, int nv, const void* w, int n, int ncol, void* out, void* stream);
+int ddlak_multi_axpy(const void* V, long long vstride, int nv, const void* coef, void* w, int n, int ncol,
+                     void* stream);
+int ddlak_scale_cols(const void* x, void* y, int n, int ncol, double alpha, const void* nrm2, void* stream);
+
 /* Number of kernel launches the layer has made in this process. */
 long long ddlak_launch_count(void);
 

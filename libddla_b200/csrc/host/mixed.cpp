@@ -1,19 +1,51 @@
 // ddla::pposv_mixed -- FP64-accurate Hermitian positive-definite solve from a
 // low-precision tensor-core Cholesky factor plus refinement (no reference
-// counterpart; the LAPACK ?sposv contract).
+// counterpart; the contract of LAPACK ?sposv).
+//
+//   1. W = fl32(A) (lower), ||A||_inf from the full symmetric A;
+//   2. W = L L^T with the trailing updates on the tensor cores (BF16 or TF32
+//      operands, FP32 accumulation and storage, FP64 diagonal blocks); when the
+//      low-precision factorization breaks down, W is rebuilt with the diagonal
+//      scaled by 1 + c*u (a relative shift) and factored again;
+//   3. X = L^-T L^-1 B (FP32 factor, FP64 vectors);
+//   4. refinement: R = B - A X in FP64 against the untouched A, D = L^-T L^-1 R,
+//      X += D, until every column meets ||r|| <= ||x|| ||A|| eps sqrt(n) (the
+//      ?sposv test); when a sweep fails to halve the scaled residual the
+//      correction is computed by GMRES preconditioned by the factor instead;
+//   5. if neither converges within the budget, the FP64 path (ppotrf/ppotrs on A)
+//      produces X and iter = -(sweeps + 1).
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <limits>
 #include <stdexcept>
+#include <string>
 #include <vector>
 
 #include <ddla/ddla.h>
 #include <ddla_kernels.h>
 
 #include "ddla_stream.h"
+#include "gmres.h"
 
 namespace ddla {
+
+namespace {
+
+constexpr int kMaxSweeps = 30;        // as ?sposv's ITERMAX
+constexpr int kMaxShiftTries = 4;
+
+void ck(int e, const char* what) { detail::kernel_check(e, what); }
+
+struct Scalars {
+    double anrm;
+    int info;
+    int status;
+};
+
+}  // namespace
 
 void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nrhs, double* A, const int* descA,
                  const double* B, const int* descB, double* X, const int* descX, int& info, MixedReport* report)
@@ -29,18 +61,144 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
     if (n && (!A || (nrhs && (!B || !X)))) throw std::invalid_argument("pposv_mixed: null matrix");
     MixedReport rep;
     info = 0;
-    if (n == 0) {
+    if (report) *report = rep;
+    if (n == 0) return;
+    cudaStream_t st = h->stream;
+    const long long lda = descA[DDLA_LLD_], ldb = descB[DDLA_LLD_], ldx = descX[DDLA_LLD_];
+    auto copy_b_to_x = [&] {
+        if (nrhs)
+            detail::cuda_check(cudaMemcpy2DAsync(X, ldx * sizeof(double), B, ldb * sizeof(double),
+                                                 n * sizeof(double), nrhs, cudaMemcpyDeviceToDevice, st),
+                               "copy B to X");
+    };
+    auto fp64_path = [&](int sweeps) {
+        copy_b_to_x();
+        pposv<double>(h, 'L', 'L', 'N', n, nrhs, A, 1, 1, descA, X, 1, 1, descX, info);
+        rep.iter = precision == 'D' ? 0 : -(sweeps + 1);
         if (report) *report = rep;
+    };
+    if (precision == 'D') {
+        fp64_path(0);
         return;
     }
-    if (precision != 'D') throw std::invalid_argument("pposv_mixed: low-precision factor not available");
-    const long long ldb = descB[DDLA_LLD_], ldx = descX[DDLA_LLD_];
-    if (nrhs)
-        detail::cuda_check(cudaMemcpy2DAsync(X, ldx * sizeof(double), B, ldb * sizeof(double), n * sizeof(double),
-                                             nrhs, cudaMemcpyDeviceToDevice, h->stream),
-                           "copy B to X");
-    pposv<double>(h, 'L', 'L', 'N', n, nrhs, A, 1, 1, descA, X, 1, 1, descX, info);
-    if (report) *report = rep;
+    if (nrhs == 0) return;
+
+    // ---- workspace ----------------------------------------------------------
+    const long long ldw = (n + 3) / 4 * 4;
+    const std::size_t pbytes = ddlak_mixed_panel_bytes(n);
+    const std::size_t sbytes = ddlak_potrs_workspace(n, std::max(1, nrhs));
+    const int kry = GmresIR::kRestart;
+    const std::size_t bytes = detail::padded_bytes<float>((std::size_t)ldw * n) + 2 * pbytes +
+                              3 * detail::padded_bytes<double>((std::size_t)n * std::max(1, nrhs)) +
+                              detail::padded_bytes<double>(n) + detail::padded_bytes<Scalars>(1) +
+                              2 * detail::padded_bytes<double>(std::max(1, nrhs)) + sbytes +
+                              GmresIR::workspace_bytes(n, std::max(1, nrhs), kry);
+    detail::DeviceScratch ws(h, bytes);
+    char* w = ws.data();
+    float* W = detail::take<float>(w, (std::size_t)ldw * n);
+    void* P0 = w;
+    w += pbytes;
+    void* P1 = w;
+    w += pbytes;
+    double* R = detail::take<double>(w, (std::size_t)n * std::max(1, nrhs));
+    double* D = detail::take<double>(w, (std::size_t)n * std::max(1, nrhs));
+    double* Bc = detail::take<double>(w, (std::size_t)n * std::max(1, nrhs));
+    double* colsum = detail::take<double>(w, n);
+    Scalars* sc = detail::take<Scalars>(w, 1);
+    double* xn = detail::take<double>(w, std::max(1, nrhs));
+    double* rn = detail::take<double>(w, std::max(1, nrhs));
+    void* swork = w;
+    w += sbytes;
+    void* gwork = w;
+
+    Scalars hs{};
+    auto read_scalars = [&] {
+        detail::cuda_check(cudaMemcpyAsync(h->host_word, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st),
+                           "scalar read-back");
+        detail::cuda_check(cudaStreamSynchronize(st), "stream synchronisation");
+        std::memcpy(&hs, h->host_word, sizeof(Scalars));
+    };
+
+    // ---- 1 + 2: convert and factor (with a relative diagonal shift on breakdown) ----
+    const double u = precision == 'B' ? std::ldexp(1.0, -8) : std::ldexp(1.0, -11);
+    double shift = 0.0;
+    bool factored = false;
+    for (int attempt = 0; attempt < kMaxShiftTries && !factored; ++attempt) {
+        ck(ddlak_convert_lower(n, A, lda, W, ldw, 1.0 + shift, colsum, &sc->anrm, st), "convert to FP32");
+        ck(ddlak_potrf_mixed(precision, n, W, ldw, P0, P1, &sc->info, &sc->status, st), "mixed factorization");
+        read_scalars();
+        if (hs.status != 0) throw std::runtime_error("pposv_mixed: a tensor-core update wait timed out");
+        if (hs.info == 0) factored = true;
+        else shift = shift == 0.0 ? 2.0 * u : shift * 8.0;
+    }
+    rep.shift = factored ? shift : 0.0;
+    const double anrm = hs.anrm;
+    if (!factored || !(anrm > 0) || !std::isfinite(anrm) || nrhs == 0) {
+        fp64_path(0);
+        return;
+    }
+
+    // ---- 3: initial solve ----------------------------------------------------------
+    const double eps = std::numeric_limits<double>::epsilon() / 2;  // unit roundoff, as LAPACK dlamch('E')
+    const double cte = anrm * eps * std::sqrt((double)n);
+    detail::cuda_check(cudaMemcpy2DAsync(Bc, n * sizeof(double), B, ldb * sizeof(double), n * sizeof(double), nrhs,
+                                         cudaMemcpyDeviceToDevice, st),
+                       "copy B");
+    detail::cuda_check(cudaMemcpy2DAsync(X, ldx * sizeof(double), Bc, n * sizeof(double), n * sizeof(double), nrhs,
+                                         cudaMemcpyDeviceToDevice, st),
+                       "copy B to X");
+    ck(ddlak_potrs_mixed(n, nrhs, W, ldw, X, ldx, swork, sbytes, st), "initial solve");
+
+    std::vector<double> hx(nrhs), hr(nrhs);
+    auto residual_check = [&](double& worst) -> bool {
+        ck(ddlak_symm_residual(n, nrhs, A, lda, X, ldx, Bc, n, R, n, st), "residual");
+        ck(ddlak_colmax(n, nrhs, X, ldx, xn, st), "norm x");
+        ck(ddlak_colmax(n, nrhs, R, n, rn, st), "norm r");
+        detail::cuda_check(cudaMemcpyAsync(hx.data(), xn, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st), "norms");
+        detail::cuda_check(cudaMemcpyAsync(hr.data(), rn, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st), "norms");
+        detail::cuda_check(cudaStreamSynchronize(st), "stream synchronisation");
+        bool ok = true;
+        worst = 0;
+        for (int j = 0; j < nrhs; ++j) {
+            if (!std::isfinite(hr[j]) || !std::isfinite(hx[j])) return false;
+            ok = ok && hr[j] <= hx[j] * cte;
+            worst = std::max(worst, hx[j] > 0 ? hr[j] / (hx[j] * anrm) : (hr[j] > 0 ? INFINITY : 0.0));
+        }
+        return ok;
+    };
+
+    // ---- 4: refinement ---------------------------------------------------------------
+    double worst = 0, prev = INFINITY;
+    int sweeps = 0;
+    bool use_gmres = false;
+    GmresIR gmres(h, n, nrhs, A, lda, W, ldw, swork, sbytes, gwork, kry);
+    while (true) {
+        const bool ok = residual_check(worst);
+        rep.backward_error = worst;
+        if (ok) {
+            rep.iter = sweeps;
+            rep.gmres = use_gmres ? 1 : 0;
+            if (report) *report = rep;
+            return;
+        }
+        if (!std::isfinite(worst) || sweeps >= kMaxSweeps) break;
+        if (!use_gmres && sweeps > 0 && worst > 0.5 * prev) use_gmres = true;  // IR stagnates: switch to GMRES-IR
+        prev = worst;
+        if (use_gmres) {
+            // D = A^-1 R by left-preconditioned GMRES; each Krylov iteration counts as a sweep
+            const int its = gmres.solve(R, D, std::min(kry, kMaxSweeps - sweeps));
+            sweeps += std::max(1, its);
+        } else {
+            detail::cuda_check(cudaMemcpyAsync(D, R, sizeof(double) * n * nrhs, cudaMemcpyDeviceToDevice, st),
+                               "copy residual");
+            ck(ddlak_potrs_mixed(n, nrhs, W, ldw, D, n, swork, sbytes, st), "correction solve");
+            ++sweeps;
+        }
+        ck(ddlak_axpy(n, nrhs, 1.0, D, n, X, ldx, st), "update x");
+    }
+    rep.gmres = use_gmres ? 1 : 0;
+    // ---- 5: FP64 fallback ---------------------------------------------------------------
+    fp64_path(sweeps);
 }
 
 }  // namespace ddla

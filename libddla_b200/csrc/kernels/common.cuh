@@ -146,4 +146,56 @@ __device__ __forceinline__ bool bounded_wait_geq(const int* flag, int want, int*
 
 __host__ __device__ __forceinline__ long long ceil_div(long long a, long long b) { return (a + b - 1) / b; }
 
+// Asynchronous global -> shared copy of one element (zero-filled when !valid).
+template <int BYTES>
+__device__ __forceinline__ void cp_async_elem(void* smem, const void* gmem, bool valid)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(s), "l"(gmem), "n"(BYTES),
+                 "r"(valid ? BYTES : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_wait_all()
+{
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+// Load the L-view block L(r0+i, c0+j), i < rows, j < cols (and i >= j when
+// lower), into s[i + j*ld] with cp.async (one copy per element, coalesced for
+// either storage), then conjugate in place for 'U' complex storage.  Entries
+// outside the block are zero.  Ends with __syncthreads().
+template <class T, bool UP>
+__device__ __forceinline__ void load_lview_block(T* s, int ld, const T* A, long long lda, long long r0, long long c0,
+                                                 int rows, int cols, int brows, int bcols, bool lower)
+{
+    for (int idx = threadIdx.x; idx < brows * bcols; idx += blockDim.x) {
+        int i, j;
+        if (UP) { j = idx % bcols; i = idx / bcols; } else { i = idx % brows; j = idx / brows; }
+        const bool valid = i < rows && j < cols && (!lower || i >= j);
+        const T* src = UP ? A + (c0 + j) + (r0 + i) * lda : A + (r0 + i) + (c0 + j) * lda;
+        cp_async_elem<sizeof(T)>(&s[i + j * ld], valid ? src : A, valid);
+    }
+    cp_async_commit_wait_all();
+    __syncthreads();
+    if (UP && Traits<T>::cplx) {
+        for (int idx = threadIdx.x; idx < brows * bcols; idx += blockDim.x) {
+            const int i = idx % brows, j = idx / brows;
+            s[i + j * ld] = cj(s[i + j * ld]);
+        }
+        __syncthreads();
+    }
+}
+
+// Linear index b over the lower triangle of a tile grid (row-major: (0,0),
+// (1,0),(1,1),(2,0),...) -> tile (I, J) with J <= I.
+__device__ __forceinline__ void tile_of_tri(long long b, int& I, int& J)
+{
+    long long i = (long long)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
+    while ((i + 1) * (i + 2) / 2 <= b) ++i;
+    while (i * (i + 1) / 2 > b) --i;
+    I = (int)i;
+    J = (int)(b - i * (i + 1) / 2);
+}
+
 }  // namespace ddlak

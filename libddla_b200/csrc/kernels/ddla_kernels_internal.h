@@ -5,12 +5,19 @@
 
 namespace ddlak {
 
-// C -= L21 * L21^H on the lower tiles of the trailing matrix after block column
-// [k0, k0+nbk) of an order-n factorization (L view, see common.cuh).
+// C(i,j) -= sum_{k0 <= c < k0+nbk} L(i,c) conj(L(j,c)) for the lower-triangle
+// entries of the region rows [t0, n) x columns [t0, n) (cols == 0) or
+// columns [t0, t0+cols) (cols > 0), in the L view of common.cuh.
 template <class T, bool UP>
-cudaError_t trailing_update(T* A, long long lda, int k0, int nbk, int n, const int* dinfo, cudaStream_t st);
+cudaError_t trailing_update(T* A, long long lda, int k0, int nbk, int n, long long t0, int cols, const int* dinfo,
+                            cudaStream_t st);
+
+// X * L11^H = A21 for the rows below the diagonal block [k0, k0+nbk) (potrf.cu).
+template <class T, bool UP>
+cudaError_t launch_trsm_panel(T* A, long long lda, int k0, int nbk, int n, const int* dinfo, cudaStream_t s);
 
 template <class T, bool UP>
-cudaError_t trailing_update_simt(T* A, long long lda, int k0, int nbk, int n, const int* dinfo, cudaStream_t st);
+cudaError_t trailing_update_simt(T* A, long long lda, int k0, int nbk, int n, long long t0, int cols,
+                                 const int* dinfo, cudaStream_t st);
 
 }  // namespace ddlak

@@ -1,0 +1,714 @@
+// Mixed-precision Cholesky for ddla::pposv_mixed (no reference counterpart).
+//
+// The FP64 matrix A (lower) is copied to an FP32 working matrix W; W is
+// factored with the blocked right-looking scheme of potrf.cu, but
+//   * each diagonal block is factored in FP64 (FP32 storage widened in shared
+//     memory, diag_factor.cuh) and rounded back to FP32;
+//   * the panel solve runs in FP32 on W (k_trsm_panel<float>);
+//   * the panel is packed into a K-contiguous operand copy P (BF16, or FP32
+//     rounded to TF32) and the trailing update C -= P_I P_J^T runs on the
+//     5th-generation tensor cores: one elected thread issues tcgen05.mma into a
+//     128x128 FP32 accumulator in TMEM, operands arrive by TMA (128-byte
+//     swizzled, no cluster multicast), and all four warps read the accumulator
+//     back with tcgen05.ld for the FP32 read-modify-write of W.
+// The FP64 residuals and the refinement live in mixed.cpp / potrs.cu; the
+// symmetric residual R = B - A X (FP64, lower-stored A) is here too.
+#include <cuda_bf16.h>
+
+#include <mutex>
+
+#include "common.cuh"
+#include "ddla_kernels_internal.h"
+#include "diag_factor.cuh"
+#include "profile.h"
+#include "tc_common.cuh"
+
+namespace ddlak {
+
+namespace {
+
+constexpr int MX_NB = 128;  // block width of the mixed factorization (= UMMA tile)
+
+// ---------------------------------------------------------------------------
+// A (FP64, lower) -> W (FP32, lower); diagonal scaled by diag_scale;
+// colsum[j] += sum_i |A(i,j)| over the full symmetric matrix (for ||A||_inf).
+// One CTA per 64x64 lower tile.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_convert_lower(const double* __restrict__ A, long long lda,
+                                                       float* __restrict__ W, long long ldw, int n, double diag_scale,
+                                                       double* __restrict__ colsum)
+{
+    int I, J;
+    tile_of_tri(blockIdx.x, I, J);
+    const long long ri = (long long)I * 64, rj = (long long)J * 64;
+    __shared__ double csum[64];
+    __shared__ double rsum[4][64];
+    const int r = threadIdx.x & 63, cg = threadIdx.x >> 6;
+    if (threadIdx.x < 64) csum[threadIdx.x] = 0.0;
+    __syncthreads();
+    double rs = 0.0;
+    double vals[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+        const long long i = ri + r, j = rj + cg + 4 * u;
+        vals[u] = (i < n && j < n && i >= j) ? A[i + j * lda] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+        const long long i = ri + r, j = rj + cg + 4 * u;
+        if (i < n && j < n && i >= j) {
+            const double a = vals[u];
+            W[i + j * ldw] = (float)(i == j ? a * diag_scale : a);
+            const double aa = fabs(a);
+            atomicAdd(&csum[cg + 4 * u], aa);
+            if (i != j) rs += aa;
+        }
+    }
+    rsum[cg][r] = rs;
+    __syncthreads();
+    if (threadIdx.x < 64) {
+        const int t = threadIdx.x;
+        if (rj + t < n && csum[t] != 0.0) atomicAdd(&colsum[rj + t], csum[t]);
+        const double rt = rsum[0][t] + rsum[1][t] + rsum[2][t] + rsum[3][t];
+        if (ri + t < n && rt != 0.0) atomicAdd(&colsum[ri + t], rt);
+    }
+}
+
+// out[0] = max(v[0..n)), v >= 0
+__global__ void __launch_bounds__(256) k_max_nonneg(const double* __restrict__ v, int n, double* out)
+{
+    double m = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = fmax(m, v[i]);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<unsigned long long*>(out), __double_as_longlong(m));
+}
+
+// ---------------------------------------------------------------------------
+// diagonal block: FP32 storage, FP64 arithmetic
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_potrf_diag_mixed(float* __restrict__ W, long long ldw, int k0, int nbk,
+                                                          int* __restrict__ info)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* s = reinterpret_cast<double*>(smem_raw);
+    const int ld = nbk + 1;
+    if (*(volatile int*)info != 0) return;
+    const int total = nbk * nbk;
+    for (int base = 0; base < total; base += 16 * 256) {
+        float v[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            const int idx = base + u * 256 + threadIdx.x;
+            const int i = idx % nbk, j = idx / nbk;
+            v[u] = (idx < total && i >= j) ? W[(k0 + i) + (long long)(k0 + j) * ldw] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            const int idx = base + u * 256 + threadIdx.x;
+            if (idx < total) s[(idx % nbk) + (idx / nbk) * ld] = (double)v[u];
+        }
+    }
+    __syncthreads();
+    const int fail = factor_block_smem<double>(s, ld, nbk);
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const int i = idx % nbk, j = idx / nbk;
+        if (i >= j) W[(k0 + i) + (long long)(k0 + j) * ldw] = (float)s[i + j * ld];
+    }
+    if (fail && threadIdx.x == 0) *info = k0 + fail;
+}
+
+// ---------------------------------------------------------------------------
+// panel rows [pr0, n) x columns [k0, k0+nbk) of W -> P, K-contiguous:
+// P[r*nbk + k] = round(W[(pr0+r) + (k0+k)*ldw]) (BF16, or FP32 rounded to TF32)
+// ---------------------------------------------------------------------------
+template <bool TF32>
+__global__ void __launch_bounds__(256) k_pack_panel(const float* __restrict__ W, long long ldw, int n, long long pr0,
+                                                    int k0, int nbk, void* __restrict__ P, const int* __restrict__ info)
+{
+    __shared__ float t[32][33];
+    if (*(volatile int*)info != 0) return;
+    const long long r0 = (long long)blockIdx.x * 32;
+    const int kk0 = blockIdx.y * 32;
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const long long row = pr0 + r0 + threadIdx.x;
+        t[y][threadIdx.x] = row < n ? W[row + (long long)(k0 + kk0 + y) * ldw] : 0.f;
+    }
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const long long r = r0 + y;
+        if (pr0 + r >= n) continue;
+        const float x = t[threadIdx.x][y];
+        const long long off = r * nbk + kk0 + threadIdx.x;
+        if (TF32) {
+            uint32_t b;
+            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(b) : "f"(x));
+            reinterpret_cast<uint32_t*>(P)[off] = b;
+        } else {
+            reinterpret_cast<__nv_bfloat16*>(P)[off] = __float2bfloat16_rn(x);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// tcgen05 trailing update: W(i,j) -= sum_k P(i-pr0, k) P(j-pr0, k) on the lower
+// entries of one 128x128 tile of the region (rows [t0,n), cols [t0,n) or
+// [t0, t0+cols)).  128 threads: thread 0 issues TMA, thread 32 issues MMA,
+// all four warps run the epilogue on their 32 TMEM lanes.
+// ---------------------------------------------------------------------------
+constexpr int MU_STAGES = 2;
+constexpr int MU_TILE_BYTES = 128 * 128;  // 128 rows x 128 bytes
+constexpr size_t MU_SMEM = (size_t)MU_STAGES * 2 * MU_TILE_BYTES + 1024;
+
+enum : int { MU_ERR_EMPTY = 0x21, MU_ERR_FULL = 0x22, MU_ERR_DONE = 0x23 };
+
+template <bool TF32>
+__global__ void __launch_bounds__(128, 2) k_mixed_update(const __grid_constant__ CUtensorMap pmap,
+                                                         float* __restrict__ W, long long ldw, int n, long long t0,
+                                                         long long pr0, int cols, int nkb,
+                                                         const int* __restrict__ info, int* __restrict__ status)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[MU_STAGES], empty[MU_STAGES], done;
+    __shared__ uint32_t s_tmem;
+    if (*(volatile const int*)info != 0) return;
+    int I, J;
+    if (cols == 0) {
+        tile_of_tri(blockIdx.x, I, J);
+    } else {
+        const int nct = (cols + 127) / 128;
+        J = blockIdx.x % nct;
+        I = blockIdx.x / nct;
+        if (I < J) return;
+    }
+    const long long cend = cols == 0 ? (long long)n : t0 + cols;
+    const long long ri = t0 + (long long)I * 128, rj = t0 + (long long)J * 128;
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < MU_STAGES; ++s) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        tc::mbar_init(&done, 1);
+        tc::mbar_fence_init();
+    }
+    if (warp == 0) tc::tmem_alloc(&s_tmem, 128);
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = s_tmem;
+
+    if (threadIdx.x == 0) {
+        tc::prefetch_tmap(&pmap);
+        for (int kb = 0; kb < nkb; ++kb) {
+            const int s = kb % MU_STAGES;
+            if (kb >= MU_STAGES && !tc::mbar_wait(&empty[s], ((kb / MU_STAGES) - 1) & 1, status, MU_ERR_EMPTY)) break;
+            unsigned char* sa = base + (size_t)s * 2 * MU_TILE_BYTES;
+            tc::mbar_expect_tx(&full[s], 2 * MU_TILE_BYTES);
+            const int x = kb * (TF32 ? 32 : 64);
+            tc::tma_load_2d(sa, &pmap, &full[s], x, (int)(ri - pr0));
+            tc::tma_load_2d(sa + MU_TILE_BYTES, &pmap, &full[s], x, (int)(rj - pr0));
+        }
+    } else if (threadIdx.x == 32) {
+        constexpr uint32_t idesc = tc::idesc_m128_n128<TF32>();
+        bool ok = true;
+        for (int kb = 0; kb < nkb && ok; ++kb) {
+            const int s = kb % MU_STAGES;
+            ok = tc::mbar_wait(&full[s], (kb / MU_STAGES) & 1, status, MU_ERR_FULL);
+            if (!ok) break;
+            tc::tc_fence_after();
+            const unsigned char* sa = base + (size_t)s * 2 * MU_TILE_BYTES;
+            const uint64_t ad = tc::smem_desc_sw128(sa), bd = tc::smem_desc_sw128(sa + MU_TILE_BYTES);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)  // four K steps of 32 bytes per 128-byte row
+                tc::umma<TF32>(tmem, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0 ? 1u : 0u);
+            tc::umma_commit(&empty[s]);
+        }
+        tc::umma_commit(&done);
+    }
+    __syncwarp();
+
+    // epilogue
+    bool ok = tc::mbar_wait(&done, 0, status, MU_ERR_DONE);
+    ok = __all_sync(0xffffffffu, ok);
+    tc::tc_fence_after();
+    if (ok) {
+        const long long i = ri + 32 * warp + lane;
+#pragma unroll 1
+        for (int c = 0; c < 4; ++c) {
+            float v[32];
+            tc::tmem_ld_32x32b_x32(tmem + ((uint32_t)(32 * warp) << 16) + 32 * c, v);
+            float w[32];
+#pragma unroll
+            for (int e = 0; e < 32; ++e) {
+                const long long j = rj + 32 * c + e;
+                w[e] = (i < n && j < cend && i >= j) ? __ldcg(W + i + j * ldw) : 0.f;
+            }
+#pragma unroll
+            for (int e = 0; e < 32; ++e) {
+                const long long j = rj + 32 * c + e;
+                if (i < n && j < cend && i >= j) W[i + j * ldw] = w[e] - v[e];
+            }
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, 128);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// R = B - A X for symmetric A stored in its lower triangle (FP64), up to 16
+// right-hand sides per chunk (grid.y).  CTA I owns the 64-row block I and
+// reads the row strip A(I, 0..I) and the column strip A(I+1.., I) (the latter
+// transposed), so there are no atomics and the result is deterministic.
+// ---------------------------------------------------------------------------
+constexpr int SR = 64;
+__global__ void __launch_bounds__(256) k_symm_residual(const double* __restrict__ A, long long lda, int n, int nrhs,
+                                                       const double* __restrict__ X, long long ldx,
+                                                       const double* __restrict__ B, long long ldb,
+                                                       double* __restrict__ R, long long ldr)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double (*Tb)[SR][SR + 1] = reinterpret_cast<double (*)[SR][SR + 1]>(smem_raw);  // 2 tile buffers, raw [col][row]
+    double (*Xs)[17] = reinterpret_cast<double (*)[17]>(smem_raw + sizeof(double) * 2 * SR * (SR + 1));
+    const int I = blockIdx.x;
+    const int N = (int)ceil_div(n, SR);
+    const long long i0 = (long long)I * SR;
+    const int nrows = (int)((n - i0) < SR ? (n - i0) : SR);
+    const int r0 = blockIdx.y * 16;
+    const int nr = nrhs - r0 < 16 ? nrhs - r0 : 16;
+    const int tr = threadIdx.x & 63, tg = threadIdx.x >> 6;
+    double acc[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int r = tg + 4 * q;
+        acc[q] = (tr < nrows && r < nr) ? B[(i0 + tr) + (r0 + r) * ldb] : 0.0;
+    }
+    // visit v = 0..N-1: J = v; for v <= I the row-strip tile A(I, J) (raw rows of I, cols of J),
+    // for v > I the column-strip tile A(J, I) (raw rows of J, cols of I), used transposed.
+    auto issue = [&](int v, int buf) {
+        const int J = v;
+        const long long rr = v <= I ? i0 : (long long)J * SR;  // first raw row
+        const long long cc = v <= I ? (long long)J * SR : i0;  // first raw col
+        const int nrr = (int)((n - rr) < SR ? (n - rr) : SR);
+        const int ncc = (int)((n - cc) < SR ? (n - cc) : SR);
+        for (int idx = threadIdx.x; idx < SR * SR; idx += blockDim.x) {
+            const int rrow = idx % SR, ccol = idx / SR;
+            const bool valid = rrow < nrr && ccol < ncc && (rr + rrow >= cc + ccol);
+            cp_async_elem<8>(&Tb[buf][ccol][rrow], valid ? A + (rr + rrow) + (cc + ccol) * lda : A, valid);
+        }
+    };
+    issue(0, 0);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    for (int v = 0; v < N; ++v) {
+        if (v + 1 < N) issue(v + 1, (v + 1) & 1);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        const long long j0 = (long long)v * SR;
+        const int ncols = (int)((n - j0) < SR ? (n - j0) : SR);
+        for (int idx = threadIdx.x; idx < SR * 16; idx += blockDim.x) {
+            const int k = idx % SR, r = idx / SR;
+            Xs[k][r] = (k < ncols && r < nr) ? X[(j0 + k) + (r0 + r) * ldx] : 0.0;
+        }
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        __syncthreads();
+        const double (*Tt)[SR + 1] = Tb[v & 1];
+        if (v < I) {
+#pragma unroll 8
+            for (int k = 0; k < SR; ++k) {
+                const double a = Tt[k][tr];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[q] = fma(-a, Xs[k][tg + 4 * q], acc[q]);
+            }
+        } else if (v == I) {
+            // symmetric diagonal tile from its lower half: A(tr, k) = T[k][tr] (tr >= k) or T[tr][k]
+#pragma unroll 8
+            for (int k = 0; k < SR; ++k) {
+                const double a = tr >= k ? Tt[k][tr] : Tt[tr][k];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[q] = fma(-a, Xs[k][tg + 4 * q], acc[q]);
+            }
+        } else {
+#pragma unroll 8
+            for (int k = 0; k < SR; ++k) {
+                const double a = Tt[tr][k];  // A(J-row k, I-col tr)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[q] = fma(-a, Xs[k][tg + 4 * q], acc[q]);
+            }
+        }
+        __syncthreads();
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int r = tg + 4 * q;
+        if (tr < nrows && r < nr) R[(i0 + tr) + (r0 + r) * ldr] = acc[q];
+    }
+}
+
+// out[j] = max_i |M(i,j)| (out zeroed by the caller; atomics on the bit pattern of non-negative doubles)
+__global__ void __launch_bounds__(256) k_colmax(const double* __restrict__ M, long long ld, int n, int ncol,
+                                                double* __restrict__ out)
+{
+    const int j = blockIdx.y;
+    double m = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(M[i + j * ld]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && j < ncol)
+        atomicMax(reinterpret_cast<unsigned long long*>(out + j), __double_as_longlong(m));
+}
+
+// Y += alpha * X (n x ncol, column-major)
+__global__ void __launch_bounds__(256) k_axpy(int n, int ncol, double alpha, const double* __restrict__ X,
+                                              long long ldx, double* __restrict__ Y, long long ldy)
+{
+    const long long total = (long long)n * ncol;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long i = t % n, j = t / n;
+        Y[i + j * ldy] += alpha * X[i + j * ldx];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// GMRES helpers on column blocks (n x ncol, column-major, ld = n).  Vectors
+// V_0..V_{nv-1} are stored vstride doubles apart.
+// ---------------------------------------------------------------------------
+// out[i*ncol + c] = <V_i(:,c), w(:,c)>, one CTA per (i, c), fixed reduction order
+__global__ void __launch_bounds__(256) k_multidot(const double* __restrict__ V, long long vstride, int nv,
+                                                  const double* __restrict__ w, int n, int ncol,
+                                                  double* __restrict__ out)
+{
+    const int i = blockIdx.x, c = blockIdx.y;
+    const double* v = V + i * vstride + (long long)c * n;
+    const double* x = w + (long long)c * n;
+    double s = 0.0;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) s = fma(v[r], x[r], s);
+    __shared__ double part[8];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += part[k];
+        out[i * ncol + c] = t;
+    }
+}
+
+// w(:,c) -= sum_i coef[i*ncol + c] V_i(:,c)
+__global__ void __launch_bounds__(256) k_multi_axpy(const double* __restrict__ V, long long vstride, int nv,
+                                                    const double* __restrict__ coef, double* __restrict__ w, int n,
+                                                    int ncol)
+{
+    const long long total = (long long)n * ncol;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / n);
+        double acc = w[t];
+        for (int i = 0; i < nv; ++i) acc = fma(-coef[i * ncol + c], V[i * vstride + t], acc);
+        w[t] = acc;
+    }
+}
+
+// y(:,c) = alpha * x(:,c) / sqrt(nrm2[c])  (nrm2 == nullptr: y = alpha * x)
+__global__ void __launch_bounds__(256) k_scale_cols(const double* __restrict__ x, double* __restrict__ y, int n,
+                                                    int ncol, double alpha, const double* __restrict__ nrm2)
+{
+    const long long total = (long long)n * ncol;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / n);
+        double s = alpha;
+        if (nrm2) {
+            const double q = nrm2[c];
+            s = q > 0.0 ? alpha / sqrt(q) : 0.0;
+        }
+        y[t] = s * x[t];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeFn encode_fn()
+{
+    static EncodeFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeFn>(p);
+    });
+    return fn;
+}
+
+// P: rows x kp elements, K contiguous; box = 128 rows x 128 bytes, 128-byte swizzle
+bool encode_panel_map(CUtensorMap* map, const void* P, long long rows, int kp, bool tf32)
+{
+    EncodeFn fn = encode_fn();
+    if (!fn) return false;
+    const cuuint64_t esize = tf32 ? 4 : 2;
+    const cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)kp * esize};
+    const cuuint32_t box[2] = {(cuuint32_t)(128 / esize), 128u};
+    const cuuint32_t estr[2] = {1u, 1u};
+    const CUresult r = fn(map, tf32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                          const_cast<void*>(P), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+struct MixedStreams {
+    cudaStream_t hi = nullptr;
+    cudaEvent_t start = nullptr, panel = nullptr, rest = nullptr;
+};
+MixedStreams& mixed_streams()
+{
+    static thread_local MixedStreams res[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    MixedStreams& r = res[dev & 63];
+    if (r.hi == nullptr) {
+        int least = 0, greatest = 0;
+        cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        cudaStreamCreateWithPriority(&r.hi, cudaStreamNonBlocking, greatest);
+        cudaEventCreateWithFlags(&r.start, cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&r.panel, cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&r.rest, cudaEventDisableTiming);
+    }
+    return r;
+}
+
+template <bool TF32>
+cudaError_t mixed_update(float* W, long long ldw, int n, long long t0, long long pr0, int cols, const void* P,
+                         int nbk, const int* dinfo, int* status, cudaStream_t st)
+{
+    const long long m = (long long)n - t0;
+    if (m <= 0) return cudaSuccess;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaFuncSetAttribute(k_mixed_update<TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MU_SMEM);
+    });
+    CUtensorMap map;
+    if (!encode_panel_map(&map, P, (long long)n - pr0, nbk, TF32)) return cudaErrorInvalidValue;
+    const long long t = ceil_div(m, 128);
+    const long long grid = cols == 0 ? t * (t + 1) / 2 : t * ceil_div(cols, 128);
+    const int nkb = nbk / (TF32 ? 32 : 64);
+    const double md = (double)m, cw = cols ? (double)cols : md;
+    const double fl = cols ? 2.0 * nbk * (md * cw - cw * (cw - 1) / 2) : md * (md + 1) * nbk;
+    ProfScope ps(PK_MIXED_UPDATE, st, fl, 4.0 * (cols ? 2.0 * md * cw : md * (md + 1)));
+    k_mixed_update<TF32><<<(unsigned)grid, 128, MU_SMEM, st>>>(map, W, ldw, n, t0, pr0, cols, nkb, dinfo, status);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+template <bool TF32>
+cudaError_t potrf_mixed_enqueue(float* W, long long ldw, int n, void* P0, void* P1, int* dinfo, int* status,
+                                cudaStream_t st)
+{
+    constexpr int NB = MX_NB;
+    const size_t diag_smem = (size_t)NB * (NB + 1) * sizeof(double);
+    static std::once_flag once;
+    std::call_once(once, [&] {
+        cudaFuncSetAttribute(k_potrf_diag_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem);
+    });
+    MixedStreams& L = mixed_streams();
+    cudaStream_t hi = L.hi;
+    void* P[2] = {P0, P1};
+
+    auto diag_panel_pack = [&](int k0, int slot, cudaStream_t s) -> cudaError_t {
+        const int nbk = n - k0 < NB ? n - k0 : NB;
+        {
+            ProfScope ps(PK_MIXED_OTHER, s, (double)nbk * nbk * nbk / 3.0, 4.0 * nbk * (nbk + 1));
+            k_potrf_diag_mixed<<<1, 256, (size_t)nbk * (nbk + 1) * sizeof(double), s>>>(W, ldw, k0, nbk, dinfo);
+        }
+        note_launches(1);
+        const long long m = (long long)n - k0 - nbk;
+        if (m <= 0) return cudaGetLastError();
+        cudaError_t e = launch_trsm_panel<float, false>(W, ldw, k0, nbk, n, dinfo, s);
+        if (e != cudaSuccess) return e;
+        dim3 grid((unsigned)ceil_div(m, 32), nbk / 32);
+        {
+            ProfScope ps(PK_MIXED_OTHER, s, 0.0, (double)m * nbk * (4.0 + (TF32 ? 4.0 : 2.0)));
+            k_pack_panel<TF32><<<grid, dim3(32, 8), 0, s>>>(W, ldw, n, (long long)k0 + nbk, k0, nbk, P[slot], dinfo);
+        }
+        note_launches(1);
+        return cudaGetLastError();
+    };
+
+    cudaEventRecord(L.start, st);
+    cudaStreamWaitEvent(hi, L.start, 0);
+    cudaError_t e = diag_panel_pack(0, 0, hi);
+    if (e != cudaSuccess) return e;
+    cudaEventRecord(L.panel, hi);
+    bool have_rest = false;
+    int step = 0;
+    for (int k0 = 0; k0 + NB < n; k0 += NB, ++step) {
+        const long long t0 = (long long)k0 + NB;
+        const long long m = (long long)n - t0;
+        const int slot = step & 1;
+        cudaStreamWaitEvent(st, L.panel, 0);
+        if (m > NB) {
+            e = mixed_update<TF32>(W, ldw, n, t0 + NB, t0, 0, P[slot], NB, dinfo, status, st);
+            if (e != cudaSuccess) return e;
+        }
+        if (have_rest) cudaStreamWaitEvent(hi, L.rest, 0);
+        if (m > NB) {
+            cudaEventRecord(L.rest, st);
+            have_rest = true;
+        } else {
+            have_rest = false;
+        }
+        const int cols = m < NB ? (int)m : NB;
+        e = mixed_update<TF32>(W, ldw, n, t0, t0, cols, P[slot], NB, dinfo, status, hi);
+        if (e != cudaSuccess) return e;
+        e = diag_panel_pack((int)t0, slot ^ 1, hi);
+        if (e != cudaSuccess) return e;
+        cudaEventRecord(L.panel, hi);
+    }
+    cudaStreamWaitEvent(st, L.panel, 0);
+    if (have_rest) cudaStreamWaitEvent(st, L.rest, 0);
+    return cudaGetLastError();
+}
+
+}  // namespace
+}  // namespace ddlak
+
+extern "C" unsigned long long ddlak_mixed_panel_bytes(int n)
+{
+    // one K-contiguous panel copy: n rows x 128 columns of FP32 (the larger operand type)
+    return ((unsigned long long)(n > 0 ? n : 0) * ddlak::MX_NB * 4 + 255) / 256 * 256;
+}
+
+extern "C" int ddlak_convert_lower(int n, const void* A, long long lda, void* W, long long ldw, double diag_scale,
+                                   void* colsum, void* anrm, void* stream)
+{
+    using namespace ddlak;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (n <= 0) return 0;
+    cudaError_t e = cudaMemsetAsync(colsum, 0, sizeof(double) * n, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(anrm, 0, sizeof(double), st);
+    if (e != cudaSuccess) return (int)e;
+    const long long t = ceil_div(n, 64);
+    {
+        ProfScope ps(PK_MIXED_OTHER, st, 0.0, 6.0 * (double)n * n);
+        k_convert_lower<<<(unsigned)(t * (t + 1) / 2), 256, 0, st>>>(static_cast<const double*>(A), lda,
+                                                                     static_cast<float*>(W), ldw, n, diag_scale,
+                                                                     static_cast<double*>(colsum));
+        k_max_nonneg<<<148, 256, 0, st>>>(static_cast<const double*>(colsum), n, static_cast<double*>(anrm));
+    }
+    note_launches(2);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int ddlak_potrf_mixed(char precision, int n, void* W, long long ldw, void* P0, void* P1, int* dinfo,
+                                 int* status, void* stream)
+{
+    using namespace ddlak;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(dinfo, 0, sizeof(int), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, sizeof(int), st);
+    if (e != cudaSuccess) return (int)e;
+    if (n <= 0) return 0;
+    if (ldw % 4 != 0) return (int)cudaErrorInvalidValue;  // keeps every W column 16-byte aligned
+    float* w = static_cast<float*>(W);
+    if (precision == 'T') return (int)potrf_mixed_enqueue<true>(w, ldw, n, P0, P1, dinfo, status, st);
+    if (precision == 'B') return (int)potrf_mixed_enqueue<false>(w, ldw, n, P0, P1, dinfo, status, st);
+    return (int)cudaErrorInvalidValue;
+}
+
+extern "C" int ddlak_symm_residual(int n, int nrhs, const void* A, long long lda, const void* X, long long ldx,
+                                   const void* B, long long ldb, void* R, long long ldr, void* stream)
+{
+    using namespace ddlak;
+    if (n <= 0 || nrhs <= 0) return 0;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t smem = sizeof(double) * (2 * SR * (SR + 1) + SR * 17);
+    static std::once_flag once;
+    std::call_once(once, [&] {
+        cudaFuncSetAttribute(k_symm_residual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    });
+    dim3 grid((unsigned)ceil_div(n, SR), (unsigned)ceil_div(nrhs, 16));
+    {
+        ProfScope ps(PK_SYMM_RESIDUAL, st, 2.0 * (double)n * n * nrhs, 8.0 * (double)n * (n + 1) / 2 * 2);
+        k_symm_residual<<<grid, 256, smem, st>>>(static_cast<const double*>(A), lda, n, nrhs,
+                                                 static_cast<const double*>(X), ldx, static_cast<const double*>(B),
+                                                 ldb, static_cast<double*>(R), ldr);
+    }
+    note_launches(1);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int ddlak_colmax(int n, int ncol, const void* M, long long ld, void* out, void* stream)
+{
+    using namespace ddlak;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double) * (ncol > 0 ? ncol : 0), st);
+    if (e != cudaSuccess || n <= 0 || ncol <= 0) return (int)e;
+    dim3 grid((unsigned)(ceil_div(n, 256) < 64 ? ceil_div(n, 256) : 64), (unsigned)ncol);
+    k_colmax<<<grid, 256, 0, st>>>(static_cast<const double*>(M), ld, n, ncol, static_cast<double*>(out));
+    note_launches(1);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int ddlak_multidot(const void* V, long long vstride, int nv, const void* w, int n, int ncol, void* out,
+                              void* stream)
+{
+    using namespace ddlak;
+    if (nv <= 0 || n <= 0 || ncol <= 0) return 0;
+    k_multidot<<<dim3(nv, ncol), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const double*>(V), vstride, nv, static_cast<const double*>(w), n, ncol, static_cast<double*>(out));
+    note_launches(1);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int ddlak_multi_axpy(const void* V, long long vstride, int nv, const void* coef, void* w, int n, int ncol,
+                                void* stream)
+{
+    using namespace ddlak;
+    if (nv <= 0 || n <= 0 || ncol <= 0) return 0;
+    const long long total = (long long)n * ncol;
+    const long long grid = ceil_div(total, 256) < 1184 ? ceil_div(total, 256) : 1184;
+    k_multi_axpy<<<(unsigned)grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const double*>(V), vstride, nv, static_cast<const double*>(coef), static_cast<double*>(w), n,
+        ncol);
+    note_launches(1);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int ddlak_scale_cols(const void* x, void* y, int n, int ncol, double alpha, const void* nrm2, void* stream)
+{
+    using namespace ddlak;
+    if (n <= 0 || ncol <= 0) return 0;
+    const long long total = (long long)n * ncol;
+    const long long grid = ceil_div(total, 256) < 1184 ? ceil_div(total, 256) : 1184;
+    k_scale_cols<<<(unsigned)grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const double*>(x), static_cast<double*>(y), n, ncol, alpha, static_cast<const double*>(nrm2));
+    note_launches(1);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int ddlak_axpy(int n, int ncol, double alpha, const void* X, long long ldx, void* Y, long long ldy,
+                          void* stream)
+{
+    using namespace ddlak;
+    if (n <= 0 || ncol <= 0) return 0;
+    const long long total = (long long)n * ncol;
+    const long long grid = ceil_div(total, 256) < 1184 ? ceil_div(total, 256) : 1184;
+    k_axpy<<<(unsigned)grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(n, ncol, alpha,
+                                                                         static_cast<const double*>(X), ldx,
+                                                                         static_cast<double*>(Y), ldy);
+    note_launches(1);
+    return (int)cudaGetLastError();
+}

@@ -1,18 +1,26 @@
-// Blocked right-looking Cholesky (ddla::ppotrf / ddla::potrf on a 1x1 grid).
+// Blocked right-looking Cholesky with look-ahead (ddla::ppotrf / ddla::potrf on
+// a 1x1 grid).
 //
 // Replaces the vendor call the reference makes at src/Cholesky/potrf.cpp:106-113
-// (cusolverDn?potrf) with three kernels per block column k:
-//   1. k_potrf_diag   -- the nb x nb diagonal block factored in shared memory,
-//                        one __syncthreads per column, info detected in-kernel;
-//   2. k_trsm_panel   -- L21 = A21 * L11^{-H}, row blocks owned by warps, columns
-//                        by lanes, warp-shuffle broadcast of each solved entry;
-//   3. trailing update -- C -= L21 * L21^H on the lower tiles of the trailing
-//                        matrix (FP64 DMMA tiles for double, see syrk.cu).
+// (cusolverDn?potrf).  Per block column k of width NB:
+//   1. k_potrf_diag   -- the NB x NB diagonal block in shared memory, factored in
+//                        32-wide steps (diag_factor.cuh); info detected in-kernel;
+//   2. k_trsm_panel   -- L21 = A21 * L11^{-H}: warps own rows, lanes own columns,
+//                        each solved entry broadcast with a warp shuffle;
+//   3. trailing update -- C -= L21 * L21^H on lower tiles (FP64 DMMA for double,
+//                        syrk.cu; register-tiled SIMT for the other types).
+// Look-ahead: the update of block column k+1 plus the diagonal block and panel
+// of k+1 run on a high-priority internal stream while the update of the rest
+// of the trailing matrix runs on the caller's stream; events order the two so
+// that no tile is touched by both at once.
 // info follows LAPACK ?potrf: the order of the first leading minor that is not
 // positive definite (diagonal value <= 0 or NaN), 0 on success.  Every kernel
 // returns immediately once info is set, so the first failure is the one kept.
+#include <mutex>
+
 #include "common.cuh"
 #include "ddla_kernels_internal.h"
+#include "diag_factor.cuh"
 #include "profile.h"
 
 namespace ddlak {
@@ -24,45 +32,12 @@ template <class T, bool UP>
 __global__ void __launch_bounds__(256) k_potrf_diag(T* __restrict__ A, long long lda, int k0, int nbk,
                                                     int* __restrict__ info)
 {
-    using R = real_t<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* s = reinterpret_cast<T*>(smem_raw);
     const int ld = nbk + 1;
     if (*(volatile int*)info != 0) return;
-
-    for (int idx = threadIdx.x; idx < nbk * nbk; idx += blockDim.x) {
-        const int i = idx % nbk, j = idx / nbk;
-        if (i >= j) s[i + j * ld] = lview_ld<T, UP>(A, lda, k0 + i, k0 + j);
-    }
-    __syncthreads();
-
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    int fail = 0;
-    R dprev = R(1);
-    for (int j = 0; j < nbk; ++j) {
-        const R d = re(s[j + j * ld]);
-        // Column j-1 was last read by the previous iteration's update: scale it now.
-        if (j > 0) {
-            const R inv = R(1) / sqrt(dprev);
-            for (int i = j + threadIdx.x; i < nbk; i += blockDim.x) s[i + (j - 1) * ld] = scal(s[i + (j - 1) * ld], inv);
-            if (threadIdx.x == 0) s[(j - 1) + (j - 1) * ld] = from_real<T>(sqrt(dprev));
-        }
-        if (!(d > R(0))) { fail = j + 1; break; }
-        const R invd = R(1) / d;
-        for (int k = j + 1 + warp; k < nbk; k += nw) {
-            const T lkj = scal(cj(s[k + j * ld]), invd);
-            for (int i = k + lane; i < nbk; i += 32) s[i + k * ld] = fms(s[i + k * ld], s[i + j * ld], lkj);
-        }
-        dprev = d;
-        __syncthreads();
-    }
-    if (!fail) {
-        const int j = nbk;
-        const R inv = R(1) / sqrt(dprev);
-        for (int i = j + threadIdx.x; i < nbk; i += blockDim.x) s[i + (j - 1) * ld] = scal(s[i + (j - 1) * ld], inv);
-        if (threadIdx.x == 0) s[(j - 1) + (j - 1) * ld] = from_real<T>(sqrt(dprev));
-    }
-    __syncthreads();
+    load_lview_block<T, UP>(s, ld, A, lda, k0, k0, nbk, nbk, nbk, nbk, true);
+    const int fail = factor_block_smem<T>(s, ld, nbk);
     for (int idx = threadIdx.x; idx < nbk * nbk; idx += blockDim.x) {
         const int i = idx % nbk, j = idx / nbk;
         if (i >= j) lview_st<T, UP>(A, lda, k0 + i, k0 + j, s[i + j * ld]);
@@ -82,18 +57,17 @@ __global__ void __launch_bounds__(256) k_trsm_panel(T* __restrict__ A, long long
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* l11 = reinterpret_cast<T*>(smem_raw);  // [c + j*ldl], c,j < NQ*32, zero outside nbk
     const int ldl = NQ * 32 + 1;
+    __shared__ R s_rinv[NQ * 32];
     if (*(volatile int*)info != 0) return;
 
-    for (int idx = threadIdx.x; idx < NQ * 32 * NQ * 32; idx += blockDim.x) {
-        const int c = idx % (NQ * 32), j = idx / (NQ * 32);
-        T v = zero<T>();
-        if (c < nbk && j < nbk && c >= j) v = lview_ld<T, UP>(A, lda, k0 + c, k0 + j);
-        l11[c + j * ldl] = v;
-    }
+    load_lview_block<T, UP>(l11, ldl, A, lda, k0, k0, nbk, nbk, NQ * 32, NQ * 32, true);
+    // multiply by reciprocal pivots, as reference BLAS ?trsm does for side 'R'
+    for (int j = threadIdx.x; j < NQ * 32; j += blockDim.x) s_rinv[j] = j < nbk ? R(1) / re(l11[j + j * ldl]) : R(0);
     __syncthreads();
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long row0 = (long long)k0 + nbk + ((long long)blockIdx.x * (blockDim.x >> 5) + warp) * PR;
+    if (row0 >= n) return;
     T p[PR][NQ];
 #pragma unroll
     for (int r = 0; r < PR; ++r)
@@ -109,19 +83,13 @@ __global__ void __launch_bounds__(256) k_trsm_panel(T* __restrict__ A, long long
         for (int jj = 0; jj < 32; ++jj) {
             const int j = qj * 32 + jj;
             if (j >= nbk) break;
-            const R djj = re(l11[j + j * ldl]);
+            const R rjj = s_rinv[j];
             T x[PR];
 #pragma unroll
             for (int r = 0; r < PR; ++r) {
-                T v = divr(p[r][qj], djj);
+                const T v = scal(p[r][qj], rjj);
                 if (lane == jj) p[r][qj] = v;
-                if constexpr (Traits<T>::cplx) {
-                    v.x = __shfl_sync(0xffffffffu, v.x, jj);
-                    v.y = __shfl_sync(0xffffffffu, v.y, jj);
-                } else {
-                    v = __shfl_sync(0xffffffffu, v, jj);
-                }
-                x[r] = v;
+                x[r] = shfl(v, jj);
             }
 #pragma unroll
             for (int q = qj; q < NQ; ++q) {
@@ -145,29 +113,28 @@ __global__ void __launch_bounds__(256) k_trsm_panel(T* __restrict__ A, long long
 }
 
 // ---------------------------------------------------------------------------
-// 3. generic trailing update (SIMT; every type).  64x64 tiles of the lower
-//    trailing matrix, 16-wide k chunks through shared memory, 4x4 per thread.
+// 3. generic trailing update (SIMT; every type).  64x64 tiles, 16-wide k
+//    chunks through shared memory, 4x4 per thread.  Region: rows [t0, n) and
+//    columns [t0, n) (cols == 0, lower triangle of tiles) or [t0, t0+cols).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void tri_tile(long long b, int& I, int& J)
-{
-    long long i = (long long)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
-    while ((i + 1) * (i + 2) / 2 <= b) ++i;
-    while (i * (i + 1) / 2 > b) --i;
-    I = (int)i;
-    J = (int)(b - i * (i + 1) / 2);
-}
-
 template <class T, bool UP>
 __global__ void __launch_bounds__(256) k_syrk_simt(T* __restrict__ A, long long lda, int k0, int nbk, int n,
-                                                   const int* __restrict__ info)
+                                                   long long t0, int cols, const int* __restrict__ info)
 {
     constexpr int BT = 64, BK = 16;
     __shared__ T As[BK][BT + 1];
     __shared__ T Bs[BK][BT + 1];
     if (*(volatile int*)info != 0) return;
     int I, J;
-    tri_tile(blockIdx.x, I, J);
-    const long long t0 = (long long)k0 + nbk;
+    if (cols == 0) {
+        tile_of_tri(blockIdx.x, I, J);
+    } else {
+        const int nct = (cols + BT - 1) / BT;
+        J = blockIdx.x % nct;
+        I = blockIdx.x / nct;
+        if (I < J) return;
+    }
+    const long long cend = cols == 0 ? (long long)n : t0 + cols;
     const long long ri = t0 + (long long)I * BT, rj = t0 + (long long)J * BT;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     T acc[4][4];
@@ -182,7 +149,7 @@ __global__ void __launch_bounds__(256) k_syrk_simt(T* __restrict__ A, long long 
             if (UP) { k = idx % BK; i = idx / BK; } else { i = idx % BT; k = idx / BT; }
             const bool kin = kc + k < nbk;
             As[k][i] = (kin && ri + i < n) ? lview_ld<T, UP>(A, lda, ri + i, k0 + kc + k) : zero<T>();
-            Bs[k][i] = (kin && rj + i < n) ? lview_ld<T, UP>(A, lda, rj + i, k0 + kc + k) : zero<T>();
+            Bs[k][i] = (kin && rj + i < cend) ? lview_ld<T, UP>(A, lda, rj + i, k0 + kc + k) : zero<T>();
         }
         __syncthreads();
 #pragma unroll
@@ -204,17 +171,86 @@ __global__ void __launch_bounds__(256) k_syrk_simt(T* __restrict__ A, long long 
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             const long long i = ri + tx + 16 * a, j = rj + ty + 16 * b;
-            if (i < n && j < n && i >= j) {
+            if (i < n && j < cend && i >= j) {
                 T c = lview_ld<T, UP>(A, lda, i, j);
                 lview_st<T, UP>(A, lda, i, j, sub(c, acc[a][b]));
             }
         }
 }
 
+template <class T, bool UP>
+cudaError_t trailing_update_simt(T* A, long long lda, int k0, int nbk, int n, long long t0, int cols, const int* dinfo,
+                                 cudaStream_t st)
+{
+    const long long m = (long long)n - t0;
+    if (m <= 0) return cudaSuccess;
+    const long long t = ceil_div(m, 64);
+    const long long grid = cols == 0 ? t * (t + 1) / 2 : t * ceil_div(cols, 64);
+    k_syrk_simt<T, UP><<<(unsigned)grid, 256, 0, st>>>(A, lda, k0, nbk, n, t0, cols, dinfo);
+    return cudaGetLastError();
+}
+
+#define DDLAK_INST_SIMT(T, UP)                                                                                      \
+    template cudaError_t trailing_update_simt<T, UP>(T*, long long, int, int, int, long long, int, const int*,     \
+                                                     cudaStream_t);
+DDLAK_INST_SIMT(float, false)
+DDLAK_INST_SIMT(float, true)
+DDLAK_INST_SIMT(double, false)
+DDLAK_INST_SIMT(double, true)
+DDLAK_INST_SIMT(cf32, false)
+DDLAK_INST_SIMT(cf32, true)
+DDLAK_INST_SIMT(cf64, false)
+DDLAK_INST_SIMT(cf64, true)
+#undef DDLAK_INST_SIMT
+
 // ---------------------------------------------------------------------------
 // host-side enqueue of the whole factorization
 // ---------------------------------------------------------------------------
 template <class T> constexpr int potrf_nb() { return sizeof(T) == 16 ? 64 : 128; }
+
+template <class T, bool UP>
+cudaError_t launch_trsm_panel(T* A, long long lda, int k0, int nbk, int n, const int* dinfo, cudaStream_t s)
+{
+    constexpr int NQ = potrf_nb<T>() / 32;
+    constexpr int PR = sizeof(T) >= 16 ? 4 : 8;
+    const size_t panel_smem = (size_t)(NQ * 32) * (NQ * 32 + 1) * sizeof(T);
+    static std::once_flag once;
+    std::call_once(once, [&] {
+        cudaFuncSetAttribute(k_trsm_panel<T, UP, NQ, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)panel_smem);
+    });
+    const long long m = (long long)n - k0 - nbk;
+    if (m <= 0) return cudaSuccess;
+    const double cf = Traits<T>::cplx ? 4.0 : 1.0, md = (double)m, b = nbk;
+    ProfScope ps(PK_TRSM_PANEL, s, cf * md * b * b, sizeof(T) * (2.0 * md * b + b * (b + 1) / 2));
+    k_trsm_panel<T, UP, NQ, PR><<<(unsigned)ceil_div(m, 8 * PR), 256, panel_smem, s>>>(A, lda, k0, nbk, n, dinfo);
+    note_launches(1);
+    return cudaGetLastError();
+}
+template cudaError_t launch_trsm_panel<float, false>(float*, long long, int, int, int, const int*, cudaStream_t);
+
+namespace {
+struct LookaheadRes {
+    cudaStream_t hi = nullptr;
+    cudaEvent_t start = nullptr, panel = nullptr, rest = nullptr;
+};
+LookaheadRes& lookahead_res()
+{
+    static thread_local LookaheadRes res[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    LookaheadRes& r = res[dev & 63];
+    if (r.hi == nullptr) {
+        int least = 0, greatest = 0;
+        cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        cudaStreamCreateWithPriority(&r.hi, cudaStreamNonBlocking, greatest);
+        cudaEventCreateWithFlags(&r.start, cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&r.panel, cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&r.rest, cudaEventDisableTiming);
+    }
+    return r;
+}
+}  // namespace
 
 template <class T, bool UP>
 static cudaError_t potrf_enqueue(T* A, long long lda, int n, int* dinfo, cudaStream_t st)
@@ -224,59 +260,79 @@ static cudaError_t potrf_enqueue(T* A, long long lda, int n, int* dinfo, cudaStr
     constexpr int PR = sizeof(T) >= 16 ? 4 : 8;
     const size_t diag_smem = (size_t)NB * (NB + 1) * sizeof(T);
     const size_t panel_smem = (size_t)(NQ * 32) * (NQ * 32 + 1) * sizeof(T);
-    static bool attr_done = false;
-    if (!attr_done) {
+    static std::once_flag attr_once;
+    std::call_once(attr_once, [&] {
         cudaFuncSetAttribute(k_potrf_diag<T, UP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem);
         cudaFuncSetAttribute(k_trsm_panel<T, UP, NQ, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)panel_smem);
-        attr_done = true;
-    }
+    });
     const double cf = Traits<T>::cplx ? 4.0 : 1.0;  // real flops per multiply-add relative to a real one
-    for (int k0 = 0; k0 < n; k0 += NB) {
+    LookaheadRes& L = lookahead_res();
+    cudaStream_t hi = L.hi;
+
+    auto diag_and_panel = [&](int k0, cudaStream_t s) {
         const int nbk = n - k0 < NB ? n - k0 : NB;
         const double b = nbk;
         {
-            ProfScope ps(PK_POTRF_DIAG, st, cf * b * b * b / 3.0, sizeof(T) * b * (b + 1));
-            k_potrf_diag<T, UP><<<1, 256, (size_t)nbk * (nbk + 1) * sizeof(T), st>>>(A, lda, k0, nbk, dinfo);
+            ProfScope ps(PK_POTRF_DIAG, s, cf * b * b * b / 3.0, sizeof(T) * b * (b + 1));
+            k_potrf_diag<T, UP><<<1, 256, (size_t)nbk * (nbk + 1) * sizeof(T), s>>>(A, lda, k0, nbk, dinfo);
         }
         note_launches(1);
         const long long m = (long long)n - k0 - nbk;
-        if (m <= 0) break;
-        const int rows_per_cta = 8 * PR;
+        if (m <= 0) return;
         const double md = (double)m;
         {
-            ProfScope ps(PK_TRSM_PANEL, st, cf * md * b * b, sizeof(T) * (2.0 * md * b + b * (b + 1) / 2));
-            k_trsm_panel<T, UP, NQ, PR><<<(unsigned)ceil_div(m, rows_per_cta), 256, panel_smem, st>>>(A, lda, k0,
-                                                                                                       nbk, n, dinfo);
+            ProfScope ps(PK_TRSM_PANEL, s, cf * md * b * b, sizeof(T) * (2.0 * md * b + b * (b + 1) / 2));
+            k_trsm_panel<T, UP, NQ, PR><<<(unsigned)ceil_div(m, 8 * PR), 256, panel_smem, s>>>(A, lda, k0, nbk, n,
+                                                                                                dinfo);
         }
         note_launches(1);
-        {
-            ProfScope ps(PK_SYRK_UPDATE, st, cf * md * (md + 1) * b, sizeof(T) * (md * (md + 1) + md * b));
-            const cudaError_t e = trailing_update<T, UP>(A, lda, k0, nbk, n, dinfo, st);
+    };
+    auto update = [&](int k0, long long t0, int cols, cudaStream_t s) -> cudaError_t {
+        const int nbk = NB;
+        const double md = (double)(n - t0), b = nbk;
+        const double cw = cols ? (double)cols : md;
+        const double fl = cols ? cf * 2.0 * b * (md * cw - cw * (cw - 1) / 2) : cf * md * (md + 1) * b;
+        ProfScope ps(PK_SYRK_UPDATE, s, fl, sizeof(T) * ((cols ? 2.0 * md * cw : md * (md + 1)) + md * b));
+        const cudaError_t e = trailing_update<T, UP>(A, lda, k0, nbk, n, t0, cols, dinfo, s);
+        note_launches(1);
+        return e;
+    };
+
+    // fork: the internal stream starts after everything already queued on st
+    cudaEventRecord(L.start, st);
+    cudaStreamWaitEvent(hi, L.start, 0);
+    diag_and_panel(0, hi);
+    cudaEventRecord(L.panel, hi);
+    bool have_rest = false;
+    for (int k0 = 0; k0 + NB < n; k0 += NB) {
+        const long long t0 = (long long)k0 + NB;       // first row of the trailing matrix
+        const long long m = (long long)n - t0;
+        // the rest of the trailing matrix (block columns >= k+2) on st, once panel k exists
+        cudaStreamWaitEvent(st, L.panel, 0);
+        if (m > NB) {
+            const cudaError_t e = update(k0, t0 + NB, 0, st);
             if (e != cudaSuccess) return e;
         }
-        note_launches(1);
+        // block column k+1 was last written by the previous rest update
+        if (have_rest) cudaStreamWaitEvent(hi, L.rest, 0);
+        if (m > NB) {
+            cudaEventRecord(L.rest, st);
+            have_rest = true;
+        } else {
+            have_rest = false;
+        }
+        const int cols = m < NB ? (int)m : NB;
+        const cudaError_t e = update(k0, t0, cols, hi);
+        if (e != cudaSuccess) return e;
+        diag_and_panel((int)t0, hi);
+        cudaEventRecord(L.panel, hi);
     }
+    // join
+    cudaStreamWaitEvent(st, L.panel, 0);
+    if (have_rest) cudaStreamWaitEvent(st, L.rest, 0);
     return cudaGetLastError();
 }
-
-template <class T, bool UP>
-cudaError_t trailing_update_simt(T* A, long long lda, int k0, int nbk, int n, const int* dinfo, cudaStream_t st)
-{
-    const long long m = (long long)n - k0 - nbk;
-    const long long t = ceil_div(m, 64);
-    k_syrk_simt<T, UP><<<(unsigned)(t * (t + 1) / 2), 256, 0, st>>>(A, lda, k0, nbk, n, dinfo);
-    return cudaSuccess;
-}
-
-template cudaError_t trailing_update_simt<float, false>(float*, long long, int, int, int, const int*, cudaStream_t);
-template cudaError_t trailing_update_simt<float, true>(float*, long long, int, int, int, const int*, cudaStream_t);
-template cudaError_t trailing_update_simt<double, false>(double*, long long, int, int, int, const int*, cudaStream_t);
-template cudaError_t trailing_update_simt<double, true>(double*, long long, int, int, int, const int*, cudaStream_t);
-template cudaError_t trailing_update_simt<cf32, false>(cf32*, long long, int, int, int, const int*, cudaStream_t);
-template cudaError_t trailing_update_simt<cf32, true>(cf32*, long long, int, int, int, const int*, cudaStream_t);
-template cudaError_t trailing_update_simt<cf64, false>(cf64*, long long, int, int, int, const int*, cudaStream_t);
-template cudaError_t trailing_update_simt<cf64, true>(cf64*, long long, int, int, int, const int*, cudaStream_t);
 
 template <class T>
 static cudaError_t potrf_typed(char uplo, int n, void* A, long long lda, int* dinfo, cudaStream_t st)

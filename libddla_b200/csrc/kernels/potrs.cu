@@ -12,11 +12,21 @@
 // started, so the waits always end; each wait is additionally bounded by a
 // clock budget and reports DDLAK_WAIT_TIMEOUT instead of spinning forever.
 //
+// Each CTA streams the off-diagonal tiles of its block row through a
+// double-buffered cp.async ring (the tile loads do not depend on other CTAs,
+// only the solved blocks do), visiting them in publication order, then solves
+// its diagonal block with one warp per pair of right-hand sides using
+// reciprocal pivots and warp shuffles.
+//
 // The right-hand sides are a view X(i, r): B[i + r*ldb] for side 'L' and
 // conj(B[r + i*ldb]) for side 'R' (X * A = B  <=>  A * X^H = B^H, since A is
 // Hermitian).  They are processed in chunks of RC columns; chunk c uses its own
 // flag row and tickets interleave chunks so the ordering argument holds per
 // chunk.
+#include <mutex>
+
+#include <ddla_kernels.h>
+
 #include "common.cuh"
 #include "ddla_kernels_internal.h"
 #include "profile.h"
@@ -29,12 +39,6 @@ constexpr int RB = 64;   // rows per block row
 constexpr int RC = 16;   // right-hand sides per chunk
 constexpr int NT = 256;  // threads per CTA
 
-template <class T, bool BT>
-__device__ __forceinline__ T x_ld(const T* B, long long ldb, long long i, long long r)
-{
-    if (BT) return cj(B[r + i * ldb]);
-    return B[i + r * ldb];
-}
 template <class T, bool BT>
 __device__ __forceinline__ T x_ld_cg(const T* B, long long ldb, long long i, long long r)
 {
@@ -52,15 +56,53 @@ __device__ __forceinline__ void x_st(T* B, long long ldb, long long i, long long
     else B[i + r * ldb] = v;
 }
 
-template <class T, bool UP, bool BT>
-__global__ void __launch_bounds__(NT) k_potrs_fused(const T* __restrict__ A, long long lda, T* B, long long ldb, int n,
-                                                    int nrhs, int nchunks, int* flags, int* ticket, int* status)
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <class T>
+__device__ __forceinline__ T shfl_t(T v, int src)
 {
+    if constexpr (Traits<T>::cplx) {
+        v.x = __shfl_sync(0xffffffffu, v.x, src);
+        v.y = __shfl_sync(0xffffffffu, v.y, src);
+        return v;
+    } else {
+        return __shfl_sync(0xffffffffu, v, src);
+    }
+}
+
+// Shared-memory layout (elements of T unless noted):
+//   Lbuf[2][RB][RB+1]  raw off-diagonal tiles, Lbuf[b][k][i]
+//   Xs[RB][RC+1]       the solved block of the other block row
+//   Acc[RB][RC+1]      this block row's right-hand sides
+//   Rinv[RB]           reciprocal pivots (real type)
+// The factor is stored as TL and the right-hand sides as TX (TL == TX on the
+// plain path; an FP32 factor with FP64 vectors for the mixed-precision solves).
+template <class TL, class TX>
+__host__ __device__ constexpr size_t potrs_smem_bytes()
+{
+    return sizeof(TL) * 2 * (size_t)RB * (RB + 1) + sizeof(TX) * 2 * (size_t)RB * (RC + 1) + sizeof(real_t<TX>) * RB;
+}
+
+template <class TX, class TL>
+__device__ __forceinline__ TX widen(TL v)
+{
+    if constexpr (std::is_same<TX, TL>::value) return v;
+    else return static_cast<TX>(v);
+}
+
+template <class TL, class TX, bool UP, bool BT>
+__global__ void __launch_bounds__(NT) k_potrs_fused(const TL* __restrict__ A, long long lda, TX* B, long long ldb,
+                                                    int n, int nrhs, int nchunks, int* flags, int* ticket,
+                                                    int* status)
+{
+    using T = TX;
     using R = real_t<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T (*Ls)[RB + 1] = reinterpret_cast<T (*)[RB + 1]>(smem_raw);                 // off-diagonal tile, Ls[k][i]
-    T (*Xs)[RC + 1] = reinterpret_cast<T (*)[RC + 1]>(smem_raw + sizeof(T) * RB * (RB + 1));  // other row's block
-    T (*acc_s)[RC + 1] = Xs + RB;
+    TL (*Lbuf)[RB][RB + 1] = reinterpret_cast<TL (*)[RB][RB + 1]>(smem_raw);
+    T (*Xs)[RC + 1] = reinterpret_cast<T (*)[RC + 1]>(smem_raw + sizeof(TL) * 2 * RB * (RB + 1));
+    T (*Acc)[RC + 1] = Xs + RB;
+    R* Rinv = reinterpret_cast<R*>(Acc + RB);
     __shared__ int s_t;
     __shared__ int s_abort;
     if (threadIdx.x == 0) { s_t = atomicAdd(ticket, 1); s_abort = 0; }
@@ -76,11 +118,46 @@ __global__ void __launch_bounds__(NT) k_potrs_fused(const T* __restrict__ A, lon
     const int nr = (int)((nrhs - r0) < RC ? (nrhs - r0) : RC);
     const long long i0 = (long long)blk * RB;
     const int nrows = (int)((n - i0) < RB ? (n - i0) : RB);
+    // raw tile element (i, k): A[(i0+i) + (j0+k)*lda] when p1, A[(j0+k) + (i0+i)*lda] otherwise;
+    // the operator entry is that value, conjugated when !p1 (see the four cases of the L view)
+    const bool p1 = (fwd != UP);
 
-    // thread -> (row, rhs group): rows tid%64, rhs (tid/64) + 4*q
-    const int tr = threadIdx.x & (RB - 1);
-    const int tg = threadIdx.x >> 6;
+    const int tr = threadIdx.x & (RB - 1);  // row of the block row
+    const int tg = threadIdx.x >> 6;        // rhs group: columns tg, tg+4, tg+8, tg+12
     T acc[RC / 4];
+
+    // Visit the other block rows in publication order (forward 0, 1, ..; backward N-1, N-2, ..):
+    // every wait but the last one is already satisfied when reached.
+    const int nvisit = fwd ? blk : N - 1 - blk;
+    auto visit = [&](int v) { return fwd ? v : N - 1 - v; };
+    auto issue_tile = [&](int j, int buf) {
+        const long long j0 = (long long)j * RB;
+        const int ncols = (int)((n - j0) < RB ? (n - j0) : RB);
+        for (int idx = threadIdx.x; idx < RB * RB; idx += NT) {
+            int i, k;
+            const TL* src;
+            if (p1) { i = idx % RB; k = idx / RB; src = A + (i0 + i) + (j0 + k) * lda; }
+            else { k = idx % RB; i = idx / RB; src = A + (j0 + k) + (i0 + i) * lda; }
+            const bool valid = i < nrows && k < ncols;
+            cp_async_elem<sizeof(TL)>(&Lbuf[buf][k][i], valid ? src : A, valid);
+        }
+    };
+    // the diagonal block, raw: D[c][r] = A[(i0+r) + (i0+c)*lda] for 'L', A[(i0+c) + (i0+r)*lda] for 'U';
+    // L(r, c) = D[c][r] ('L') or conj(D[c][r]) ('U') for r >= c.  Prefetched into the ring slot
+    // the last off-diagonal tile leaves free, so it is resident when the solve reaches it.
+    auto issue_diag = [&](int buf) {
+        for (int idx = threadIdx.x; idx < RB * RB; idx += NT) {
+            int r, c;
+            const TL* src;
+            if (!UP) { r = idx % RB; c = idx / RB; src = A + (i0 + r) + (i0 + c) * lda; }
+            else { c = idx % RB; r = idx / RB; src = A + (i0 + c) + (i0 + r) * lda; }
+            const bool valid = r < nrows && c < nrows;
+            cp_async_elem<sizeof(TL)>(&Lbuf[buf][c][r], valid ? src : A, valid);
+        }
+    };
+    if (nvisit > 0) issue_tile(visit(0), 0);
+    else issue_diag(0);
+    cp_commit();
 
     if (!fwd) {
         // the block row's own forward result must be published first
@@ -89,7 +166,7 @@ __global__ void __launch_bounds__(NT) k_potrs_fused(const T* __restrict__ A, lon
             __threadfence();
         }
         __syncthreads();
-        if (s_abort) return;
+        if (s_abort) { cp_wait<0>(); return; }
     }
 #pragma unroll
     for (int q = 0; q < RC / 4; ++q) {
@@ -97,135 +174,140 @@ __global__ void __launch_bounds__(NT) k_potrs_fused(const T* __restrict__ A, lon
         acc[q] = (tr < nrows && r < nr) ? x_ld_cg<T, BT>(B, ldb, i0 + tr, r0 + r) : zero<T>();
     }
 
-    const int jbeg = fwd ? 0 : blk + 1;
-    const int jend = fwd ? blk : N;
-    for (int j = jbeg; j < jend; ++j) {
+    for (int v = 0; v < nvisit; ++v) {
+        const int j = visit(v);
         const long long j0 = (long long)j * RB;
         const int ncols = (int)((n - j0) < RB ? (n - j0) : RB);
-        // tile: forward L(i0+i, j0+k); backward L^H(i0+i, j0+k) = conj(L(j0+k, i0+i))
-        for (int idx = threadIdx.x; idx < RB * RB; idx += NT) {
-            int i, k;
-            if (fwd != UP) { i = idx % RB; k = idx / RB; } else { k = idx % RB; i = idx / RB; }
-            T v = zero<T>();
-            if (i < nrows && k < ncols)
-                v = fwd ? lview_ld<T, UP>(A, lda, i0 + i, j0 + k) : cj(lview_ld<T, UP>(A, lda, j0 + k, i0 + i));
-            Ls[k][i] = v;
-        }
+        if (v + 1 < nvisit) issue_tile(visit(v + 1), (v + 1) & 1);
+        else issue_diag((v + 1) & 1);
+        cp_commit();
         if (threadIdx.x == 0) {
             if (!bounded_wait_geq(&cflags[fwd ? j : N + j], 1, status)) s_abort = 1;
             __threadfence();
         }
         __syncthreads();
-        if (s_abort) return;
+        if (s_abort) { cp_wait<0>(); return; }
         for (int idx = threadIdx.x; idx < RB * RC; idx += NT) {
             const int k = idx % RB, r = idx / RB;
             Xs[k][r] = (k < ncols && r < nr) ? x_ld_cg<T, BT>(B, ldb, j0 + k, r0 + r) : zero<T>();
         }
+        cp_wait<1>();
         __syncthreads();
+        const TL (*Lt)[RB + 1] = Lbuf[v & 1];
+        if (p1) {
 #pragma unroll 8
-        for (int k = 0; k < RB; ++k) {
-            const T l = Ls[k][tr];
+            for (int k = 0; k < RB; ++k) {
+                const T l = widen<T>(Lt[k][tr]);
 #pragma unroll
-            for (int q = 0; q < RC / 4; ++q) acc[q] = fms(acc[q], l, Xs[k][tg + 4 * q]);
+                for (int q = 0; q < RC / 4; ++q) acc[q] = fms(acc[q], l, Xs[k][tg + 4 * q]);
+            }
+        } else {
+#pragma unroll 8
+            for (int k = 0; k < RB; ++k) {
+                const T l = cj(widen<T>(Lt[k][tr]));
+#pragma unroll
+                for (int q = 0; q < RC / 4; ++q) acc[q] = fms(acc[q], l, Xs[k][tg + 4 * q]);
+            }
         }
         __syncthreads();
     }
+    cp_wait<0>();
 
-    // diagonal block: forward solves L_bb y = acc, backward L_bb^H x = acc
-    for (int idx = threadIdx.x; idx < RB * RB; idx += NT) {
-        const int i = idx % RB, k = idx / RB;
-        // Ls[k][i] = L_bb(i, k) for i >= k
-        Ls[k][i] = (i < nrows && k < nrows && i >= k) ? lview_ld<T, UP>(A, lda, i0 + i, i0 + k) : zero<T>();
-    }
+    const TL (*D)[RB + 1] = Lbuf[nvisit & 1];
+    // L(r, c) for r >= c, and conj(L(c, r)) for c > r, from the raw diagonal block
+    auto lval = [&](int r, int c) { return UP ? cj(widen<T>(D[c][r])) : widen<T>(D[c][r]); };
+    auto lcval = [&](int c, int r) { return UP ? widen<T>(D[r][c]) : cj(widen<T>(D[r][c])); };
 #pragma unroll
-    for (int q = 0; q < RC / 4; ++q) acc_s[tr][tg + 4 * q] = acc[q];
+    for (int q = 0; q < RC / 4; ++q) Acc[tr][tg + 4 * q] = acc[q];
+    __syncthreads();
+    for (int k = threadIdx.x; k < RB; k += NT) Rinv[k] = k < nrows ? R(1) / re(widen<T>(D[k][k])) : R(0);
     __syncthreads();
     {
-        // 8 warps x 2 rhs columns; lanes own rows lane and lane+32
+        // warp w solves right-hand sides 2w and 2w+1 together; lanes own rows lane and lane+32
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        for (int rr = 0; rr < RC / 8; ++rr) {
-            const int r = warp * (RC / 8) + rr;
-            T v0 = acc_s[lane][r], v1 = acc_s[lane + 32][r];
-            if (fwd) {
-                for (int k = 0; k < nrows; ++k) {
-                    const R dkk = re(Ls[k][k]);
-                    T xk;
-                    if (k < 32) {
-                        if (lane == k) v0 = divr(v0, dkk);
-                        xk = v0;
-                        if constexpr (Traits<T>::cplx) {
-                            xk.x = __shfl_sync(0xffffffffu, xk.x, k);
-                            xk.y = __shfl_sync(0xffffffffu, xk.y, k);
-                        } else xk = __shfl_sync(0xffffffffu, xk, k);
-                        if (lane > k) v0 = fms(v0, Ls[k][lane], xk);
-                        v1 = fms(v1, Ls[k][lane + 32], xk);
-                    } else {
-                        if (lane == k - 32) v1 = divr(v1, dkk);
-                        xk = v1;
-                        if constexpr (Traits<T>::cplx) {
-                            xk.x = __shfl_sync(0xffffffffu, xk.x, k - 32);
-                            xk.y = __shfl_sync(0xffffffffu, xk.y, k - 32);
-                        } else xk = __shfl_sync(0xffffffffu, xk, k - 32);
-                        if (lane + 32 > k) v1 = fms(v1, Ls[k][lane + 32], xk);
-                    }
-                }
-            } else {
-                for (int k = nrows - 1; k >= 0; --k) {
-                    const R dkk = re(Ls[k][k]);
-                    T xk;
-                    // x_k = v_k / d_kk;  v_i -= conj(L(k, i)) x_k for i < k
-                    if (k < 32) {
-                        if (lane == k) v0 = divr(v0, dkk);
-                        xk = v0;
-                        if constexpr (Traits<T>::cplx) {
-                            xk.x = __shfl_sync(0xffffffffu, xk.x, k);
-                            xk.y = __shfl_sync(0xffffffffu, xk.y, k);
-                        } else xk = __shfl_sync(0xffffffffu, xk, k);
-                        if (lane < k) v0 = fms(v0, cj(Ls[lane][k]), xk);
-                    } else {
-                        if (lane == k - 32) v1 = divr(v1, dkk);
-                        xk = v1;
-                        if constexpr (Traits<T>::cplx) {
-                            xk.x = __shfl_sync(0xffffffffu, xk.x, k - 32);
-                            xk.y = __shfl_sync(0xffffffffu, xk.y, k - 32);
-                        } else xk = __shfl_sync(0xffffffffu, xk, k - 32);
-                        if (lane + 32 < k) v1 = fms(v1, cj(Ls[lane + 32][k]), xk);
-                        v0 = fms(v0, cj(Ls[lane][k]), xk);
+        const int ra = 2 * warp, rb = 2 * warp + 1;
+        T a0 = Acc[lane][ra], a1 = Acc[lane + 32][ra];
+        T b0 = Acc[lane][rb], b1 = Acc[lane + 32][rb];
+        if (fwd) {
+            for (int k = 0; k < nrows; ++k) {
+                const R rk = Rinv[k];
+                if (k < 32) {
+                    if (lane == k) { a0 = scal(a0, rk); b0 = scal(b0, rk); }
+                    const T xa = shfl_t(a0, k), xb = shfl_t(b0, k);
+                    const T l0 = lval(lane, k), l1 = lval(lane + 32, k);
+                    if (lane > k) { a0 = fms(a0, l0, xa); b0 = fms(b0, l0, xb); }
+                    a1 = fms(a1, l1, xa);
+                    b1 = fms(b1, l1, xb);
+                } else {
+                    if (lane == k - 32) { a1 = scal(a1, rk); b1 = scal(b1, rk); }
+                    const T xa = shfl_t(a1, k - 32), xb = shfl_t(b1, k - 32);
+                    if (lane + 32 > k) {
+                        const T l1 = lval(lane + 32, k);
+                        a1 = fms(a1, l1, xa);
+                        b1 = fms(b1, l1, xb);
                     }
                 }
             }
-            acc_s[lane][r] = v0;
-            acc_s[lane + 32][r] = v1;
+        } else {
+            // x_k = v_k / L_kk; v_i -= conj(L(k, i)) x_k for i < k
+            for (int k = nrows - 1; k >= 0; --k) {
+                const R rk = Rinv[k];
+                if (k < 32) {
+                    if (lane == k) { a0 = scal(a0, rk); b0 = scal(b0, rk); }
+                    const T xa = shfl_t(a0, k), xb = shfl_t(b0, k);
+                    if (lane < k) {
+                        const T l0 = lcval(k, lane);
+                        a0 = fms(a0, l0, xa);
+                        b0 = fms(b0, l0, xb);
+                    }
+                } else {
+                    if (lane == k - 32) { a1 = scal(a1, rk); b1 = scal(b1, rk); }
+                    const T xa = shfl_t(a1, k - 32), xb = shfl_t(b1, k - 32);
+                    const T l0 = lcval(k, lane);
+                    a0 = fms(a0, l0, xa);
+                    b0 = fms(b0, l0, xb);
+                    if (lane + 32 < k) {
+                        const T l1 = lcval(k, lane + 32);
+                        a1 = fms(a1, l1, xa);
+                        b1 = fms(b1, l1, xb);
+                    }
+                }
+            }
         }
+        Acc[lane][ra] = a0;
+        Acc[lane + 32][ra] = a1;
+        Acc[lane][rb] = b0;
+        Acc[lane + 32][rb] = b1;
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < RB * RC; idx += NT) {
         const int i = idx % RB, r = idx / RB;
-        if (i < nrows && r < nr) x_st<T, BT>(B, ldb, i0 + i, r0 + r, acc_s[i][r]);
+        if (i < nrows && r < nr) x_st<T, BT>(B, ldb, i0 + i, r0 + r, Acc[i][r]);
     }
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) st_release(&cflags[fwd ? blk : N + blk], 1);
 }
 
-template <class T, bool UP, bool BT>
-cudaError_t potrs_launch(const T* A, long long lda, T* B, long long ldb, int n, int nrhs, int* flags, int* ticket,
+template <class T, bool UP, bool BT, class TL = T>
+cudaError_t potrs_launch(const TL* A, long long lda, T* B, long long ldb, int n, int nrhs, int* flags, int* ticket,
                          int* status, cudaStream_t st)
 {
     const int N = (int)ceil_div(n, RB);
     const int nchunks = (int)ceil_div(nrhs, RC);
     const long long grid = 2LL * N * nchunks;
-    const size_t smem = sizeof(T) * ((size_t)RB * (RB + 1) + 2 * (size_t)RB * (RC + 1));
+    const size_t smem = potrs_smem_bytes<TL, T>();
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_potrs_fused<T, UP, BT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_potrs_fused<TL, T, UP, BT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
     const double cf = Traits<T>::cplx ? 4.0 : 1.0;
     const double nd = n, rd = nrhs;
-    ProfScope ps(PK_POTRS_FUSED, st, cf * 2.0 * nd * nd * rd, sizeof(T) * (nd * (nd + 1) + 4.0 * nd * rd));
-    k_potrs_fused<T, UP, BT><<<(unsigned)grid, NT, smem, st>>>(A, lda, B, ldb, n, nrhs, nchunks, flags, ticket,
-                                                                status);
+    ProfScope ps(PK_POTRS_FUSED, st, cf * 2.0 * nd * nd * rd,
+                 sizeof(TL) * nd * (nd + 1) + sizeof(T) * 4.0 * nd * rd);
+    k_potrs_fused<TL, T, UP, BT><<<(unsigned)grid, NT, smem, st>>>(A, lda, B, ldb, n, nrhs, nchunks, flags, ticket,
+                                                                    status);
     note_launches(1);
     return cudaGetLastError();
 }
@@ -243,8 +325,38 @@ cudaError_t potrs_typed(char uplo, char side, int n, int nrhs, const void* A, lo
     return potrs_launch<T, false, false>(a, lda, b, ldb, n, nrhs, flags, ticket, status, st);
 }
 
+cudaError_t potrs_dispatch(char type, char uplo, char side, int n, int nrhs, const void* A, long long lda, void* B,
+                           long long ldb, int* flags, int* ticket, int* status, cudaStream_t st)
+{
+    switch (type) {
+    case 's': return potrs_typed<float>(uplo, side, n, nrhs, A, lda, B, ldb, flags, ticket, status, st);
+    case 'd': return potrs_typed<double>(uplo, side, n, nrhs, A, lda, B, ldb, flags, ticket, status, st);
+    case 'c': return potrs_typed<cf32>(uplo, side, n, nrhs, A, lda, B, ldb, flags, ticket, status, st);
+    case 'z': return potrs_typed<cf64>(uplo, side, n, nrhs, A, lda, B, ldb, flags, ticket, status, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
 }  // namespace
 }  // namespace ddlak
+
+// Solve with an FP32 factor (uplo 'L') and FP64 right-hand sides in place
+// (the refinement solves of the mixed-precision path); same scratch as ddlak_potrs.
+extern "C" int ddlak_potrs_mixed(int n, int nrhs, const void* L32, long long ldl, void* B, long long ldb, void* work,
+                                 unsigned long long work_bytes, void* stream)
+{
+    using namespace ddlak;
+    if (n <= 0 || nrhs <= 0) return 0;
+    if (work_bytes < ddlak_potrs_workspace(n, nrhs)) return (int)cudaErrorInvalidValue;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(work, 0, ddlak_potrs_workspace(n, nrhs), st);
+    if (e != cudaSuccess) return (int)e;
+    int* status = static_cast<int*>(work);
+    int* flags = reinterpret_cast<int*>(static_cast<char*>(work) + 256);
+    return (int)potrs_launch<double, false, false, float>(static_cast<const float*>(L32), ldl,
+                                                          static_cast<double*>(B), ldb, n, nrhs, flags, status + 1,
+                                                          status, st);
+}
 
 // Scratch: [status int][ticket int] padded to 256 B, then nchunks * 2N flags.
 extern "C" unsigned long long ddlak_potrs_workspace(int n, int nrhs)
@@ -267,12 +379,5 @@ extern "C" int ddlak_potrs(char type, char uplo, char side, int n, int nrhs, con
     int* status = static_cast<int*>(work);
     int* ticket = status + 1;
     int* flags = reinterpret_cast<int*>(static_cast<char*>(work) + 256);
-    switch (type) {
-    case 's': e = potrs_typed<float>(uplo, side, n, nrhs, A, lda, B, ldb, flags, ticket, status, st); break;
-    case 'd': e = potrs_typed<double>(uplo, side, n, nrhs, A, lda, B, ldb, flags, ticket, status, st); break;
-    case 'c': e = potrs_typed<cf32>(uplo, side, n, nrhs, A, lda, B, ldb, flags, ticket, status, st); break;
-    case 'z': e = potrs_typed<cf64>(uplo, side, n, nrhs, A, lda, B, ldb, flags, ticket, status, st); break;
-    default: return (int)cudaErrorInvalidValue;
-    }
-    return (int)e;
+    return (int)potrs_dispatch(type, uplo, side, n, nrhs, A, lda, B, ldb, flags, ticket, status, st);
 }

@@ -374,7 +374,7 @@ def test_diag_logdet_cases(handle, golden, p):
             else:
                 assert abs(res[0] - e[0]) < tol * (1 + abs(e[0]))
                 assert abs(math.remainder(float(res[1]) - e[1], 2 * math.pi)) < tol
-            assert np.array_equal(dA.to_host(full_lld=True).view(np.uint8), host.view(np.uint8))
+            assert dA.to_host(full_lld=True).tobytes(order="F") == host.tobytes(order="F")
         k += 1
 
 
