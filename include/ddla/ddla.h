@@ -54,6 +54,14 @@ void potrf(const DdlaHandle_t& handle, char uplo, int n, T* A, int lda, int* inf
 template <typename T>
 void diag_logdet(const DdlaHandle_t& handle, int n, const T* A, int lda, std::complex<real_type_t<T>>& result);
 
+// ppotrs<double> that allocates nothing (no reference counterpart): for callers
+// that cannot allocate device memory while running.  The solve's flags live in
+// a fixed device array inside the library (n <= 65536, nrhs <= 256; larger
+// sizes throw std::invalid_argument).  The first call on a device should come
+// before any stream capture; overlapping calls race on the shared array.
+void ppotrs_noalloc(const DdlaHandle_t& handle, char side, char uplo, char trans, int n, int nrhs, const double* A,
+                    const int* descA, double* B, const int* descB);
+
 // Workspace split of the reference's check / size / run components
 // (src/Cholesky/cholesky_workspace.h:133-154, 207-222, 239-249; plan_util.h).
 // The *_workspace_size functions report device bytes; *_run performs the

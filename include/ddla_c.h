@@ -129,6 +129,20 @@ int ddla_c_ppotrs_workspace_size(void* handle, char side, int n, int nrhs, const
 int ddla_z_ppotrs_workspace_size(void* handle, char side, int n, int nrhs, const int* descA, const int* descB,
                                  long long* bytes);
 
+/* ddla_d_ppotrs without any allocation.  No counterpart in the reference: its
+ * ppotrs always allocates workspace per call.  This entry serves callers that
+ * must not allocate device memory once they run -- a serving loop that reserves
+ * its whole memory budget up front, or code whose CUDA allocator belongs to
+ * another framework -- by keeping the solve's few kilobytes of flags in a fixed
+ * device array inside the library (128 KB, present on every device that loads
+ * the library until the process exits).  Same arguments, checks and result as
+ * ddla_d_ppotrs, limited to n <= 65536 and nrhs <= 256 (larger sizes return
+ * status 6 with a message, before any device work).  The first call on a device
+ * looks the array up, so make it before any stream capture; calls that overlap
+ * on the GPU share the array and race. */
+int ddla_d_ppotrs_noalloc(void* handle, char side, char uplo, char trans, int n, int nrhs, const void* A,
+                          const int* descA, void* B, const int* descB);
+
 /* Mixed-precision solve (no reference counterpart; LAPACK dsposv semantics,
  * see ddla::pposv_mixed in include/ddla/ddla.h).  precision: 'B' BF16 or 'T'
  * TF32 tensor-core factor, 'D' plain FP64.  report (may be NULL) receives

@@ -38,6 +38,18 @@ unsigned long long ddlak_potrs_workspace(int n, int nrhs);
 int ddlak_potrs(char type, char uplo, char side, int n, int nrhs, const void* A, long long lda, void* B,
                 long long ldb, void* work, unsigned long long work_bytes, void* stream);
 
+/* ddlak_potrs with its scratch in a fixed device array owned by the library
+ * instead of caller memory: no allocation of any kind.  Limits (n <= 65536,
+ * nrhs <= 256) are reported by ddlak_potrs_fixed_scratch_limits; larger
+ * problems return cudaErrorInvalidValue before touching the device.  The first
+ * call on a device looks the array's device address up (with that device
+ * current), so it should come before any stream capture.  Every call shares the
+ * array: calls that overlap on the GPU race.  *status_word receives the device
+ * address of the status word (nonzero after the launch: a wait gave up). */
+int ddlak_potrs_fixed_scratch_limits(int* max_n, int* max_nrhs);
+int ddlak_potrs_fixed_scratch(char type, char uplo, char side, int n, int nrhs, const void* A, long long lda,
+                              void* B, long long ldb, int** status_word, void* stream);
+
 /* Bytes of device scratch ddlak_diag_logsum needs. */
 unsigned long long ddlak_logdet_workspace(void);
 

@@ -385,6 +385,16 @@ DDLA_C_TYPED(c, std::complex<float>)
 DDLA_C_TYPED(z, std::complex<double>)
 #undef DDLA_C_TYPED
 
+int ddla_d_ppotrs_noalloc(void* handle, char side, char uplo, char trans, int n, int nrhs, const void* A,
+                          const int* descA, void* B, const int* descB)
+{
+    return run(handle, [&](ddla::DdlaHandle_t h) -> int {
+        ddla::ppotrs_noalloc(h, side, uplo, trans, n, nrhs, static_cast<const double*>(A), descA,
+                             static_cast<double*>(B), descB);
+        return ST_SUCCESS;
+    });
+}
+
 int ddla_c_get_stream(void* handle, void** stream)
 {
     if (handle == nullptr) return ST_INVALID_HANDLE;

@@ -175,6 +175,25 @@ void pposv(const DdlaHandle_t& h, char side, char uplo, char trans, int n, int n
     detail::cuda_check(cudaStreamSynchronize(h->stream), "stream synchronisation");
 }
 
+// ppotrs with the solve's flags in the library's fixed device array: no
+// allocation.  For callers that cannot allocate device memory while running.
+void ppotrs_noalloc(const DdlaHandle_t& h, char side, char uplo, char trans, int n, int nrhs, const double* A,
+                    const int* da, double* B, const int* db)
+{
+    ppotrs_check(h, side, uplo, trans, n, nrhs, A, da, B, db);
+    if (n == 0 || nrhs == 0) return;
+    int max_n = 0, max_rhs = 0;
+    ddlak_potrs_fixed_scratch_limits(&max_n, &max_rhs);
+    if (n > max_n || nrhs > max_rhs)
+        throw std::invalid_argument("ppotrs_noalloc: the fixed scratch serves n <= " + std::to_string(max_n) +
+                                    " and nrhs <= " + std::to_string(max_rhs));
+    int* status = nullptr;
+    detail::kernel_check(ddlak_potrs_fixed_scratch('d', uplo, side, n, nrhs, A, da[DDLA_LLD_], B, db[DDLA_LLD_],
+                                                   &status, h->stream),
+                         "potrs kernel (fixed scratch)");
+    if (read_device_int(h, status) != 0) throw std::runtime_error("ppotrs_noalloc: a device wait timed out");
+}
+
 template <typename T>
 void potrf(const DdlaHandle_t& h, char uplo, int n, T* A, int lda, int* info)
 {

@@ -367,6 +367,76 @@ extern "C" unsigned long long ddlak_potrs_workspace(int n, int nrhs)
     return 256 + ((C * 2 * N * sizeof(int) + 255) / 256) * 256;
 }
 
+// ---------------------------------------------------------------------------
+// The same fused solve with its scratch in a fixed, library-owned device array
+// instead of memory the caller or the allocator provides.  The array lives
+// for the whole process on every device that loads the library (128 KB + 256 B),
+// which bounds the problem: n <= 65536 (1024 block rows of 64) and nrhs <= 256
+// (16 chunks of 16).  All calls share it, so calls that overlap on the GPU
+// race on it; the words that must start at zero are cleared on the caller's
+// stream before each launch.
+// ---------------------------------------------------------------------------
+namespace ddlak {
+namespace {
+constexpr int kFixedMaxN = 65536;
+constexpr int kFixedMaxRhs = 256;
+constexpr int kFixedHeaderInts = 64;  // status, ticket, padding to 256 bytes
+constexpr int kFixedFlagInts = 2 * (kFixedMaxN / RB) * (kFixedMaxRhs / RC);
+__device__ __align__(256) int g_potrs_fixed_scratch[kFixedHeaderInts + kFixedFlagInts];
+
+// Device address of the array on the current device; looked up once per
+// device (the first call on a device does the lookup, with that device current).
+int* fixed_scratch_ptr(int* err)
+{
+    static std::mutex mu;
+    static int* ptrs[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 64) {
+        *err = e != cudaSuccess ? (int)e : (int)cudaErrorInvalidDevice;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    if (ptrs[dev] == nullptr) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_potrs_fixed_scratch);
+        if (e != cudaSuccess) {
+            *err = (int)e;
+            return nullptr;
+        }
+        ptrs[dev] = static_cast<int*>(p);
+    }
+    *err = 0;
+    return ptrs[dev];
+}
+}  // namespace
+}  // namespace ddlak
+
+extern "C" int ddlak_potrs_fixed_scratch_limits(int* max_n, int* max_nrhs)
+{
+    if (max_n) *max_n = ddlak::kFixedMaxN;
+    if (max_nrhs) *max_nrhs = ddlak::kFixedMaxRhs;
+    return 0;
+}
+
+extern "C" int ddlak_potrs_fixed_scratch(char type, char uplo, char side, int n, int nrhs, const void* A,
+                                         long long lda, void* B, long long ldb, int** status_word, void* stream)
+{
+    using namespace ddlak;
+    if (n <= 0 || nrhs <= 0) return 0;
+    if (n > kFixedMaxN || nrhs > kFixedMaxRhs) return (int)cudaErrorInvalidValue;
+    int err = 0;
+    int* base = fixed_scratch_ptr(&err);
+    if (base == nullptr) return err;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t flag_ints = (size_t)2 * ceil_div(n, RB) * ceil_div(nrhs, RC);
+    cudaError_t e = cudaMemsetAsync(base, 0, (kFixedHeaderInts + flag_ints) * sizeof(int), st);
+    if (e != cudaSuccess) return (int)e;
+    if (status_word) *status_word = base;
+    return (int)potrs_dispatch(type, uplo, side, n, nrhs, A, lda, B, ldb, base + kFixedHeaderInts, base + 1, base,
+                               st);
+}
+
 extern "C" int ddlak_potrs(char type, char uplo, char side, int n, int nrhs, const void* A, long long lda, void* B,
                            long long ldb, void* work, unsigned long long work_bytes, void* stream)
 {
