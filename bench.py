@@ -1,32 +1,37 @@
 """Benchmark of the B200 Cholesky path: FP64-accurate pposv TFLOP/s at n=32768.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--n 32768] [--nrhs 8] [--kappa 1e6] [--precision auto|B|T|D]
+                    [--n 32768] [--nrhs 8] [--kappa 1e6] [--no-cpu] [--no-plain]
 
-Workload: ddla pposv (uplo 'L', side 'L') of a double n x n SPD matrix
-A = U diag(s) U^T (U = product of 4 Householder reflectors with N(0,1) vectors,
-s geometric from 1 to 1/kappa) with nrhs N(0,1) right-hand sides, to FP64
-accuracy.  One step = one pposv call.  TFLOP/s are counted on the FP64
-factor+solve count n^3/3 + 2 n^2 nrhs for every path (plain FP64 and
-mixed precision + refinement alike).  The 8.6 GB matrix is larger than the
-126 MB L2, so no L2 flush is needed between steps.
+Workload: solve A X = B to FP64 accuracy for a double n x n SPD matrix
+A = U diag(s) U^T (U = product of 4 Householder reflectors with N(0,1)
+vectors, s geometric from 1 to 1/kappa) and nrhs N(0,1) right-hand sides,
+uplo 'L'.  One step = one solve.  Two paths are timed:
+  mixed+IR : ddla_d_pposv_mixed (tensor-core BF16 or TF32 factor, FP64
+             refinement / GMRES-IR, ?sposv stopping test) -- the headline value
+             is the faster of the two precisions;
+  plain    : ddla_d_pposv (FP64 factor on the FP64 tensor cores + fused solve).
+TFLOP/s use the FP64 factor+solve count n^3/3 + 2 n^2 nrhs for both paths.
+The 8.6 GB matrix is larger than the 126 MB L2, so no L2 flush is needed.
 
-Device timing: CUDA events on the library handle's stream around each pposv
-call; A is restored from a pristine copy between steps outside the events
-(the plain path overwrites A with its factor).  The timed loop is bracketed by
-a barrier and a device synchronize on both sides; the max over ranks is taken.
-With --gpus N > 1 every rank solves its own independent system (replicas:
-a single pposv on a 1x1 grid does not shard), so scaling is weak.
+Device timing: CUDA events on the library handle's stream around each call,
+summed over the K steps; the plain path restores A from a pristine copy
+outside the events (it overwrites A with its factor; the mixed path leaves A
+unchanged).  The timed loop is bracketed by a barrier and a device
+synchronize on both sides; the max over ranks is taken.  With --gpus N > 1
+every rank solves its own system (replicas: one pposv on a 1x1 grid does not
+shard), so scaling is weak.
 
-e2e: the same pposv through the public C ABI with host buffers -- the H2D copy
-of A and B from pinned memory, the solve and the D2H copy of X, all inside
-the events.  The reference arm (--impl reference) times the reference's own
-CPU implementation of the path (LAPACK dpotrf + two dtrsm, the calls its CPU
-handle makes) on the host cores over a bounded sample of the same workload.
+e2e: the headline path through the public C ABI with host buffers -- the H2D
+copy of A and B from pinned memory, the solve and the D2H copy of X, inside the
+events.  The reference arm (--impl reference) times the reference's own CPU
+implementation of the path (LAPACK dpotrf + two dtrsm, the calls its CPU handle
+makes) on the host cores over a bounded sample of the same workload.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -43,6 +48,8 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "pposv TFLOP/s n=32768 at FP64 accuracy (plain vs mixed+IR)"
 UNIT = "TFLOP/s"
+KIND = {"potrf_diag": 0, "trsm_panel": 1, "syrk_update": 2, "potrs_fused": 3, "logdet": 4, "mixed_update": 5,
+        "mixed_other": 6, "symm_residual": 7}
 
 
 def flops_pposv(n: int, nrhs: int) -> float:
@@ -51,6 +58,17 @@ def flops_pposv(n: int, nrhs: int) -> float:
 
 def measured_peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            pass
+    return {}
+
+
+def traffic_summary() -> dict:
+    """Per-launch DRAM traffic of the dominant kernels from the committed ncu summary (profiles/)."""
+    p = ROOT / "profiles" / "dram_traffic.json"
     if p.exists():
         try:
             return json.loads(p.read_text())
@@ -190,9 +208,17 @@ def fp64_peak_tflops(torch, device) -> float:
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def run_ours(args, rank: int, world: int, local_rank: int):
-    import ctypes
+def read_kernels(C):
+    out = {}
+    for name, kind in KIND.items():
+        ms, cnt, fl, by = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_double(), ctypes.c_double()
+        C.ddla_c_profile_read(kind, ctypes.byref(ms), ctypes.byref(cnt), ctypes.byref(fl), ctypes.byref(by), 1)
+        if cnt.value:
+            out[name] = {"ms": ms.value, "launches": cnt.value, "flops": fl.value, "bytes": by.value}
+    return out
 
+
+def run_ours(args, rank: int, world: int, local_rank: int):
     import torch
 
     from libddla_b200 import ddla
@@ -207,87 +233,127 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     C.check_status(C.ddla_c_get_stream(h.ptr, ctypes.byref(sp)), "get_stream")
     stream = torch.cuda.ExternalStream(sp.value, device=device)
 
-    A0 = householder_spd(n, args.kappa, 0xDD1A0003 + rank, device=device)
+    A0 = householder_spd(n, args.kappa, 0xDD1A0003 + rank, device=device)  # symmetric: row-major == column-major
+    Apristine = A0.clone()
     gB = torch.Generator(device=device).manual_seed(0xDD1A0103 + rank)
     B0 = torch.randn(nrhs, n, generator=gB, device=device, dtype=torch.float64)  # column-major n x nrhs
-    A = torch.empty_like(A0)
     X = torch.empty_like(B0)
     torch.cuda.synchronize()
-    dA = ddla.DistributedMatrix.wrap(h, A.data_ptr(), n, n, n, np.float64, mb=256, nb=256)
-    dB = ddla.DistributedMatrix.wrap(h, X.data_ptr(), n, nrhs, n, np.float64, mb=256, nb=256)
-    A0_col = A0  # symmetric: row-major storage of A0 is its column-major transpose, equal to itself
+    desc = lambda ptr, rows, cols: ddla.DistributedMatrix.wrap(h, ptr, rows, cols, n, np.float64, mb=256, nb=256)
+    dA0 = desc(A0.data_ptr(), n, n)
+    dB0 = desc(B0.data_ptr(), n, nrhs)
+    dX = desc(X.data_ptr(), n, nrhs)
+    rep_arr = (ctypes.c_double * 4)()
 
-    def restore():
-        with torch.cuda.stream(stream):
-            A.copy_(A0_col)
-            X.copy_(B0)
+    def mixed_solve(prec):
+        info = ctypes.c_int(0)
+        C.check_status(C.ddla_d_pposv_mixed(h.ptr, b"L", prec.encode(), n, nrhs, dA0.data_ptr, dA0.desc.ctypes.data,
+                                            dB0.data_ptr, dB0.desc.ctypes.data, dX.data_ptr, dX.desc.ctypes.data,
+                                            ctypes.byref(info), rep_arr), "pposv_mixed")
+        return info.value, {"iter": int(rep_arr[0]), "gmres": int(rep_arr[1]), "shift": rep_arr[2],
+                            "backward_error": rep_arr[3]}
 
-    def solve():
-        _, info = ddla.pposv(dA, dB, "L")
-        return info
+    def backward_error(Xt) -> float:
+        R = B0.T - A0 @ Xt.T
+        an = A0.abs().sum(dim=0).max()
+        return float((R.abs().max(dim=0).values / (an * Xt.T.abs().max(dim=0).values)).max())
 
-    def backward_error() -> float:
-        # ||b - A x||_inf / (||A||_inf ||x||_inf), A symmetric in A0
-        R = B0.T - A0 @ X.T
-        an = A0.abs().sum(dim=1).max()
-        return float((R.abs().max(dim=0).values / (an * X.T.abs().max(dim=0).values)).max())
+    def timed(fn, pre=None):
+        """W warm-up + K device-timed calls; returns (total ms, per-step results, kernels, launches, clocks)."""
+        for _ in range(args.warmup):
+            if pre:
+                pre()
+            fn()
+        torch.cuda.synchronize()
+        launches0 = C.ddla_c_launch_count()
+        C.ddla_c_profile_read(-1, None, None, None, None, 1)
+        C.ddla_c_profile_enable(1)
+        times, res = [], []
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            for _ in range(args.steps):
+                if pre:
+                    pre()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                res.append(fn())
+                e1.record(stream)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        C.ddla_c_profile_enable(0)
+        launches = C.ddla_c_launch_count() - launches0
+        total = torch.tensor([sum(times)], device=device, dtype=torch.float64)
+        if world > 1:
+            torch.distributed.all_reduce(total, op=torch.distributed.ReduceOp.MAX)
+        return float(total.item()), res, read_kernels(C), launches, clk.summary()
 
-    for _ in range(args.warmup):
-        restore()
-        info = solve()
-        assert info == 0, info
-    torch.cuda.synchronize()
-    bwd = backward_error()
+    tf = lambda total_ms: world * flops_pposv(n, nrhs) * args.steps / (total_ms * 1e-3) / 1e12
 
-    launches0 = C.ddla_c_launch_count()
-    C.ddla_c_profile_read(-1, None, None, None, None, 1)
-    C.ddla_c_profile_enable(1)
-    times = []
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(torch.cuda.current_device()) as clk:
-        for _ in range(args.steps):
-            restore()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            info = solve()
-            e1.record(stream)
-            e1.synchronize()
-            times.append(e0.elapsed_time(e1))
-    torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    C.ddla_c_profile_enable(0)
-    launches = C.ddla_c_launch_count() - launches0
-    total_ms = sum(times)
-    t = torch.tensor([total_ms], device=device, dtype=torch.float64)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    total_ms = float(t.item())
-    ms_step = total_ms / args.steps
-    value = world * flops_pposv(n, nrhs) * args.steps / (total_ms * 1e-3) / 1e12
+    # ---- mixed precision + refinement (headline) ----
+    mixed = {}
+    for prec in ("B", "T"):
+        fell_back = [False]
 
-    kern = {}
-    for kind, name in ((2, "syrk_update"), (0, "potrf_diag"), (1, "trsm_panel"), (3, "potrs_fused")):
-        ms, cnt, fl, by = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_double(), ctypes.c_double()
-        C.ddla_c_profile_read(kind, ctypes.byref(ms), ctypes.byref(cnt), ctypes.byref(fl), ctypes.byref(by), 1)
-        kern[name] = {"ms": ms.value, "launches": cnt.value, "flops": fl.value, "bytes": by.value}
+        def solve_and_note(prec=prec):
+            r = mixed_solve(prec)
+            fell_back[0] = r[1]["iter"] < 0  # the FP64 fallback overwrote A with its factor
+            return r
 
-    # e2e through the public API with host buffers
+        def restore_if_needed():
+            if fell_back[0]:
+                with torch.cuda.stream(stream):
+                    A0.copy_(Apristine)
+                fell_back[0] = False
+
+        total, res, kern, launches, clocks = timed(solve_and_note, pre=restore_if_needed)
+        restore_if_needed()
+        info, rep = res[-1]
+        assert info == 0, (prec, info)
+        mixed[prec] = {"value": tf(total), "ms_per_step": total / args.steps, "report": rep,
+                       "backward_error": backward_error(X), "kernels": kern, "launches": launches, "clocks": clocks}
+    best = max(mixed, key=lambda p: mixed[p]["value"] if mixed[p]["report"]["iter"] >= 0 else -1)
+    head = mixed[best]
+
+    # ---- plain FP64 ----
+    plain = None
+    if not args.no_plain:
+        A = torch.empty_like(A0)
+        dA = desc(A.data_ptr(), n, n)
+
+        def restore():
+            with torch.cuda.stream(stream):
+                A.copy_(A0)
+                X.copy_(B0)
+
+        def plain_solve():
+            _, info = ddla.pposv(dA, dX, "L")
+            return info
+
+        total, res, kern, launches, clocks = timed(plain_solve, pre=restore)
+        assert all(r == 0 for r in res)
+        plain = {"value": tf(total), "ms_per_step": total / args.steps, "backward_error": backward_error(X),
+                 "kernels": kern, "launches": launches}
+        del A
+
+    # ---- e2e through the public API with host buffers (headline path) ----
     Ah = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
     Ah.copy_(A0)
     Bh = torch.empty((nrhs, n), dtype=torch.float64, pin_memory=True)
     Bh.copy_(B0)
-    Xh = torch.empty_like(Bh).pin_memory()
+    Xh = torch.empty((nrhs, n), dtype=torch.float64, pin_memory=True)
     e2e_ms = []
-    for _ in range(max(1, min(2, args.steps))):
+    for _ in range(max(1, min(3, args.steps))):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        C.check_status(C.ddla_c_memcpy(h.ptr, A.data_ptr(), Ah.data_ptr(), Ah.numel() * 8), "h2d A")
-        C.check_status(C.ddla_c_memcpy(h.ptr, X.data_ptr(), Bh.data_ptr(), Bh.numel() * 8), "h2d B")
-        info = solve()
+        C.check_status(C.ddla_c_memcpy(h.ptr, A0.data_ptr(), Ah.data_ptr(), Ah.numel() * 8), "h2d A")
+        C.check_status(C.ddla_c_memcpy(h.ptr, B0.data_ptr(), Bh.data_ptr(), Bh.numel() * 8), "h2d B")
+        info, _ = mixed_solve(best)
         C.check_status(C.ddla_c_memcpy(h.ptr, Xh.data_ptr(), X.data_ptr(), X.numel() * 8), "d2h X")
         h.synchronize()
         e1.record(stream)
@@ -296,33 +362,47 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     e2e_value = world * flops_pposv(n, nrhs) / (statistics.median(e2e_ms) * 1e-3) / 1e12
 
     peaks = measured_peaks()
-    fp64_peak = fp64_peak_tflops(torch, device)
-    dom = kern["syrk_update"]
-    achieved = dom["flops"] / (dom["ms"] * 1e-3) / 1e12 if dom["ms"] > 0 else None
-
+    traffic = traffic_summary()
+    dom = head["kernels"].get("mixed_update", {})
+    gbs = dom["bytes"] / (dom["ms"] * 1e-3) / 1e9 if dom.get("ms") else None
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    roof = {"bound": "hbm", "kernel": "k_mixed_update (tcgen05 trailing update, FP32 W read-modify-write)",
+            "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm if gbs else None,
+            "traffic": traffic.get("k_mixed_update", {}).get("bytes_per_launch_at_bench"),
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks.get("hbm_gbs") else "fallback 6650 GB/s",
+            "launches": dom.get("launches"), "avg_launch_ms": (dom["ms"] / dom["launches"]) if dom.get("launches") else None}
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"pposv d uplo=L n={n} nrhs={nrhs} A=U diag(s) U^T kappa={args.kappa:g}",
-                   "path": "plain FP64 (blocked potrf: smem diag + warp panel trsm + DMMA syrk; fused trsv)",
+                   "path": f"mixed+IR precision {best} (tcgen05 {'BF16' if best == 'B' else 'TF32'} factor, "
+                           f"FP64 refinement)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU 1x1 grid",
-                   "l2": "inputs 8.6 GB > 126 MB L2, no flush", "backward_error": bwd},
-        "roofline": {"bound": "tensor", "kernel": "k_syrk_dmma (FP64 DMMA trailing update)",
-                     "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                     "frac": (achieved / fp64_peak) if achieved else None, "traffic": None,
-                     "peak_source": "cuBLAS DGEMM 8192^3 best-of-5 measured in this run (FP64 absent from MEASURED_PEAKS.json)"},
-        "kernels": kern,
+                   "l2": "inputs 8.6 GB > 126 MB L2, no flush", "report": head["report"],
+                   "backward_error": head["backward_error"]},
+        "roofline": roof,
+        "mixed": {p: {k: v for k, v in d.items() if k != "kernels"} for p, d in mixed.items()},
+        "plain": None if plain is None else {k: v for k, v in plain.items() if k != "kernels"},
+        "kernels": head["kernels"],
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": (Ah.numel() + Bh.numel()) * 8,
                 "d2h_bytes_per_step": Xh.numel() * 8, "ms_per_step": statistics.median(e2e_ms)},
-        "gpu_launches": int(launches),
-        "clocks": clk.summary(),
-        "peaks_file": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained")},
+        "gpu_launches": int(head["launches"]),
+        "clocks": head["clocks"],
     }
+    if plain is not None:
+        dm = plain["kernels"].get("syrk_update", {})
+        ach = dm["flops"] / (dm["ms"] * 1e-3) / 1e12 if dm.get("ms") else None
+        fp64 = fp64_peak_tflops(torch, device)
+        line["roofline_plain"] = {"bound": "tensor", "kernel": "k_syrk_dmma (FP64 DMMA trailing update)",
+                                  "achieved": ach, "peak": fp64, "unit": "TFLOP/s", "frac": ach / fp64 if ach else None,
+                                  "traffic": traffic.get("k_syrk_dmma", {}).get("bytes_per_launch_at_bench"),
+                                  "peak_source": "cuBLAS DGEMM 8192^3 best-of-5 measured in this run"}
+        line["speedup_mixed_over_plain"] = head["value"] / plain["value"]
     if rank == 0 and world == 1 and not args.no_cpu:
-        tf, sample, info = cpu_sample(budget_s=12.0, nrhs=nrhs, kappa=args.kappa)
-        line["cpu_baseline"] = {"value": tf, "unit": UNIT, "cores": int(info.get("threads") or os.cpu_count()),
-                                "kind": "port", "sample": sample}
+        cpu_tf, sample, info = cpu_sample(budget_s=12.0, nrhs=nrhs, kappa=args.kappa)
+        line["cpu_baseline"] = {"value": cpu_tf, "unit": UNIT,
+                                "cores": int(info.get("threads") or os.cpu_count()), "kind": "port", "sample": sample}
     if rank == 0:
         print(json.dumps(line), flush=True)
     h.destroy()
@@ -338,6 +418,7 @@ def main(argv=None):
     ap.add_argument("--nrhs", type=int, default=8)
     ap.add_argument("--kappa", type=float, default=1e6)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
     args = ap.parse_args(argv)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

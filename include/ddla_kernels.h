@@ -76,10 +76,16 @@ int ddlak_convert_lower(int n, const void* A, long long lda, void* W, long long 
 int ddlak_potrf_mixed(char precision, int n, void* W, long long ldw, void* P0, void* P1, int* dinfo, int* status,
                       void* stream);
 
+/* Inverses (FP64) of the 64 x 64 diagonal blocks of an FP32 factor (lower):
+ * ddlak_inv_diag_bytes(n) bytes, one column-major block per block row. */
+unsigned long long ddlak_inv_diag_bytes(int n);
+int ddlak_inv_diag_blocks(int n, const void* L32, long long ldl, void* Dinv, void* stream);
+
 /* In-place solve L L^T X = B with an FP32 factor (lower, ldl) and FP64 B;
- * scratch as ddlak_potrs_workspace(n, nrhs). */
-int ddlak_potrs_mixed(int n, int nrhs, const void* L32, long long ldl, void* B, long long ldb, void* work,
-                      unsigned long long work_bytes, void* stream);
+ * scratch as ddlak_potrs_workspace(n, nrhs).  Dinv (may be NULL) holds the
+ * inverted diagonal blocks; with it the diagonal steps are products. */
+int ddlak_potrs_mixed(int n, int nrhs, const void* L32, long long ldl, const void* Dinv, void* B, long long ldb,
+                      void* work, unsigned long long work_bytes, void* stream);
 
 /* R = B - A X, A symmetric FP64 stored in its lower triangle; deterministic. */
 int ddlak_symm_residual(int n, int nrhs, const void* A, long long lda, const void* X, long long ldx, const void* B,

@@ -22,7 +22,7 @@ public:
     static std::size_t workspace_bytes(int n, int nrhs, int m);
 
     GmresIR(const DdlaHandle_t& h, int n, int nrhs, const double* A, long long lda, const float* L32, long long ldl,
-            void* solve_work, std::size_t solve_bytes, void* work, int m);
+            const double* Dinv, void* solve_work, std::size_t solve_bytes, void* work, int m);
 
     // D = approximately A^-1 R (both n x nrhs, ld = n).  Runs at most maxit
     // Arnoldi steps, stopping early when every column's preconditioned
@@ -36,6 +36,7 @@ private:
     long long lda_;
     const float* L_;
     long long ldl_;
+    const double* Dinv_;  // inverted diagonal blocks of L_ (ddlak_inv_diag_blocks)
     void* swork_;
     std::size_t sbytes_;
     double* V_;      // (m+1) blocks of n x nrhs

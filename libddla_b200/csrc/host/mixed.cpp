@@ -92,7 +92,8 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
                               3 * detail::padded_bytes<double>((std::size_t)n * std::max(1, nrhs)) +
                               detail::padded_bytes<double>(n) + detail::padded_bytes<Scalars>(1) +
                               2 * detail::padded_bytes<double>(std::max(1, nrhs)) + sbytes +
-                              GmresIR::workspace_bytes(n, std::max(1, nrhs), kry);
+                              GmresIR::workspace_bytes(n, std::max(1, nrhs), kry) +
+                              (std::size_t)ddlak_inv_diag_bytes(n) + 256;
     detail::DeviceScratch ws(h, bytes);
     char* w = ws.data();
     float* W = detail::take<float>(w, (std::size_t)ldw * n);
@@ -104,6 +105,7 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
     double* D = detail::take<double>(w, (std::size_t)n * std::max(1, nrhs));
     double* Bc = detail::take<double>(w, (std::size_t)n * std::max(1, nrhs));
     double* colsum = detail::take<double>(w, n);
+    double* Dinv = detail::take<double>(w, ddlak_inv_diag_bytes(n) / sizeof(double));
     Scalars* sc = detail::take<Scalars>(w, 1);
     double* xn = detail::take<double>(w, std::max(1, nrhs));
     double* rn = detail::take<double>(w, std::max(1, nrhs));
@@ -147,7 +149,8 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
     detail::cuda_check(cudaMemcpy2DAsync(X, ldx * sizeof(double), Bc, n * sizeof(double), n * sizeof(double), nrhs,
                                          cudaMemcpyDeviceToDevice, st),
                        "copy B to X");
-    ck(ddlak_potrs_mixed(n, nrhs, W, ldw, X, ldx, swork, sbytes, st), "initial solve");
+    ck(ddlak_inv_diag_blocks(n, W, ldw, Dinv, st), "diagonal block inverses");
+    ck(ddlak_potrs_mixed(n, nrhs, W, ldw, Dinv, X, ldx, swork, sbytes, st), "initial solve");
 
     std::vector<double> hx(nrhs), hr(nrhs);
     auto residual_check = [&](double& worst) -> bool {
@@ -171,7 +174,7 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
     double worst = 0, prev = INFINITY;
     int sweeps = 0;
     bool use_gmres = false;
-    GmresIR gmres(h, n, nrhs, A, lda, W, ldw, swork, sbytes, gwork, kry);
+    GmresIR gmres(h, n, nrhs, A, lda, W, ldw, Dinv, swork, sbytes, gwork, kry);
     while (true) {
         const bool ok = residual_check(worst);
         rep.backward_error = worst;
@@ -191,7 +194,7 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
         } else {
             detail::cuda_check(cudaMemcpyAsync(D, R, sizeof(double) * n * nrhs, cudaMemcpyDeviceToDevice, st),
                                "copy residual");
-            ck(ddlak_potrs_mixed(n, nrhs, W, ldw, D, n, swork, sbytes, st), "correction solve");
+            ck(ddlak_potrs_mixed(n, nrhs, W, ldw, Dinv, D, n, swork, sbytes, st), "correction solve");
             ++sweeps;
         }
         ck(ddlak_axpy(n, nrhs, 1.0, D, n, X, ldx, st), "update x");

@@ -130,6 +130,9 @@ __device__ __forceinline__ void st_release(int* p, int v)
 __device__ __forceinline__ bool bounded_wait_geq(const int* flag, int want, int* status)
 {
     if (ld_acquire(flag) >= want) return true;
+    // a short tight spin first: the producer is usually microseconds away
+    for (int it = 0; it < 4096; ++it)
+        if (ld_acquire(flag) >= want) return true;
     const long long t0 = clock64();
     unsigned ns = 32;
     while (true) {

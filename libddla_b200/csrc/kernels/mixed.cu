@@ -262,38 +262,37 @@ __global__ void __launch_bounds__(128, 2) k_mixed_update(const __grid_constant__
 
 // ---------------------------------------------------------------------------
 // R = B - A X for symmetric A stored in its lower triangle (FP64), up to 16
-// right-hand sides per chunk (grid.y).  CTA I owns the 64-row block I and
-// reads the row strip A(I, 0..I) and the column strip A(I+1.., I) (the latter
-// transposed), so there are no atomics and the result is deterministic.
+// right-hand sides per chunk (grid.z).  Block row I of the result needs the
+// row strip A(I, 0..I) and the column strip A(I+1.., I) (used transposed); the
+// strip is split over grid.y CTAs that stream their tiles through a 3-stage
+// cp.async ring and fold their partial sums into R with atomics (R holds B on
+// entry), so small n still fills every SM.
 // ---------------------------------------------------------------------------
 constexpr int SR = 64;
+constexpr int SR_STAGES = 3;
 __global__ void __launch_bounds__(256) k_symm_residual(const double* __restrict__ A, long long lda, int n, int nrhs,
                                                        const double* __restrict__ X, long long ldx,
-                                                       const double* __restrict__ B, long long ldb,
-                                                       double* __restrict__ R, long long ldr)
+                                                       double* __restrict__ R, long long ldr, int per_split)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double (*Tb)[SR][SR + 1] = reinterpret_cast<double (*)[SR][SR + 1]>(smem_raw);  // 2 tile buffers, raw [col][row]
-    double (*Xs)[17] = reinterpret_cast<double (*)[17]>(smem_raw + sizeof(double) * 2 * SR * (SR + 1));
+    double (*Tb)[SR][SR + 1] = reinterpret_cast<double (*)[SR][SR + 1]>(smem_raw);  // raw tiles [col][row]
+    double (*Xs)[17] = reinterpret_cast<double (*)[17]>(smem_raw + sizeof(double) * SR_STAGES * SR * (SR + 1));
     const int I = blockIdx.x;
     const int N = (int)ceil_div(n, SR);
+    const int vbeg = blockIdx.y * per_split;
+    const int vend = (vbeg + per_split) < N ? (vbeg + per_split) : N;
+    if (vbeg >= vend) return;
     const long long i0 = (long long)I * SR;
     const int nrows = (int)((n - i0) < SR ? (n - i0) : SR);
-    const int r0 = blockIdx.y * 16;
+    const int r0 = blockIdx.z * 16;
     const int nr = nrhs - r0 < 16 ? nrhs - r0 : 16;
     const int tr = threadIdx.x & 63, tg = threadIdx.x >> 6;
-    double acc[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int r = tg + 4 * q;
-        acc[q] = (tr < nrows && r < nr) ? B[(i0 + tr) + (r0 + r) * ldb] : 0.0;
-    }
-    // visit v = 0..N-1: J = v; for v <= I the row-strip tile A(I, J) (raw rows of I, cols of J),
-    // for v > I the column-strip tile A(J, I) (raw rows of J, cols of I), used transposed.
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    // visit v: for v <= I the row-strip tile A(I, v) (raw rows of I, cols of v),
+    // for v > I the column-strip tile A(v, I) (raw rows of v, cols of I), used transposed
     auto issue = [&](int v, int buf) {
-        const int J = v;
-        const long long rr = v <= I ? i0 : (long long)J * SR;  // first raw row
-        const long long cc = v <= I ? (long long)J * SR : i0;  // first raw col
+        const long long rr = v <= I ? i0 : (long long)v * SR;
+        const long long cc = v <= I ? (long long)v * SR : i0;
         const int nrr = (int)((n - rr) < SR ? (n - rr) : SR);
         const int ncc = (int)((n - cc) < SR ? (n - cc) : SR);
         for (int idx = threadIdx.x; idx < SR * SR; idx += blockDim.x) {
@@ -302,10 +301,15 @@ __global__ void __launch_bounds__(256) k_symm_residual(const double* __restrict_
             cp_async_elem<8>(&Tb[buf][ccol][rrow], valid ? A + (rr + rrow) + (cc + ccol) * lda : A, valid);
         }
     };
-    issue(0, 0);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    for (int v = 0; v < N; ++v) {
-        if (v + 1 < N) issue(v + 1, (v + 1) & 1);
+#pragma unroll
+    for (int s = 0; s < SR_STAGES - 1; ++s) {
+        if (vbeg + s < vend) issue(vbeg + s, s);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    for (int v = vbeg; v < vend; ++v) {
+        const int slot = (v - vbeg) % SR_STAGES;
+        const int pre = v + SR_STAGES - 1;
+        if (pre < vend) issue(pre, (pre - vbeg) % SR_STAGES);
         asm volatile("cp.async.commit_group;" ::: "memory");
         const long long j0 = (long long)v * SR;
         const int ncols = (int)((n - j0) < SR ? (n - j0) : SR);
@@ -313,15 +317,15 @@ __global__ void __launch_bounds__(256) k_symm_residual(const double* __restrict_
             const int k = idx % SR, r = idx / SR;
             Xs[k][r] = (k < ncols && r < nr) ? X[(j0 + k) + (r0 + r) * ldx] : 0.0;
         }
-        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        asm volatile("cp.async.wait_group %0;" ::"n"(SR_STAGES - 1) : "memory");
         __syncthreads();
-        const double (*Tt)[SR + 1] = Tb[v & 1];
+        const double (*Tt)[SR + 1] = Tb[slot];
         if (v < I) {
 #pragma unroll 8
             for (int k = 0; k < SR; ++k) {
                 const double a = Tt[k][tr];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) acc[q] = fma(-a, Xs[k][tg + 4 * q], acc[q]);
+                for (int q = 0; q < 4; ++q) acc[q] = fma(a, Xs[k][tg + 4 * q], acc[q]);
             }
         } else if (v == I) {
             // symmetric diagonal tile from its lower half: A(tr, k) = T[k][tr] (tr >= k) or T[tr][k]
@@ -329,14 +333,14 @@ __global__ void __launch_bounds__(256) k_symm_residual(const double* __restrict_
             for (int k = 0; k < SR; ++k) {
                 const double a = tr >= k ? Tt[k][tr] : Tt[tr][k];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) acc[q] = fma(-a, Xs[k][tg + 4 * q], acc[q]);
+                for (int q = 0; q < 4; ++q) acc[q] = fma(a, Xs[k][tg + 4 * q], acc[q]);
             }
         } else {
 #pragma unroll 8
             for (int k = 0; k < SR; ++k) {
-                const double a = Tt[tr][k];  // A(J-row k, I-col tr)
+                const double a = Tt[tr][k];  // A(row k of block v, col tr of block I)
 #pragma unroll
-                for (int q = 0; q < 4; ++q) acc[q] = fma(-a, Xs[k][tg + 4 * q], acc[q]);
+                for (int q = 0; q < 4; ++q) acc[q] = fma(a, Xs[k][tg + 4 * q], acc[q]);
             }
         }
         __syncthreads();
@@ -345,7 +349,7 @@ __global__ void __launch_bounds__(256) k_symm_residual(const double* __restrict_
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int r = tg + 4 * q;
-        if (tr < nrows && r < nr) R[(i0 + tr) + (r0 + r) * ldr] = acc[q];
+        if (tr < nrows && r < nr) atomicAdd(&R[(i0 + tr) + (r0 + r) * ldr], -acc[q]);
     }
 }
 
@@ -634,17 +638,26 @@ extern "C" int ddlak_symm_residual(int n, int nrhs, const void* A, long long lda
     using namespace ddlak;
     if (n <= 0 || nrhs <= 0) return 0;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const size_t smem = sizeof(double) * (2 * SR * (SR + 1) + SR * 17);
+    if (R != B) {
+        const cudaError_t e = cudaMemcpy2DAsync(R, ldr * sizeof(double), B, ldb * sizeof(double), n * sizeof(double),
+                                                nrhs, cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return (int)e;
+    }
+    const size_t smem = sizeof(double) * (SR_STAGES * SR * (SR + 1) + SR * 17);
     static std::once_flag once;
     std::call_once(once, [&] {
         cudaFuncSetAttribute(k_symm_residual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     });
-    dim3 grid((unsigned)ceil_div(n, SR), (unsigned)ceil_div(nrhs, 16));
+    const int N = (int)ceil_div(n, SR);
+    int nsplit = (int)ceil_div(4 * 148, N);
+    nsplit = nsplit < 1 ? 1 : (nsplit > N ? N : nsplit);
+    const int per = (int)ceil_div(N, nsplit);
+    nsplit = (int)ceil_div(N, per);
+    dim3 grid((unsigned)N, (unsigned)nsplit, (unsigned)ceil_div(nrhs, 16));
     {
-        ProfScope ps(PK_SYMM_RESIDUAL, st, 2.0 * (double)n * n * nrhs, 8.0 * (double)n * (n + 1) / 2 * 2);
+        ProfScope ps(PK_SYMM_RESIDUAL, st, 2.0 * (double)n * n * nrhs, 8.0 * (double)n * (n + 1));
         k_symm_residual<<<grid, 256, smem, st>>>(static_cast<const double*>(A), lda, n, nrhs,
-                                                 static_cast<const double*>(X), ldx, static_cast<const double*>(B),
-                                                 ldb, static_cast<double*>(R), ldr);
+                                                 static_cast<const double*>(X), ldx, static_cast<double*>(R), ldr, per);
     }
     note_launches(1);
     return (int)cudaGetLastError();

@@ -76,12 +76,14 @@ __device__ __forceinline__ T shfl_t(T v, int src)
 //   Xs[RB][RC+1]       the solved block of the other block row
 //   Acc[RB][RC+1]      this block row's right-hand sides
 //   Rinv[RB]           reciprocal pivots (real type)
+//   Ibuf[RB][RB+1]     (INV mode) the precomputed inverse of the diagonal block
 // The factor is stored as TL and the right-hand sides as TX (TL == TX on the
 // plain path; an FP32 factor with FP64 vectors for the mixed-precision solves).
-template <class TL, class TX>
+template <class TL, class TX, bool INV = false>
 __host__ __device__ constexpr size_t potrs_smem_bytes()
 {
-    return sizeof(TL) * 2 * (size_t)RB * (RB + 1) + sizeof(TX) * 2 * (size_t)RB * (RC + 1) + sizeof(real_t<TX>) * RB;
+    return sizeof(TL) * 2 * (size_t)RB * (RB + 1) + sizeof(TX) * 2 * (size_t)RB * (RC + 1) + sizeof(real_t<TX>) * RB +
+           (INV ? sizeof(TX) * (size_t)RB * (RB + 1) + 16 : 0);
 }
 
 template <class TX, class TL>
@@ -91,15 +93,20 @@ __device__ __forceinline__ TX widen(TL v)
     else return static_cast<TX>(v);
 }
 
-template <class TL, class TX, bool UP, bool BT>
+// INV: the diagonal step multiplies by Dinv (TX, one RB x RB column-major block per
+// block row, entries (r, c) of inv(L_bb), zero outside the block) instead of
+// substituting; for the repeated solves of the refinement with one factor.
+template <class TL, class TX, bool UP, bool BT, bool INV = false>
 __global__ void __launch_bounds__(NT) k_potrs_fused(const TL* __restrict__ A, long long lda, TX* B, long long ldb,
                                                     int n, int nrhs, int nchunks, int* flags, int* ticket,
-                                                    int* status)
+                                                    int* status, const TX* __restrict__ Dinv)
 {
     using T = TX;
     using R = real_t<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TL (*Lbuf)[RB][RB + 1] = reinterpret_cast<TL (*)[RB][RB + 1]>(smem_raw);
+    T (*Ibuf)[RB + 1] = reinterpret_cast<T (*)[RB + 1]>(
+        smem_raw + ((potrs_smem_bytes<TL, TX, false>() + 15) / 16) * 16);
     T (*Xs)[RC + 1] = reinterpret_cast<T (*)[RC + 1]>(smem_raw + sizeof(TL) * 2 * RB * (RB + 1));
     T (*Acc)[RC + 1] = Xs + RB;
     R* Rinv = reinterpret_cast<R*>(Acc + RB);
@@ -146,6 +153,14 @@ __global__ void __launch_bounds__(NT) k_potrs_fused(const TL* __restrict__ A, lo
     // L(r, c) = D[c][r] ('L') or conj(D[c][r]) ('U') for r >= c.  Prefetched into the ring slot
     // the last off-diagonal tile leaves free, so it is resident when the solve reaches it.
     auto issue_diag = [&](int buf) {
+        if constexpr (INV) {
+            const T* src0 = Dinv + (long long)blk * RB * RB;
+            for (int idx = threadIdx.x; idx < RB * RB; idx += NT) {
+                const int r = idx % RB, c = idx / RB;
+                cp_async_elem<sizeof(T)>(&Ibuf[c][r], src0 + idx, true);
+            }
+            return;
+        }
         for (int idx = threadIdx.x; idx < RB * RB; idx += NT) {
             int r, c;
             const TL* src;
@@ -220,9 +235,34 @@ __global__ void __launch_bounds__(NT) k_potrs_fused(const TL* __restrict__ A, lo
 #pragma unroll
     for (int q = 0; q < RC / 4; ++q) Acc[tr][tg + 4 * q] = acc[q];
     __syncthreads();
-    for (int k = threadIdx.x; k < RB; k += NT) Rinv[k] = k < nrows ? R(1) / re(widen<T>(D[k][k])) : R(0);
+    if constexpr (!INV)
+        for (int k = threadIdx.x; k < RB; k += NT) Rinv[k] = k < nrows ? R(1) / re(widen<T>(D[k][k])) : R(0);
     __syncthreads();
-    {
+    if constexpr (INV) {
+        // diagonal step as a product with the precomputed inverse block:
+        // forward x = inv(L_bb) acc, backward x = inv(L_bb)^H acc
+        T out[RC / 4];
+#pragma unroll
+        for (int q = 0; q < RC / 4; ++q) out[q] = zero<T>();
+        if (fwd) {
+#pragma unroll 8
+            for (int k = 0; k < RB; ++k) {
+                const T m = Ibuf[k][tr];
+#pragma unroll
+                for (int q = 0; q < RC / 4; ++q) out[q] = fma_(out[q], m, Acc[k][tg + 4 * q]);
+            }
+        } else {
+#pragma unroll 8
+            for (int k = 0; k < RB; ++k) {
+                const T m = cj(Ibuf[tr][k]);
+#pragma unroll
+                for (int q = 0; q < RC / 4; ++q) out[q] = fma_(out[q], m, Acc[k][tg + 4 * q]);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < RC / 4; ++q) Acc[tr][tg + 4 * q] = out[q];
+    } else {
         // warp w solves right-hand sides 2w and 2w+1 together; lanes own rows lane and lane+32
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
         const int ra = 2 * warp, rb = 2 * warp + 1;
@@ -289,25 +329,26 @@ __global__ void __launch_bounds__(NT) k_potrs_fused(const TL* __restrict__ A, lo
     if (threadIdx.x == 0) st_release(&cflags[fwd ? blk : N + blk], 1);
 }
 
-template <class T, bool UP, bool BT, class TL = T>
+template <class T, bool UP, bool BT, class TL = T, bool INV = false>
 cudaError_t potrs_launch(const TL* A, long long lda, T* B, long long ldb, int n, int nrhs, int* flags, int* ticket,
-                         int* status, cudaStream_t st)
+                         int* status, cudaStream_t st, const T* Dinv = nullptr)
 {
     const int N = (int)ceil_div(n, RB);
     const int nchunks = (int)ceil_div(nrhs, RC);
     const long long grid = 2LL * N * nchunks;
-    const size_t smem = potrs_smem_bytes<TL, T>();
+    const size_t smem = potrs_smem_bytes<TL, T, INV>();
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_potrs_fused<TL, T, UP, BT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_potrs_fused<TL, T, UP, BT, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
         attr = true;
     }
     const double cf = Traits<T>::cplx ? 4.0 : 1.0;
     const double nd = n, rd = nrhs;
     ProfScope ps(PK_POTRS_FUSED, st, cf * 2.0 * nd * nd * rd,
                  sizeof(TL) * nd * (nd + 1) + sizeof(T) * 4.0 * nd * rd);
-    k_potrs_fused<TL, T, UP, BT><<<(unsigned)grid, NT, smem, st>>>(A, lda, B, ldb, n, nrhs, nchunks, flags, ticket,
-                                                                    status);
+    k_potrs_fused<TL, T, UP, BT, INV><<<(unsigned)grid, NT, smem, st>>>(A, lda, B, ldb, n, nrhs, nchunks, flags,
+                                                                         ticket, status, Dinv);
     note_launches(1);
     return cudaGetLastError();
 }
@@ -340,10 +381,76 @@ cudaError_t potrs_dispatch(char type, char uplo, char side, int n, int nrhs, con
 }  // namespace
 }  // namespace ddlak
 
+// ---------------------------------------------------------------------------
+// inverses of the RB x RB diagonal blocks of an FP32 factor, in FP64: one CTA
+// per block, the block widened into shared memory, one thread per column of
+// the inverse (forward substitution against the identity).
+// ---------------------------------------------------------------------------
+namespace ddlak {
+namespace {
+__global__ void __launch_bounds__(128) k_inv_diag_blocks(const float* __restrict__ L, long long ldl, int n,
+                                                         double* __restrict__ Dinv)
+{
+    __shared__ double Ls[RB][RB + 1];  // Ls[c][r] = L(r, c)
+    const int blk = blockIdx.x;
+    const long long i0 = (long long)blk * RB;
+    const int nb = (int)((n - i0) < RB ? (n - i0) : RB);
+    for (int idx = threadIdx.x; idx < RB * RB; idx += blockDim.x) {
+        const int r = idx % RB, c = idx / RB;
+        Ls[c][r] = (r < nb && c < nb && r >= c) ? (double)L[(i0 + r) + (i0 + c) * ldl] : 0.0;
+    }
+    __syncthreads();
+    double* out = Dinv + (long long)blk * RB * RB;
+    const int c = threadIdx.x;
+    if (c < RB) {
+        double y[RB];
+#pragma unroll
+        for (int r = 0; r < RB; ++r) y[r] = 0.0;
+        if (c < nb) {
+#pragma unroll
+            for (int r = 0; r < RB; ++r) {
+                if (r >= c && r < nb) {
+                    double s = r == c ? 1.0 : 0.0;
+#pragma unroll
+                    for (int k = 0; k < RB; ++k)
+                        if (k >= c && k < r) s = fma(-Ls[k][r], y[k], s);
+                    y[r] = s / Ls[r][r];
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < RB; ++r) out[(long long)c * RB + r] = y[r];
+    }
+}
+}  // namespace
+}  // namespace ddlak
+
+extern "C" unsigned long long ddlak_inv_diag_bytes(int n)
+{
+    return n > 0 ? (unsigned long long)ddlak::ceil_div(n, ddlak::RB) * ddlak::RB * ddlak::RB * sizeof(double) : 0;
+}
+
+extern "C" int ddlak_inv_diag_blocks(int n, const void* L32, long long ldl, void* Dinv, void* stream)
+{
+    using namespace ddlak;
+    if (n <= 0) return 0;
+    const int N = (int)ceil_div(n, RB);
+    {
+        ProfScope ps(PK_MIXED_OTHER, static_cast<cudaStream_t>(stream), (double)N * RB * RB * RB / 3.0,
+                     (double)N * RB * RB * 12.0);
+        k_inv_diag_blocks<<<N, 128, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const float*>(L32), ldl, n,
+                                                                           static_cast<double*>(Dinv));
+    }
+    note_launches(1);
+    return (int)cudaGetLastError();
+}
+
 // Solve with an FP32 factor (uplo 'L') and FP64 right-hand sides in place
-// (the refinement solves of the mixed-precision path); same scratch as ddlak_potrs.
-extern "C" int ddlak_potrs_mixed(int n, int nrhs, const void* L32, long long ldl, void* B, long long ldb, void* work,
-                                 unsigned long long work_bytes, void* stream)
+// (the refinement solves of the mixed-precision path); same scratch as
+// ddlak_potrs.  With Dinv (from ddlak_inv_diag_blocks) the diagonal steps are
+// products with the precomputed inverse blocks instead of substitutions.
+extern "C" int ddlak_potrs_mixed(int n, int nrhs, const void* L32, long long ldl, const void* Dinv, void* B,
+                                 long long ldb, void* work, unsigned long long work_bytes, void* stream)
 {
     using namespace ddlak;
     if (n <= 0 || nrhs <= 0) return 0;
@@ -353,6 +460,11 @@ extern "C" int ddlak_potrs_mixed(int n, int nrhs, const void* L32, long long ldl
     if (e != cudaSuccess) return (int)e;
     int* status = static_cast<int*>(work);
     int* flags = reinterpret_cast<int*>(static_cast<char*>(work) + 256);
+    if (Dinv)
+        return (int)potrs_launch<double, false, false, float, true>(static_cast<const float*>(L32), ldl,
+                                                                    static_cast<double*>(B), ldb, n, nrhs, flags,
+                                                                    status + 1, status, st,
+                                                                    static_cast<const double*>(Dinv));
     return (int)potrs_launch<double, false, false, float>(static_cast<const float*>(L32), ldl,
                                                           static_cast<double*>(B), ldb, n, nrhs, flags, status + 1,
                                                           status, st);
