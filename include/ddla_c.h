@@ -150,6 +150,33 @@ int ddla_d_ppotrs_noalloc(void* handle, char side, char uplo, char trans, int n,
 int ddla_d_pposv_mixed(void* handle, char uplo, char precision, int n, int nrhs, void* A, const int* descA,
                        const void* B, const int* descB, void* X, const int* descX, int* info, double* report);
 
+/* Batched uneven Cholesky factor + solve + log-determinant in one persistent
+ * launch (no reference counterpart; ddla::posvVbatched, VbatchedPlan and
+ * vbatchedAutotune in include/ddla/ddla_batched.h, which give the semantics).
+ * Every array argument is device resident, as for the reference's
+ * gemmVbatched (include/ddla/ddla.h:1828-1849).  d_B may be NULL (factor and
+ * log-determinant only).  A plan captures the launch in a CUDA graph once;
+ * ddla_vbatched_plan_run replays it on the handle's stream without a host
+ * synchronisation.  ddla_vbatched_tuning reports the table in use: grid,
+ * widths[2], variant[len] per order bucket of 16 (len >= max_n/16 rounded up
+ * to the kernel's 512 or 1024) and whether it was tuned. */
+int ddla_s_posv_vbatched(void* handle, char uplo, const int* d_n, float* const* d_A, const int* d_lda,
+                         float* const* d_B, double* d_logdet, int* d_info, int batch_count, int max_n);
+int ddla_d_posv_vbatched(void* handle, char uplo, const int* d_n, double* const* d_A, const int* d_lda,
+                         double* const* d_B, double* d_logdet, int* d_info, int batch_count, int max_n);
+int ddla_s_posv_vbatched_plan(void* handle, char uplo, const int* d_n, float* const* d_A, const int* d_lda,
+                              float* const* d_B, double* d_logdet, int* d_info, int batch_count, int max_n,
+                              void** plan);
+int ddla_d_posv_vbatched_plan(void* handle, char uplo, const int* d_n, double* const* d_A, const int* d_lda,
+                              double* const* d_B, double* d_logdet, int* d_info, int batch_count, int max_n,
+                              void** plan);
+int ddla_vbatched_plan_run(void* plan);
+int ddla_vbatched_plan_info(void* plan, int* grid, double* flops);
+int ddla_vbatched_plan_destroy(void* plan);
+int ddla_vbatched_autotune(void* handle, char type, int max_n);
+int ddla_vbatched_tuning(void* handle, char type, int max_n, int* grid, int* widths, unsigned char* variant, int len,
+                         int* tuned);
+
 /* Diagnostics (no reference counterpart: the reference has no tracing).
  * ddla_c_get_stream returns the handle's CUDA stream (ddlaGetStream of
  * include/ddla/ddla_handle_t.h:337, which the reference's C ABI does not

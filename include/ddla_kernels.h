@@ -103,6 +103,29 @@ int ddlak_multi_axpy(const void* V, long long vstride, int nv, const void* coef,
                      void* stream);
 int ddlak_scale_cols(const void* x, void* y, int n, int ncol, double alpha, const void* nrm2, void* stream);
 
+/* ---- batched uneven Cholesky (ddla::posvVbatched; no reference counterpart) ---- */
+
+/* Block-column widths of the kernel's two per-matrix variants (widths[2]) for
+ * type 's'/'d' and kernel instance nmax (512 or 1024). */
+int ddlak_vbatched_variants(char type, int nmax, int* widths);
+
+/* SMs x resident CTAs of the persistent kernel on the current device (0 on error). */
+int ddlak_vbatched_max_grid(char type, int nmax);
+
+/* One persistent launch over batch matrices: d_A[i] (order d_n[i] <= nmax,
+ * ld d_lda[i]) factored in place (lower), d_B[i] solved in place when d_B is
+ * not NULL, d_logdet[i] = log det, d_info[i] = potrf info.  d_order (may be
+ * NULL) is the processing order, d_wsel[i] (may be NULL) the variant of matrix
+ * i, d_counters two ints that are zero before the launch and are left zero. */
+int ddlak_posv_vbatched(char type, int nmax, int batch, const int* d_n, void* const* d_A, const int* d_lda,
+                        void* const* d_B, double* d_logdet, int* d_info, const int* d_order,
+                        const unsigned char* d_wsel, int* d_counters, int grid, void* stream);
+
+/* Fills d_A[i] with a diagonally dominant SPD matrix of order d_n[i] and d_B[i]
+ * (when not NULL) with ones: the autotuner's synthetic input. */
+int ddlak_fill_spd_vbatched(char type, int batch, const int* d_n, void* const* d_A, const int* d_lda,
+                            void* const* d_B, void* stream);
+
 /* Number of kernel launches the layer has made in this process. */
 long long ddlak_launch_count(void);
 

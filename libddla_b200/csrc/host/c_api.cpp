@@ -9,6 +9,7 @@
 #include <string>
 
 #include <ddla/ddla.h>
+#include <ddla/ddla_batched.h>
 #include <ddla_c.h>
 #include <ddla_kernels.h>
 
@@ -424,6 +425,101 @@ int ddla_d_pposv_mixed(void* handle, char uplo, char precision, int n, int nrhs,
             report[2] = rep.shift;
             report[3] = rep.backward_error;
         }
+        return ST_SUCCESS;
+    });
+}
+
+int ddla_s_posv_vbatched(void* handle, char uplo, const int* d_n, float* const* d_A, const int* d_lda,
+                         float* const* d_B, double* d_logdet, int* d_info, int batch_count, int max_n)
+{
+    return run(handle, [&](ddla::DdlaHandle_t h) -> int {
+        ddla::posvVbatched<float>(h, uplo, d_n, d_A, d_lda, d_B, d_logdet, d_info, batch_count, max_n);
+        return ST_SUCCESS;
+    });
+}
+
+int ddla_d_posv_vbatched(void* handle, char uplo, const int* d_n, double* const* d_A, const int* d_lda,
+                         double* const* d_B, double* d_logdet, int* d_info, int batch_count, int max_n)
+{
+    return run(handle, [&](ddla::DdlaHandle_t h) -> int {
+        ddla::posvVbatched<double>(h, uplo, d_n, d_A, d_lda, d_B, d_logdet, d_info, batch_count, max_n);
+        return ST_SUCCESS;
+    });
+}
+
+int ddla_s_posv_vbatched_plan(void* handle, char uplo, const int* d_n, float* const* d_A, const int* d_lda,
+                              float* const* d_B, double* d_logdet, int* d_info, int batch_count, int max_n,
+                              void** plan)
+{
+    return run(handle, [&](ddla::DdlaHandle_t h) -> int {
+        if (!plan) return ST_INVALID_VALUE;
+        *plan = ddla::VbatchedPlan::create<float>(h, uplo, d_n, d_A, d_lda, d_B, d_logdet, d_info, batch_count,
+                                                  max_n);
+        return ST_SUCCESS;
+    });
+}
+
+int ddla_d_posv_vbatched_plan(void* handle, char uplo, const int* d_n, double* const* d_A, const int* d_lda,
+                              double* const* d_B, double* d_logdet, int* d_info, int batch_count, int max_n,
+                              void** plan)
+{
+    return run(handle, [&](ddla::DdlaHandle_t h) -> int {
+        if (!plan) return ST_INVALID_VALUE;
+        *plan = ddla::VbatchedPlan::create<double>(h, uplo, d_n, d_A, d_lda, d_B, d_logdet, d_info, batch_count,
+                                                   max_n);
+        return ST_SUCCESS;
+    });
+}
+
+int ddla_vbatched_plan_run(void* plan)
+{
+    if (!plan) return ST_INVALID_VALUE;
+    return guarded("ddla_vbatched_plan_run", [&]() -> int {
+        static_cast<ddla::VbatchedPlan*>(plan)->run();
+        return ST_SUCCESS;
+    });
+}
+
+int ddla_vbatched_plan_info(void* plan, int* grid, double* flops)
+{
+    if (!plan) return ST_INVALID_VALUE;
+    const auto* p = static_cast<ddla::VbatchedPlan*>(plan);
+    if (grid) *grid = p->grid();
+    if (flops) *flops = p->flops();
+    return ST_SUCCESS;
+}
+
+int ddla_vbatched_plan_destroy(void* plan)
+{
+    return guarded("ddla_vbatched_plan_destroy", [&]() -> int {
+        delete static_cast<ddla::VbatchedPlan*>(plan);
+        return ST_SUCCESS;
+    });
+}
+
+int ddla_vbatched_autotune(void* handle, char type, int max_n)
+{
+    return run(handle, [&](ddla::DdlaHandle_t h) -> int {
+        ddla::vbatchedAutotune(h, type, max_n);
+        return ST_SUCCESS;
+    });
+}
+
+int ddla_vbatched_tuning(void* handle, char type, int max_n, int* grid, int* widths, unsigned char* variant, int len,
+                         int* tuned)
+{
+    return run(handle, [&](ddla::DdlaHandle_t h) -> int {
+        const ddla::VbatchedTuning t = ddla::vbatchedTuning(h, type, max_n);
+        if (grid) *grid = t.grid;
+        if (widths) {
+            widths[0] = t.widths[0];
+            widths[1] = t.widths[1];
+        }
+        if (variant) {
+            if (len < (int)t.variant.size()) return ST_INVALID_VALUE;
+            std::memcpy(variant, t.variant.data(), t.variant.size());
+        }
+        if (tuned) *tuned = t.tuned ? 1 : 0;
         return ST_SUCCESS;
     });
 }

@@ -158,6 +158,12 @@ __device__ __forceinline__ void cp_async_elem(void* smem, const void* gmem, bool
                  "r"(valid ? BYTES : 0)
                  : "memory");
 }
+__device__ __forceinline__ void cp_group_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_group_wait()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit_wait_all()
 {
     asm volatile("cp.async.commit_group;" ::: "memory");

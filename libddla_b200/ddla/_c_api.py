@@ -139,7 +139,17 @@ _SIGS = {
     "ddla_c_launch_count": (_ll, []),
     "ddla_c_profile_enable": (None, [_i]),
     "ddla_c_profile_read": (_i, [_i, _dp, _llp, _dp, _dp, _i]),
+    "ddla_vbatched_plan_run": (_i, [_vp]),
+    "ddla_vbatched_plan_info": (_i, [_vp, _ip, _dp]),
+    "ddla_vbatched_plan_destroy": (_i, [_vp]),
+    "ddla_vbatched_autotune": (_i, [_vp, _c, _i]),
+    "ddla_vbatched_tuning": (_i, [_vp, _c, _i, _ip, _ip, ctypes.POINTER(ctypes.c_ubyte), _i, _ip]),
 }
+for _p in "sd":
+    _SIGS.update({
+        f"ddla_{_p}_posv_vbatched": (_i, [_vp, _c, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i]),
+        f"ddla_{_p}_posv_vbatched_plan": (_i, [_vp, _c, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, ctypes.POINTER(_vp)]),
+    })
 for _p in "sdcz":
     _SIGS.update({
         f"ddla_{_p}_gather": (_i, [_vp, _i, _i, _vp, _i, _i, _vp, _i, _vp, _i]),

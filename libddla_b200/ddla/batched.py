@@ -1,0 +1,163 @@
+"""Batched uneven Cholesky (factor + solve + log-determinant) from Python.
+
+Thin ctypes layer over ddla_{s,d}_posv_vbatched / _plan (include/ddla_c.h;
+semantics in include/ddla/ddla_batched.h).  PyTorch provides the device
+memory: `pack` copies a list of square matrices (and right-hand sides) into one
+device buffer with the device-resident order / leading-dimension / pointer
+arrays the C ABI takes.  No reference counterpart: the reference has no
+batched Cholesky; its per-matrix equivalent is ops.pposv + ops.diag_logdet.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _c_api as C
+
+_ALIGN = 32  # elements: every matrix and vector starts on a 256-byte boundary
+
+
+def _torch():
+    import torch
+    return torch
+
+
+@dataclass
+class PackedBatch:
+    """Device-resident batch: one buffer of matrices, one of right-hand sides,
+    and the arrays the C ABI reads (all torch tensors on one CUDA device)."""
+    dtype: np.dtype
+    orders: np.ndarray        # host copy of the orders
+    a_offsets: np.ndarray     # element offset of matrix i in `mats`
+    b_offsets: np.ndarray
+    mats: "object"            # torch 1-D tensor
+    rhs: "object"             # torch 1-D tensor or None
+    d_n: "object"
+    d_lda: "object"
+    d_A: "object"             # int64 device pointers
+    d_B: "object"
+    logdet: "object"          # float64 [batch]
+    info: "object"            # int32 [batch]
+    max_n: int
+
+    @property
+    def batch(self) -> int:
+        return len(self.orders)
+
+    def matrix(self, i: int):
+        """Device view of matrix i, column-major (n x n, lda = n)."""
+        n = int(self.orders[i])
+        o = int(self.a_offsets[i])
+        return self.mats[o:o + n * n].view(n, n).t()
+
+    def vector(self, i: int):
+        n = int(self.orders[i])
+        o = int(self.b_offsets[i])
+        return self.rhs[o:o + n]
+
+
+def pack(mats: Sequence[np.ndarray], rhs: Optional[Sequence[np.ndarray]] = None, device="cuda",
+         dtype=np.float64, max_n: Optional[int] = None) -> PackedBatch:
+    """Copy host matrices (square, any layout) and optional vectors to the device."""
+    torch = _torch()
+    dt = np.dtype(dtype)
+    tdt = {np.dtype(np.float64): torch.float64, np.dtype(np.float32): torch.float32}[dt]
+    orders = np.array([m.shape[0] for m in mats], dtype=np.int32)
+    for m in mats:
+        if m.ndim != 2 or m.shape[0] != m.shape[1]:
+            raise ValueError("pack: matrices must be square")
+    sizes = (orders.astype(np.int64) ** 2 + _ALIGN - 1) // _ALIGN * _ALIGN
+    a_off = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+    host = np.zeros(int(sizes.sum()) if len(sizes) else 0, dtype=dt)
+    for i, m in enumerate(mats):
+        n = orders[i]
+        host[a_off[i]:a_off[i] + n * n] = np.asarray(m, dtype=dt).ravel(order="F")
+    d_mats = torch.from_numpy(host).to(device)
+    d_rhs = None
+    b_off = np.zeros(len(mats), dtype=np.int64)
+    if rhs is not None:
+        vs = (orders.astype(np.int64) + _ALIGN - 1) // _ALIGN * _ALIGN
+        b_off = np.concatenate([[0], np.cumsum(vs)[:-1]]).astype(np.int64)
+        hb = np.zeros(int(vs.sum()) if len(vs) else 0, dtype=dt)
+        for i, v in enumerate(rhs):
+            hb[b_off[i]:b_off[i] + orders[i]] = np.asarray(v, dtype=dt).ravel()
+        d_rhs = torch.from_numpy(hb).to(device)
+    es = dt.itemsize
+    a_ptrs = d_mats.data_ptr() + a_off * es
+    b_ptrs = (d_rhs.data_ptr() + b_off * es) if d_rhs is not None else None
+    mx = int(orders.max()) if len(orders) else 0
+    return PackedBatch(
+        dtype=dt, orders=orders, a_offsets=a_off, b_offsets=b_off, mats=d_mats, rhs=d_rhs,
+        d_n=torch.from_numpy(orders).to(device),
+        d_lda=torch.from_numpy(np.maximum(orders, 1).astype(np.int32)).to(device),
+        d_A=torch.from_numpy(a_ptrs.astype(np.int64)).to(device),
+        d_B=torch.from_numpy(b_ptrs.astype(np.int64)).to(device) if b_ptrs is not None else None,
+        logdet=torch.zeros(len(mats), dtype=torch.float64, device=device),
+        info=torch.zeros(len(mats), dtype=torch.int32, device=device),
+        max_n=int(max_n if max_n is not None else mx))
+
+
+def _sfx(pb: PackedBatch) -> str:
+    return "d" if pb.dtype == np.float64 else "s"
+
+
+def _args(pb: PackedBatch):
+    return (pb.d_n.data_ptr(), pb.d_A.data_ptr(), pb.d_lda.data_ptr(),
+            pb.d_B.data_ptr() if pb.d_B is not None else None,
+            pb.logdet.data_ptr(), pb.info.data_ptr(), pb.batch, pb.max_n)
+
+
+def posv_vbatched(handle, pb: PackedBatch, uplo: str = "L") -> None:
+    """One persistent launch over the batch (enqueued on the handle's stream)."""
+    fn = getattr(C, f"ddla_{_sfx(pb)}_posv_vbatched")
+    C.check_status(fn(handle.ptr, uplo.encode(), *_args(pb)), "posv_vbatched")
+
+
+class VbatchedPlan:
+    """The launch captured once in a CUDA graph; run() replays it on the handle's
+    stream (its own CUDA stream: inputs written through torch must be complete,
+    e.g. torch.cuda.synchronize(), before run())."""
+
+    def __init__(self, handle, pb: PackedBatch, uplo: str = "L"):
+        self._pb = pb
+        self._ptr = ctypes.c_void_p()
+        fn = getattr(C, f"ddla_{_sfx(pb)}_posv_vbatched_plan")
+        C.check_status(fn(handle.ptr, uplo.encode(), *_args(pb), ctypes.byref(self._ptr)), "VbatchedPlan")
+
+    def run(self) -> None:
+        C.check_status(C.ddla_vbatched_plan_run(self._ptr), "VbatchedPlan.run")
+
+    def info(self):
+        g = ctypes.c_int()
+        f = ctypes.c_double()
+        C.check_status(C.ddla_vbatched_plan_info(self._ptr, ctypes.byref(g), ctypes.byref(f)), "VbatchedPlan.info")
+        return {"grid": g.value, "flops": f.value}
+
+    def close(self) -> None:
+        if self._ptr:
+            C.check_status(C.ddla_vbatched_plan_destroy(self._ptr), "VbatchedPlan.close")
+            self._ptr = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune(handle, dtype: str, max_n: int) -> None:
+    C.check_status(C.ddla_vbatched_autotune(handle.ptr, dtype.encode(), int(max_n)), "vbatched autotune")
+
+
+def tuning(handle, dtype: str, max_n: int) -> dict:
+    g = ctypes.c_int()
+    w = (ctypes.c_int * 2)()
+    v = (ctypes.c_ubyte * 64)()
+    t = ctypes.c_int()
+    C.check_status(C.ddla_vbatched_tuning(handle.ptr, dtype.encode(), int(max_n), ctypes.byref(g), w, v, 64,
+                                          ctypes.byref(t)), "vbatched tuning")
+    nb = (512 if max_n <= 512 else 1024) // 16
+    return {"grid": g.value, "widths": [w[0], w[1]], "variant": [v[i] for i in range(nb)], "tuned": bool(t.value)}
