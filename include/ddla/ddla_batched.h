@@ -74,6 +74,42 @@ struct VbatchedTuning {
 };
 VbatchedTuning vbatchedTuning(const DdlaHandle_t& handle, char type, int max_n);
 
+// ---- negative log marginal likelihood and its adjoint ----------------------
+// loss_b = 1/2 (y_b^T A_b^-1 y_b + log det A_b) for `batch` problems of order n,
+// packed on the device: A, L, W [batch][n*n] column-major (leading dimension n),
+// y, alpha [batch][n], X [batch][n][d] row-major, theta {l, sigma_f^2, sigma^2}
+// per problem (theta_stride 3) or shared by all (theta_stride 0), logdet / quad
+// / info [batch].  With alpha = A^-1 y the gradients are
+//   dloss/dA = 1/2 (A^-1 - alpha alpha^T),  dloss/dy = alpha,
+// and A^-1 = W^T W with W = L^-1 (lower).  Orders up to 1024 run one CTA per
+// problem (the batched factorization of posvVbatched and a batched W = L^-1);
+// larger orders take batch == 1 and the blocked single-matrix kernels.
+// All calls are enqueued on the handle's stream; the forward ones read the
+// orders back once (one synchronisation), the backward ones never synchronise.
+
+// Forward on a given matrix: A (lower triangle) is replaced by L.
+template <typename T>
+void cholNllBatched(const DdlaHandle_t& handle, int batch, int n, T* A, const T* y, T* alpha, double* logdet,
+                    double* quad, int* info);
+
+// Forward of the Gaussian-process likelihood: A = K(theta) + sigma^2 I with
+// K_ij = sigma_f^2 exp(-|x_i - x_j|^2 / (2 l^2)) is built on the device (lower
+// triangle), then factored as in cholNllBatched.
+template <typename T>
+void gpNllBatched(const DdlaHandle_t& handle, int batch, int n, int d, const T* X, const double* theta,
+                  int theta_stride, const T* y, T* A, T* alpha, double* logdet, double* quad, int* info);
+
+// Dense adjoint from the forward's L and alpha: G = 1/2 (A^-1 - alpha alpha^T),
+// full symmetric.  W is [batch][n*n] scratch.
+template <typename T>
+void cholNllGradBatched(const DdlaHandle_t& handle, int batch, int n, const T* L, const T* alpha, T* W, T* G);
+
+// Hyperparameter gradient: grad[b][0..2] = dloss_b/d{l, sigma_f^2, sigma^2}, the
+// adjoint contracted with dA/dtheta tile by tile (dA/dtheta is never stored).
+template <typename T>
+void gpNllGradBatched(const DdlaHandle_t& handle, int batch, int n, int d, const T* X, const double* theta,
+                      int theta_stride, const T* L, const T* alpha, T* W, double* grad);
+
 }  // namespace ddla
 
 #endif

@@ -177,6 +177,32 @@ int ddla_vbatched_autotune(void* handle, char type, int max_n);
 int ddla_vbatched_tuning(void* handle, char type, int max_n, int* grid, int* widths, unsigned char* variant, int len,
                          int* tuned);
 
+/* Negative log marginal likelihood loss = 1/2 (y^T A^-1 y + log det A) and its
+ * adjoint for batches of equal-order problems (no reference counterpart;
+ * ddla::cholNllBatched, gpNllBatched, cholNllGradBatched, gpNllGradBatched in
+ * include/ddla/ddla_batched.h give layouts and formulas).  Device arrays:
+ * A/L/W/G batch x n x n column-major, y/alpha batch x n, X batch x n x d
+ * row-major, theta {l, sigma_f^2, sigma^2} (theta_stride 3 per problem, 0
+ * shared), logdet/quad/info batch, grad batch x 3. */
+int ddla_s_chol_nll_batched(void* handle, int batch, int n, float* A, const float* y, float* alpha, double* logdet,
+                            double* quad, int* info);
+int ddla_d_chol_nll_batched(void* handle, int batch, int n, double* A, const double* y, double* alpha,
+                            double* logdet, double* quad, int* info);
+int ddla_s_gp_nll_batched(void* handle, int batch, int n, int d, const float* X, const double* theta,
+                          int theta_stride, const float* y, float* A, float* alpha, double* logdet, double* quad,
+                          int* info);
+int ddla_d_gp_nll_batched(void* handle, int batch, int n, int d, const double* X, const double* theta,
+                          int theta_stride, const double* y, double* A, double* alpha, double* logdet, double* quad,
+                          int* info);
+int ddla_s_chol_nll_grad_batched(void* handle, int batch, int n, const float* L, const float* alpha, float* W,
+                                 float* G);
+int ddla_d_chol_nll_grad_batched(void* handle, int batch, int n, const double* L, const double* alpha, double* W,
+                                 double* G);
+int ddla_s_gp_nll_grad_batched(void* handle, int batch, int n, int d, const float* X, const double* theta,
+                               int theta_stride, const float* L, const float* alpha, float* W, double* grad);
+int ddla_d_gp_nll_grad_batched(void* handle, int batch, int n, int d, const double* X, const double* theta,
+                               int theta_stride, const double* L, const double* alpha, double* W, double* grad);
+
 /* Diagnostics (no reference counterpart: the reference has no tracing).
  * ddla_c_get_stream returns the handle's CUDA stream (ddlaGetStream of
  * include/ddla/ddla_handle_t.h:337, which the reference's C ABI does not

@@ -126,6 +126,35 @@ int ddlak_posv_vbatched(char type, int nmax, int batch, const int* d_n, void* co
 int ddlak_fill_spd_vbatched(char type, int batch, const int* d_n, void* const* d_A, const int* d_lda,
                             void* const* d_B, void* stream);
 
+/* ---- likelihood adjoint (ddla::cholNll* / gpNll*; no reference counterpart) ----
+ * Batches of equal-order problems at fixed element strides; see
+ * include/ddla/ddla_batched.h for the formulas. */
+
+/* A = sigma_f^2 exp(-|x_i-x_j|^2/(2 l^2)) + sigma^2 delta_ij (lower triangle);
+ * X row-major n x d per problem, theta {l, sigma_f^2, sigma^2} at theta + m*tstride. */
+int ddlak_gp_build(char type, int batch, int n, int d, const void* X, long long xstride, const double* theta,
+                   int tstride, void* A, long long lda, long long astride, void* stream);
+
+/* W = L^-1 (lower triangle written) for n <= 1024, one CTA per matrix. */
+int ddlak_trtri_batched(char type, int batch, int n, const void* L, long long ldl, long long lstride, void* W,
+                        long long ldw, long long wstride, void* stream);
+
+/* out[m] = sum x_m .* y_m, and out[m] = 2 sum log L_m(i,i), in FP64. */
+int ddlak_batched_dot(char type, int batch, int n, const void* x, long long xstride, const void* y,
+                      long long ystride, double* out, void* stream);
+int ddlak_batched_logdiag(char type, int batch, int n, const void* L, long long ldl, long long lstride, double* out,
+                          void* stream);
+
+/* Adjoint contraction on 64 x 64 lower tiles of A^-1 = W^T W (mode bit 2 set: W
+ * already holds A^-1).  mode & 1 == 0: grad[m][0..2] = dloss/d{l, sigma_f^2,
+ * sigma^2} through per-tile partials (partial: ddlak_adjoint_partial_bytes);
+ * mode & 1 == 1: G = 1/2 (A^-1 - alpha alpha^T), dense symmetric. */
+unsigned long long ddlak_adjoint_partial_bytes(int batch, int n);
+int ddlak_adjoint_contract(char type, int mode, int batch, int n, const void* W, long long ldw, long long wstride,
+                           const void* alpha, long long astride, const void* X, int d, long long xstride,
+                           const double* theta, int tstride, double* partial, double* grad, void* G, long long ldg,
+                           long long gstride, void* stream);
+
 /* Number of kernel launches the layer has made in this process. */
 long long ddlak_launch_count(void);
 

@@ -524,4 +524,41 @@ int ddla_vbatched_tuning(void* handle, char type, int max_n, int* grid, int* wid
     });
 }
 
+#define DDLA_GP_C(P, T)                                                                                             \
+    int ddla_##P##_chol_nll_batched(void* handle, int batch, int n, T* A, const T* y, T* alpha, double* logdet,      \
+                                    double* quad, int* info)                                                        \
+    {                                                                                                               \
+        return run(handle, [&](ddla::DdlaHandle_t h) -> int {                                                       \
+            ddla::cholNllBatched<T>(h, batch, n, A, y, alpha, logdet, quad, info);                                  \
+            return ST_SUCCESS;                                                                                      \
+        });                                                                                                         \
+    }                                                                                                               \
+    int ddla_##P##_gp_nll_batched(void* handle, int batch, int n, int d, const T* X, const double* theta,           \
+                                  int theta_stride, const T* y, T* A, T* alpha, double* logdet, double* quad,        \
+                                  int* info)                                                                        \
+    {                                                                                                               \
+        return run(handle, [&](ddla::DdlaHandle_t h) -> int {                                                       \
+            ddla::gpNllBatched<T>(h, batch, n, d, X, theta, theta_stride, y, A, alpha, logdet, quad, info);         \
+            return ST_SUCCESS;                                                                                      \
+        });                                                                                                         \
+    }                                                                                                               \
+    int ddla_##P##_chol_nll_grad_batched(void* handle, int batch, int n, const T* L, const T* alpha, T* W, T* G)    \
+    {                                                                                                               \
+        return run(handle, [&](ddla::DdlaHandle_t h) -> int {                                                       \
+            ddla::cholNllGradBatched<T>(h, batch, n, L, alpha, W, G);                                               \
+            return ST_SUCCESS;                                                                                      \
+        });                                                                                                         \
+    }                                                                                                               \
+    int ddla_##P##_gp_nll_grad_batched(void* handle, int batch, int n, int d, const T* X, const double* theta,      \
+                                       int theta_stride, const T* L, const T* alpha, T* W, double* grad)            \
+    {                                                                                                               \
+        return run(handle, [&](ddla::DdlaHandle_t h) -> int {                                                       \
+            ddla::gpNllGradBatched<T>(h, batch, n, d, X, theta, theta_stride, L, alpha, W, grad);                   \
+            return ST_SUCCESS;                                                                                      \
+        });                                                                                                         \
+    }
+DDLA_GP_C(s, float)
+DDLA_GP_C(d, double)
+#undef DDLA_GP_C
+
 }  // extern "C"

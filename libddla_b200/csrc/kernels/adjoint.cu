@@ -1,0 +1,494 @@
+// Cholesky / solve / log-determinant adjoint for loss = 1/2 (y^T A^-1 y + log det A)
+// (no reference counterpart).  With A = L L^T and alpha = A^-1 y,
+//   dloss/dA = Abar = 1/2 (A^-1 - alpha alpha^T),   dloss/dy = alpha,
+// and A^-1 = W^T W with W = L^-1.  Kernels, over a batch of equal-order
+// matrices laid out with fixed strides:
+//   k_gp_build        A = K(theta) + sigma^2 I (squared-exponential kernel on
+//                     points in R^d), lower triangle only (all the factorization reads);
+//   k_trtri_batched   W = L^-1 (lower), one CTA per matrix (order <= 1024):
+//                     block columns of width B; for each 32-row block the rows'
+//                     partial results are staged in shared memory, all warps solve
+//                     them against the 32 x 32 diagonal block of L (a few columns
+//                     each, shuffles), and every thread updates the rows it owns
+//                     below from registers;
+//   k_adjoint_contract  (W^T W) tile by tile (64 x 64 lower tiles, k from the tile's
+//                     first row: W is lower triangular) with a fused epilogue that
+//                     either contracts Abar with dA/dtheta (recomputed from the
+//                     points, never stored) into per-tile partial sums, or writes
+//                     the dense symmetric Abar;
+//   k_adjoint_reduce  per-matrix sums of the partials in a fixed order (deterministic);
+//   k_batched_dot     y^T alpha per problem (FP64 accumulation).
+#include <cuda_runtime.h>
+
+#include <ddla_kernels.h>
+
+#include "common.cuh"
+#include "profile.h"
+
+namespace ddlak {
+namespace {
+
+constexpr int TR_NT = 256;
+constexpr int TR_NMAX = 1024;
+constexpr int CT_TILE = 64;
+constexpr int CT_KC = 16;
+constexpr int CT_NT = 256;
+
+// ---------------------------------------------------------------------------
+// A = sigma_f^2 exp(-|x_i - x_j|^2 / (2 l^2)) + sigma^2 delta_ij, lower triangle.
+// theta = {l, sigma_f^2, sigma^2} per matrix (tstride 3) or shared (tstride 0).
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void k_gp_build(int n, int d, const T* __restrict__ X, long long xstride, const double* __restrict__ theta,
+                           int tstride, T* __restrict__ A, long long lda, long long astride)
+{
+    const int m = blockIdx.z;
+    const int i = blockIdx.y * 32 + threadIdx.y, j0 = blockIdx.x * 32;
+    if (j0 > blockIdx.y * 32 + 31) return;  // tile above the diagonal
+    const T* x = X + m * xstride;
+    const double* th = theta + (long long)m * tstride;
+    const double l = th[0], sf2 = th[1], s2 = th[2];
+    const double inv2l2 = 0.5 / (l * l);
+    T* a = A + m * astride;
+    const int j = j0 + threadIdx.x;
+    if (i >= n || j >= n || j > i) return;
+    double r2 = 0.0;
+    for (int c = 0; c < d; ++c) {
+        const double dx = (double)x[(long long)i * d + c] - (double)x[(long long)j * d + c];
+        r2 += dx * dx;
+    }
+    double v = sf2 * exp(-r2 * inv2l2);
+    if (i == j) v += s2;
+    a[i + (long long)j * lda] = (T)v;
+}
+
+// ---------------------------------------------------------------------------
+// W = L^-1 for every matrix of the batch (order n <= 1024), lower triangle of W.
+// ---------------------------------------------------------------------------
+template <class T> struct TrWidth { static constexpr int B = 16; };
+template <> struct TrWidth<float> { static constexpr int B = 32; };
+
+template <class T>
+__global__ void __launch_bounds__(TR_NT, 1)
+    k_trtri_batched(int n, const T* __restrict__ Lg, long long ldl, long long lstride, T* __restrict__ Wg,
+                    long long ldw, long long wstride)
+{
+    constexpr int B = TrWidth<T>::B;
+    constexpr int RPT = TR_NMAX / TR_NT;
+    constexpr int CPW = B / (TR_NT / 32);  // columns each warp solves
+    __shared__ T Xs[2][32][B + 1];
+    __shared__ T Ls[2][32][33];
+    const T* L = Lg + blockIdx.x * lstride;
+    T* W = Wg + blockIdx.x * wstride;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    int step = 0;
+    for (int J = 0; J < n; J += B) {
+        const int nb = min(B, n - J);
+        T acc[RPT][B];
+#pragma unroll
+        for (int r = 0; r < RPT; ++r)
+#pragma unroll
+            for (int q = 0; q < B; ++q) acc[r][q] = (t + r * TR_NT == J + q && q < nb) ? T(1) : T(0);
+        const int I0 = J & ~31;
+#pragma unroll
+        for (int rb = 0; rb < RPT; ++rb) {
+            for (int wb = 0; wb < TR_NT / 32; ++wb) {
+                const int I = rb * TR_NT + wb * 32;
+                if (I < I0 || I >= n) continue;  // uniform
+                const int buf = step & 1;
+                ++step;
+                // 1. stage this row block's partial results and the diagonal block of L
+                if (warp == wb)
+#pragma unroll
+                    for (int q = 0; q < B; ++q) Xs[buf][lane][q] = acc[rb][q];
+                for (int e = t; e < 32 * 32; e += TR_NT) {
+                    const int r = e & 31, c = e >> 5;
+                    Ls[buf][r][c] = (c <= r && I + r < n) ? L[(I + r) + (long long)(I + c) * ldl] : T(0);
+                }
+                __syncthreads();
+                // 2. X_I = L_II^-1 Xs: warp w solves columns w*CPW .. w*CPW+CPW-1, lane = row
+                {
+                    T x[CPW];
+#pragma unroll
+                    for (int c = 0; c < CPW; ++c) x[c] = Xs[buf][lane][warp * CPW + c];
+                    const bool live = I + lane < n;
+#pragma unroll 4
+                    for (int k = 0; k < 32; ++k) {
+                        const T dkk = Ls[buf][k][k];
+                        const T lk = Ls[buf][lane][k];
+#pragma unroll
+                        for (int c = 0; c < CPW; ++c) {
+                            if (lane == k) x[c] = live ? x[c] / dkk : T(0);
+                            const T xk = __shfl_sync(0xffffffffu, x[c], k);
+                            if (lane > k) x[c] = fms(x[c], lk, xk);
+                        }
+                    }
+#pragma unroll
+                    for (int c = 0; c < CPW; ++c) {
+                        const int q = warp * CPW + c;
+                        Xs[buf][lane][q] = x[c];
+                        if (live && q < nb && I + lane >= J + q) W[(I + lane) + (long long)(J + q) * ldw] = x[c];
+                    }
+                }
+                __syncthreads();
+                // 3. rows below the block: acc -= L(i, I:I+32) X_I
+#pragma unroll
+                for (int r = 0; r < RPT; ++r) {
+                    if (r < rb) continue;
+                    const int i = t + r * TR_NT;
+                    if (i < I + 32 || i >= n) continue;
+                    const T* li = L + i + (long long)I * ldl;
+#pragma unroll 4
+                    for (int k = 0; k < 32; ++k) {
+                        const T l = li[(long long)k * ldl];
+#pragma unroll
+                        for (int q = 0; q < B; ++q) acc[r][q] = fms(acc[r][q], l, Xs[buf][k][q]);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// (W^T W) on 64 x 64 lower tiles with the adjoint epilogue.
+//   mode 0: partial[m][tile][0..2] = sum over the tile's i >= j of
+//           w_ij Abar_ij dA_ij/d{l, sigma_f^2, sigma^2}, w = 2 off the diagonal;
+//   mode 1: G[i + j ldg] = G[j + i ldg] = Abar_ij (dense symmetric gradient).
+// DIRECT: the operand already is A^-1 (orders above the batched inversion's
+// limit, where A^-1 comes from the fused solve on the identity): the tile is
+// read instead of multiplied.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void tile_of_lower(int t, int& ti, int& tj)
+{
+    int i = (int)((sqrtf(8.f * t + 1.f) - 1.f) * 0.5f);
+    while ((i + 1) * (i + 2) / 2 <= t) ++i;
+    while (i * (i + 1) / 2 > t) --i;
+    ti = i;
+    tj = t - i * (i + 1) / 2;
+}
+
+template <class T, int MODE, bool DIRECT>
+__global__ void __launch_bounds__(CT_NT)
+    k_adjoint_contract(int n, const T* __restrict__ Wg, long long ldw, long long wstride,
+                       const T* __restrict__ alpha_g, long long astride, const T* __restrict__ X, int d,
+                       long long xstride, const double* __restrict__ theta, int tstride, double* __restrict__ partial,
+                       T* __restrict__ G, long long ldg, long long gstride)
+{
+    __shared__ T Wi[2][CT_KC][CT_TILE];
+    __shared__ T Wj[2][CT_KC][CT_TILE];
+    __shared__ double red[3][CT_NT / 32];
+    const int m = blockIdx.y;
+    const int tile = blockIdx.x;
+    int ti, tj;
+    tile_of_lower(tile, ti, tj);
+    const int i0 = ti * CT_TILE, j0 = tj * CT_TILE;
+    const T* W = Wg + m * wstride;
+    const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+    T acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
+    // k runs over [i0, n): W(k, i) = 0 for k < i.  DIRECT: Wg holds A^-1 itself.
+    const int kbeg = i0, nk = n - kbeg;
+    const int nch = DIRECT ? 0 : (nk + CT_KC - 1) / CT_KC;
+    if constexpr (DIRECT) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int i = i0 + ty * 4 + u, j = j0 + tx * 4 + v;
+                if (i < n && j <= i) acc[u][v] = W[i + (long long)j * ldw];
+            }
+    }
+    auto stage = [&](int ch, int buf) {
+        const int k0 = kbeg + ch * CT_KC;
+        for (int e = t; e < CT_KC * CT_TILE; e += CT_NT) {
+            const int kk = e % CT_KC, c = e / CT_KC;
+            const int k = k0 + kk;
+            const int ci = i0 + c, cj = j0 + c;
+            const bool vi = k < n && ci < n && k >= ci, vj = k < n && cj < n && k >= cj;
+            cp_async_elem<sizeof(T)>(&Wi[buf][kk][c], vi ? W + k + (long long)ci * ldw : W, vi);
+            cp_async_elem<sizeof(T)>(&Wj[buf][kk][c], vj ? W + k + (long long)cj * ldw : W, vj);
+        }
+    };
+    if (nch > 0) stage(0, 0);
+    cp_group_commit();
+    for (int ch = 0; ch < nch; ++ch) {
+        if (ch + 1 < nch) stage(ch + 1, (ch + 1) & 1);
+        cp_group_commit();
+        cp_group_wait<1>();
+        __syncthreads();
+        const int buf = ch & 1;
+#pragma unroll
+        for (int kk = 0; kk < CT_KC; ++kk) {
+            T a[4], b[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                a[u] = Wi[buf][kk][ty * 4 + u];
+                b[u] = Wj[buf][kk][tx * 4 + u];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) acc[u][v] = fma_(acc[u][v], a[u], b[v]);
+        }
+        __syncthreads();
+    }
+    cp_group_wait<0>();
+
+    const T* al = alpha_g + m * astride;
+    if constexpr (MODE == 1) {
+        T* g = G + m * gstride;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int i = i0 + ty * 4 + u, j = j0 + tx * 4 + v;
+                if (i < n && j <= i) {
+                    const T ab = T(0.5) * (acc[u][v] - al[i] * al[j]);
+                    g[i + (long long)j * ldg] = ab;
+                    g[j + (long long)i * ldg] = ab;
+                }
+            }
+    } else {
+        const double* th = theta + (long long)m * tstride;
+        const double l = th[0], sf2 = th[1];
+        const double inv2l2 = 0.5 / (l * l), invl3 = 1.0 / (l * l * l);
+        const T* x = X + m * xstride;
+        double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int i = i0 + ty * 4 + u, j = j0 + tx * 4 + v;
+                if (i < n && j <= i) {
+                    const double ab = 0.5 * ((double)acc[u][v] - (double)al[i] * (double)al[j]);
+                    const double w = i == j ? 1.0 : 2.0;
+                    double r2 = 0.0;
+                    for (int c = 0; c < d; ++c) {
+                        const double dx = (double)x[(long long)i * d + c] - (double)x[(long long)j * d + c];
+                        r2 += dx * dx;
+                    }
+                    const double e = exp(-r2 * inv2l2);
+                    g0 += w * ab * sf2 * e * r2 * invl3;  // dA/dl
+                    g1 += w * ab * e;                     // dA/dsigma_f^2
+                    if (i == j) g2 += ab;                 // dA/dsigma^2
+                }
+            }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            g0 += __shfl_xor_sync(0xffffffffu, g0, o);
+            g1 += __shfl_xor_sync(0xffffffffu, g1, o);
+            g2 += __shfl_xor_sync(0xffffffffu, g2, o);
+        }
+        if ((t & 31) == 0) {
+            red[0][t >> 5] = g0;
+            red[1][t >> 5] = g1;
+            red[2][t >> 5] = g2;
+        }
+        __syncthreads();
+        if (t < 3) {
+            double s = 0.0;
+            for (int w = 0; w < CT_NT / 32; ++w) s += red[t][w];
+            partial[((long long)m * gridDim.x + tile) * 3 + t] = s;
+        }
+    }
+}
+
+// out[m] = sum_i x_m[i] y_m[i] in FP64, one CTA per vector
+template <class T>
+__global__ void k_batched_dot(int n, const T* __restrict__ x, long long xs, const T* __restrict__ y, long long ys,
+                              double* __restrict__ out)
+{
+    __shared__ double red[8];
+    const int m = blockIdx.x;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += (double)x[m * xs + i] * (double)y[m * ys + i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r += red[w];
+        out[m] = r;
+    }
+}
+
+// out[m] = 2 sum_i log L_m(i, i) in FP64 (log det of L L^T), one CTA per matrix
+template <class T>
+__global__ void k_batched_logdiag(int n, const T* __restrict__ L, long long ldl, long long ls, double* __restrict__ out)
+{
+    __shared__ double red[8];
+    const int m = blockIdx.x;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += log((double)L[m * ls + i + (long long)i * ldl]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r += red[w];
+        out[m] = 2.0 * r;
+    }
+}
+
+// grad[m][c] = sum over tiles of partial[m][tile][c], in tile order
+__global__ void k_adjoint_reduce(int ntiles, const double* __restrict__ partial, double* __restrict__ grad)
+{
+    const int m = blockIdx.x, c = threadIdx.x;
+    if (c >= 3) return;
+    double s = 0.0;
+    for (int k = 0; k < ntiles; ++k) s += partial[((long long)m * ntiles + k) * 3 + c];
+    grad[(long long)m * 3 + c] = s;
+}
+
+template <class T>
+int gp_build_t(int batch, int n, int d, const void* X, long long xstride, const double* theta, int tstride, void* A,
+               long long lda, long long astride, cudaStream_t st)
+{
+    const int nt = (n + 31) / 32;
+    dim3 grid(nt, nt, batch), block(32, 32);
+    k_gp_build<T><<<grid, block, 0, st>>>(n, d, static_cast<const T*>(X), xstride, theta, tstride, static_cast<T*>(A),
+                                         lda, astride);
+    note_launches(1);
+    return (int)cudaGetLastError();
+}
+
+template <class T>
+int trtri_t(int batch, int n, const void* L, long long ldl, long long lstride, void* W, long long ldw,
+            long long wstride, cudaStream_t st)
+{
+    k_trtri_batched<T><<<batch, TR_NT, 0, st>>>(n, static_cast<const T*>(L), ldl, lstride, static_cast<T*>(W), ldw,
+                                                wstride);
+    note_launches(1);
+    return (int)cudaGetLastError();
+}
+
+template <class T, bool DIRECT>
+int contract_t(int mode, int batch, int n, const void* W, long long ldw, long long wstride, const void* alpha,
+               long long astride, const void* X, int d, long long xstride, const double* theta, int tstride,
+               double* partial, double* grad, void* G, long long ldg, long long gstride, cudaStream_t st)
+{
+    const int nt = (n + CT_TILE - 1) / CT_TILE;
+    const int ntiles = nt * (nt + 1) / 2;
+    dim3 grid(ntiles, batch);
+    if (mode == 0) {
+        k_adjoint_contract<T, 0, DIRECT><<<grid, CT_NT, 0, st>>>(n, static_cast<const T*>(W), ldw, wstride,
+                                                         static_cast<const T*>(alpha), astride,
+                                                         static_cast<const T*>(X), d, xstride, theta, tstride, partial,
+                                                         nullptr, 0, 0);
+        k_adjoint_reduce<<<batch, 32, 0, st>>>(ntiles, partial, grad);
+        note_launches(2);
+    } else {
+        k_adjoint_contract<T, 1, DIRECT><<<grid, CT_NT, 0, st>>>(n, static_cast<const T*>(W), ldw, wstride,
+                                                         static_cast<const T*>(alpha), astride, nullptr, 0, 0,
+                                                         nullptr, 0, nullptr, static_cast<T*>(G), ldg, gstride);
+        note_launches(1);
+    }
+    return (int)cudaGetLastError();
+}
+
+}  // namespace
+}  // namespace ddlak
+
+extern "C" int ddlak_gp_build(char type, int batch, int n, int d, const void* X, long long xstride,
+                              const double* theta, int tstride, void* A, long long lda, long long astride,
+                              void* stream)
+{
+    using namespace ddlak;
+    if (batch <= 0 || n <= 0) return 0;
+    if (d < 1 || d > 16 || !X || !theta || !A || lda < n) return (int)cudaErrorInvalidValue;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    ProfScope ps(PK_ADJOINT, st, 0.0, 0.0);
+    if (type == 'd') return gp_build_t<double>(batch, n, d, X, xstride, theta, tstride, A, lda, astride, st);
+    if (type == 's') return gp_build_t<float>(batch, n, d, X, xstride, theta, tstride, A, lda, astride, st);
+    return (int)cudaErrorInvalidValue;
+}
+
+extern "C" int ddlak_trtri_batched(char type, int batch, int n, const void* L, long long ldl, long long lstride,
+                                   void* W, long long ldw, long long wstride, void* stream)
+{
+    using namespace ddlak;
+    if (batch <= 0 || n <= 0) return 0;
+    if (n > TR_NMAX || !L || !W || ldl < n || ldw < n) return (int)cudaErrorInvalidValue;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const double nn = n;
+    ProfScope ps(PK_ADJOINT, st, batch * nn * nn * nn / 3.0, batch * nn * nn * (type == 'd' ? 8.0 : 4.0));
+    if (type == 'd') return trtri_t<double>(batch, n, L, ldl, lstride, W, ldw, wstride, st);
+    if (type == 's') return trtri_t<float>(batch, n, L, ldl, lstride, W, ldw, wstride, st);
+    return (int)cudaErrorInvalidValue;
+}
+
+extern "C" unsigned long long ddlak_adjoint_partial_bytes(int batch, int n)
+{
+    const unsigned long long nt = (unsigned long long)(n + ddlak::CT_TILE - 1) / ddlak::CT_TILE;
+    return sizeof(double) * 3ull * (unsigned long long)batch * (nt * (nt + 1) / 2);
+}
+
+extern "C" int ddlak_batched_dot(char type, int batch, int n, const void* x, long long xstride, const void* y,
+                                 long long ystride, double* out, void* stream)
+{
+    using namespace ddlak;
+    if (batch <= 0) return 0;
+    if (n < 0 || !out || (n > 0 && (!x || !y))) return (int)cudaErrorInvalidValue;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (type == 'd')
+        k_batched_dot<double><<<batch, 256, 0, st>>>(n, static_cast<const double*>(x), xstride,
+                                                     static_cast<const double*>(y), ystride, out);
+    else if (type == 's')
+        k_batched_dot<float><<<batch, 256, 0, st>>>(n, static_cast<const float*>(x), xstride,
+                                                    static_cast<const float*>(y), ystride, out);
+    else
+        return (int)cudaErrorInvalidValue;
+    note_launches(1);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int ddlak_batched_logdiag(char type, int batch, int n, const void* L, long long ldl, long long lstride,
+                                     double* out, void* stream)
+{
+    using namespace ddlak;
+    if (batch <= 0) return 0;
+    if (n < 0 || !out || (n > 0 && (!L || ldl < n))) return (int)cudaErrorInvalidValue;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (type == 'd')
+        k_batched_logdiag<double><<<batch, 256, 0, st>>>(n, static_cast<const double*>(L), ldl, lstride, out);
+    else if (type == 's')
+        k_batched_logdiag<float><<<batch, 256, 0, st>>>(n, static_cast<const float*>(L), ldl, lstride, out);
+    else
+        return (int)cudaErrorInvalidValue;
+    note_launches(1);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int ddlak_adjoint_contract(char type, int mode, int batch, int n, const void* W, long long ldw,
+                                      long long wstride, const void* alpha, long long astride, const void* X, int d,
+                                      long long xstride, const double* theta, int tstride, double* partial,
+                                      double* grad, void* G, long long ldg, long long gstride, void* stream)
+{
+    using namespace ddlak;
+    if (batch <= 0 || n <= 0) return 0;
+    if (!W || !alpha || ldw < n || mode < 0 || mode > 3) return (int)cudaErrorInvalidValue;
+    if ((mode & 1) == 0 && (!X || d < 1 || d > 16 || !theta || !partial || !grad)) return (int)cudaErrorInvalidValue;
+    if ((mode & 1) == 1 && (!G || ldg < n)) return (int)cudaErrorInvalidValue;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const double nn = n;
+    ProfScope ps(PK_ADJOINT, st, batch * nn * nn * nn / 3.0, 0.0);
+    const bool direct = (mode & 2) != 0;
+    mode &= 1;
+    if (type == 'd')
+        return direct ? contract_t<double, true>(mode, batch, n, W, ldw, wstride, alpha, astride, X, d, xstride, theta,
+                                                 tstride, partial, grad, G, ldg, gstride, st)
+                      : contract_t<double, false>(mode, batch, n, W, ldw, wstride, alpha, astride, X, d, xstride,
+                                                  theta, tstride, partial, grad, G, ldg, gstride, st);
+    if (type == 's')
+        return direct ? contract_t<float, true>(mode, batch, n, W, ldw, wstride, alpha, astride, X, d, xstride, theta,
+                                                tstride, partial, grad, G, ldg, gstride, st)
+                      : contract_t<float, false>(mode, batch, n, W, ldw, wstride, alpha, astride, X, d, xstride,
+                                                 theta, tstride, partial, grad, G, ldg, gstride, st);
+    return (int)cudaErrorInvalidValue;
+}

@@ -16,7 +16,7 @@ from ._c_api import (  # noqa: F401
 from .backend import Backend, Communication, Handle  # noqa: F401
 from .layout import ProcessorLayout  # noqa: F401
 from .matrix import DistributedMatrix  # noqa: F401
-from . import batched  # noqa: F401
+from . import autograd, batched  # noqa: F401
 from .ops import diag_logdet, gather, potrf, pposv, pposv_mixed, ppotrf, ppotrs, scatter  # noqa: F401
 
 

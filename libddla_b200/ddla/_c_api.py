@@ -149,6 +149,10 @@ for _p in "sd":
     _SIGS.update({
         f"ddla_{_p}_posv_vbatched": (_i, [_vp, _c, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i]),
         f"ddla_{_p}_posv_vbatched_plan": (_i, [_vp, _c, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, ctypes.POINTER(_vp)]),
+        f"ddla_{_p}_chol_nll_batched": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
+        f"ddla_{_p}_gp_nll_batched": (_i, [_vp, _i, _i, _i, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
+        f"ddla_{_p}_chol_nll_grad_batched": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp]),
+        f"ddla_{_p}_gp_nll_grad_batched": (_i, [_vp, _i, _i, _i, _vp, _vp, _i, _vp, _vp, _vp, _vp]),
     })
 for _p in "sdcz":
     _SIGS.update({
