@@ -139,13 +139,20 @@ int ddlak_gp_build(char type, int batch, int n, int d, const void* X, long long 
 int ddlak_trtri_batched(char type, int batch, int n, const void* L, long long ldl, long long lstride, void* W,
                         long long ldw, long long wstride, void* stream);
 
+/* W = L^-1 (lower triangle written; above it W is unspecified) for any n: the
+ * fused forward substitution of ddlak_potrs on the identity, generated in the
+ * kernel, skipping its zero blocks.  Scratch: ddlak_potrs_workspace(n, n);
+ * the first int of it is the status word as for ddlak_potrs. */
+int ddlak_trtri_blocked(char type, int n, const void* L, long long ldl, void* W, long long ldw, void* work,
+                        unsigned long long work_bytes, void* stream);
+
 /* out[m] = sum x_m .* y_m, and out[m] = 2 sum log L_m(i,i), in FP64. */
 int ddlak_batched_dot(char type, int batch, int n, const void* x, long long xstride, const void* y,
                       long long ystride, double* out, void* stream);
 int ddlak_batched_logdiag(char type, int batch, int n, const void* L, long long ldl, long long lstride, double* out,
                           void* stream);
 
-/* Adjoint contraction on 64 x 64 lower tiles of A^-1 = W^T W (mode bit 2 set: W
+/* Adjoint contraction on 128 x 128 lower tiles of A^-1 = W^T W (mode bit 2 set: W
  * already holds A^-1).  mode & 1 == 0: grad[m][0..2] = dloss/d{l, sigma_f^2,
  * sigma^2} through per-tile partials (partial: ddlak_adjoint_partial_bytes);
  * mode & 1 == 1: G = 1/2 (A^-1 - alpha alpha^T), dense symmetric. */

@@ -6,7 +6,7 @@
 // log-determinant launch (posvVbatched), the backward a batched W = L^-1 and
 // the tiled (W^T W) contraction with the adjoint epilogue.  Larger orders
 // (batch 1): the blocked factorization (ddlak_potrf), the fused solve, and for
-// the backward A^-1 from the fused solve on the identity, contracted directly.
+// the backward W = L^-1 from the fused forward substitution on the identity.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -45,19 +45,6 @@ void check_theta(const char* routine, int d, const double* theta, int tstride, c
     if (d < 1 || d > 16) throw std::invalid_argument(std::string(routine) + ": point dimension outside [1, 16]");
     if (tstride != 0 && tstride != 3) throw std::invalid_argument(std::string(routine) + ": theta stride must be 0 or 3");
     if (!theta || !X) throw std::invalid_argument(std::string(routine) + ": null points or theta");
-}
-
-// Identity in W (n x n, ld n): zero fill, then ones on the diagonal through a
-// strided 2-D copy (destination pitch n+1 elements).
-template <class T>
-void set_identity(const DdlaHandle_t& h, T* W, int n)
-{
-    cudaStream_t st = h->stream;
-    detail::cuda_check(cudaMemsetAsync(W, 0, sizeof(T) * (size_t)n * n, st), "identity");
-    const std::vector<T> ones(n, T(1));
-    detail::cuda_check(cudaMemcpy2DAsync(W, sizeof(T) * ((size_t)n + 1), ones.data(), sizeof(T), sizeof(T), n,
-                                         cudaMemcpyHostToDevice, st),
-                       "identity");
 }
 
 template <class T>
@@ -109,21 +96,20 @@ void factor_solve(const DdlaHandle_t& h, int batch, int n, T* A, const T* y, T* 
     ck(ddlak_batched_dot(tcode<T>(), batch, n, y, n, alpha, n, quad, st), "y^T alpha");
 }
 
-// A^-1 tile source: W = L^-1 (batched) or A^-1 itself (large order); returns the contraction's direct bit.
+// W = L^-1 for the (W^T W) contraction: one CTA per matrix up to order 1024,
+// the fused forward substitution on the identity above.
 template <class T>
-int inverse_operand(const DdlaHandle_t& h, int batch, int n, const T* L, T* W, detail::DeviceScratch*& solve_ws)
+void inverse_factor(const DdlaHandle_t& h, int batch, int n, const T* L, T* W)
 {
     cudaStream_t st = h->stream;
     const long long nn = (long long)n * n;
     if (n <= kBatchedMaxOrder) {
         ck(ddlak_trtri_batched(tcode<T>(), batch, n, L, n, nn, W, n, nn, st), "L^-1");
-        return 0;
+        return;
     }
-    set_identity(h, W, n);
     const size_t sb = ddlak_potrs_workspace(n, n);
-    solve_ws = new detail::DeviceScratch(h, sb);
-    ck(ddlak_potrs(tcode<T>(), 'L', 'L', n, n, L, n, W, n, solve_ws->data(), sb, st), "A^-1");
-    return 2;
+    detail::DeviceScratch ws(h, sb);
+    ck(ddlak_trtri_blocked(tcode<T>(), n, L, n, W, n, ws.data(), sb, st), "L^-1");
 }
 
 }  // namespace
@@ -158,13 +144,11 @@ void cholNllGradBatched(const DdlaHandle_t& h, int batch, int n, const T* L, con
     check_shape(h, "cholNllGradBatched", batch, n);
     if (batch == 0 || n == 0) return;
     if (!L || !alpha || !W || !G) throw std::invalid_argument("cholNllGradBatched: null array");
-    detail::DeviceScratch* sws = nullptr;
-    const int direct = inverse_operand<T>(h, batch, n, L, W, sws);
+    inverse_factor<T>(h, batch, n, L, W);
     const long long nn = (long long)n * n;
-    const int e = ddlak_adjoint_contract(tcode<T>(), 1 | direct, batch, n, W, n, nn, alpha, n, nullptr, 0, 0, nullptr,
-                                         0, nullptr, nullptr, G, n, nn, h->stream);
-    delete sws;
-    ck(e, "adjoint");
+    ck(ddlak_adjoint_contract(tcode<T>(), 1, batch, n, W, n, nn, alpha, n, nullptr, 0, 0, nullptr, 0, nullptr,
+                              nullptr, G, n, nn, h->stream),
+       "adjoint");
 }
 
 template <typename T>
@@ -175,15 +159,12 @@ void gpNllGradBatched(const DdlaHandle_t& h, int batch, int n, int d, const T* X
     if (batch == 0 || n == 0) return;
     check_theta("gpNllGradBatched", d, theta, tstride, X);
     if (!L || !alpha || !W || !grad) throw std::invalid_argument("gpNllGradBatched: null array");
-    detail::DeviceScratch* sws = nullptr;
-    const int direct = inverse_operand<T>(h, batch, n, L, W, sws);
+    inverse_factor<T>(h, batch, n, L, W);
     detail::DeviceScratch part(h, ddlak_adjoint_partial_bytes(batch, n));
     const long long nn = (long long)n * n;
-    const int e = ddlak_adjoint_contract(tcode<T>(), 0 | direct, batch, n, W, n, nn, alpha, n, X, d, (long long)n * d,
-                                         theta, tstride, reinterpret_cast<double*>(part.data()), grad, nullptr, 0, 0,
-                                         h->stream);
-    delete sws;
-    ck(e, "adjoint");
+    ck(ddlak_adjoint_contract(tcode<T>(), 0, batch, n, W, n, nn, alpha, n, X, d, (long long)n * d, theta, tstride,
+                              reinterpret_cast<double*>(part.data()), grad, nullptr, 0, 0, h->stream),
+       "adjoint");
 }
 
 #define DDLA_GP_INST(T)                                                                                             \

@@ -11,7 +11,7 @@
 //                     them against the 32 x 32 diagonal block of L (a few columns
 //                     each, shuffles), and every thread updates the rows it owns
 //                     below from registers;
-//   k_adjoint_contract  (W^T W) tile by tile (64 x 64 lower tiles, k from the tile's
+//   k_adjoint_contract  (W^T W) tile by tile (128 x 128 lower tiles, k from the tile's
 //                     first row: W is lower triangular) with a fused epilogue that
 //                     either contracts Abar with dA/dtheta (recomputed from the
 //                     points, never stored) into per-tile partial sums, or writes
@@ -19,6 +19,8 @@
 //   k_adjoint_reduce  per-matrix sums of the partials in a fixed order (deterministic);
 //   k_batched_dot     y^T alpha per problem (FP64 accumulation).
 #include <cuda_runtime.h>
+
+#include <type_traits>
 
 #include <ddla_kernels.h>
 
@@ -28,10 +30,11 @@
 namespace ddlak {
 namespace {
 
-constexpr int TR_NT = 256;
+constexpr int TR_NT = 512;
 constexpr int TR_NMAX = 1024;
-constexpr int CT_TILE = 64;
-constexpr int CT_KC = 16;
+constexpr int CT_TILE = 128;
+// k-chunk of the contraction: 32 KB of static shared memory for both types
+template <class T> constexpr int ct_kc() { return 64 / (int)sizeof(T); }
 constexpr int CT_NT = 256;
 
 // ---------------------------------------------------------------------------
@@ -76,8 +79,10 @@ __global__ void __launch_bounds__(TR_NT, 1)
     constexpr int B = TrWidth<T>::B;
     constexpr int RPT = TR_NMAX / TR_NT;
     constexpr int CPW = B / (TR_NT / 32);  // columns each warp solves
-    __shared__ T Xs[2][32][B + 1];
+    __shared__ T Xs[2][32][B + 1];                  // staged rows, then the solved block (padded)
+    __shared__ __align__(16) T Xr[2][32][B];        // the solved block, row-major for 128-bit broadcast reads
     __shared__ T Ls[2][32][33];
+    __shared__ T Ri[2][32];  // reciprocal pivots of the staged diagonal block
     const T* L = Lg + blockIdx.x * lstride;
     T* W = Wg + blockIdx.x * wstride;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -105,6 +110,7 @@ __global__ void __launch_bounds__(TR_NT, 1)
                     const int r = e & 31, c = e >> 5;
                     Ls[buf][r][c] = (c <= r && I + r < n) ? L[(I + r) + (long long)(I + c) * ldl] : T(0);
                 }
+                if (t < 32) Ri[buf][t] = I + t < n ? T(1) / L[(I + t) + (long long)(I + t) * ldl] : T(0);
                 __syncthreads();
                 // 2. X_I = L_II^-1 Xs: warp w solves columns w*CPW .. w*CPW+CPW-1, lane = row
                 {
@@ -114,11 +120,11 @@ __global__ void __launch_bounds__(TR_NT, 1)
                     const bool live = I + lane < n;
 #pragma unroll 4
                     for (int k = 0; k < 32; ++k) {
-                        const T dkk = Ls[buf][k][k];
+                        const T rk = Ri[buf][k];
                         const T lk = Ls[buf][lane][k];
 #pragma unroll
                         for (int c = 0; c < CPW; ++c) {
-                            if (lane == k) x[c] = live ? x[c] / dkk : T(0);
+                            if (lane == k) x[c] = live ? x[c] * rk : T(0);
                             const T xk = __shfl_sync(0xffffffffu, x[c], k);
                             if (lane > k) x[c] = fms(x[c], lk, xk);
                         }
@@ -126,23 +132,52 @@ __global__ void __launch_bounds__(TR_NT, 1)
 #pragma unroll
                     for (int c = 0; c < CPW; ++c) {
                         const int q = warp * CPW + c;
-                        Xs[buf][lane][q] = x[c];
+                        Xr[buf][lane][q] = x[c];
                         if (live && q < nb && I + lane >= J + q) W[(I + lane) + (long long)(J + q) * ldw] = x[c];
                     }
                 }
                 __syncthreads();
-                // 3. rows below the block: acc -= L(i, I:I+32) X_I
+                // 3. rows below the block: acc -= L(i, I:I+32) X_I, four columns of L
+                // at a time (loads in flight together), rows of X_I as 128-bit broadcasts
+                bool act[RPT];
 #pragma unroll
                 for (int r = 0; r < RPT; ++r) {
-                    if (r < rb) continue;
                     const int i = t + r * TR_NT;
-                    if (i < I + 32 || i >= n) continue;
-                    const T* li = L + i + (long long)I * ldl;
-#pragma unroll 4
-                    for (int k = 0; k < 32; ++k) {
-                        const T l = li[(long long)k * ldl];
+                    act[r] = r >= rb && i >= I + 32 && i < n;
+                }
+                constexpr int VW = 16 / sizeof(T);
+                using V = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+                constexpr int KL = 4;  // columns of L loaded together
+                for (int k0 = 0; k0 < 32; k0 += KL) {
+                    T lv[RPT][KL];
 #pragma unroll
-                        for (int q = 0; q < B; ++q) acc[r][q] = fms(acc[r][q], l, Xs[buf][k][q]);
+                    for (int r = 0; r < RPT; ++r) {
+                        const T* li = L + (t + r * TR_NT) + (long long)(I + k0) * ldl;
+#pragma unroll
+                        for (int kk = 0; kk < KL; ++kk) lv[r][kk] = act[r] ? li[(long long)kk * ldl] : T(0);
+                    }
+#pragma unroll
+                    for (int kk = 0; kk < KL; ++kk) {
+                        T xr[B];
+                        const V* src = reinterpret_cast<const V*>(&Xr[buf][k0 + kk][0]);
+#pragma unroll
+                        for (int v = 0; v < B / VW; ++v) {
+                            const V w = src[v];
+                            if constexpr (VW == 2) {
+                                xr[2 * v] = w.x;
+                                xr[2 * v + 1] = w.y;
+                            } else {
+                                xr[4 * v] = w.x;
+                                xr[4 * v + 1] = w.y;
+                                xr[4 * v + 2] = w.z;
+                                xr[4 * v + 3] = w.w;
+                            }
+                        }
+#pragma unroll
+                        for (int r = 0; r < RPT; ++r)
+                            if (act[r])
+#pragma unroll
+                                for (int q = 0; q < B; ++q) acc[r][q] = fms(acc[r][q], lv[r][kk], xr[q]);
                     }
                 }
             }
@@ -151,7 +186,7 @@ __global__ void __launch_bounds__(TR_NT, 1)
 }
 
 // ---------------------------------------------------------------------------
-// (W^T W) on 64 x 64 lower tiles with the adjoint epilogue.
+// (W^T W) on 128 x 128 lower tiles with the adjoint epilogue.
 //   mode 0: partial[m][tile][0..2] = sum over the tile's i >= j of
 //           w_ij Abar_ij dA_ij/d{l, sigma_f^2, sigma^2}, w = 2 off the diagonal;
 //   mode 1: G[i + j ldg] = G[j + i ldg] = Abar_ij (dense symmetric gradient).
@@ -169,14 +204,17 @@ __device__ __forceinline__ void tile_of_lower(int t, int& ti, int& tj)
 }
 
 template <class T, int MODE, bool DIRECT>
-__global__ void __launch_bounds__(CT_NT)
+__global__ void __launch_bounds__(CT_NT, 1)
     k_adjoint_contract(int n, const T* __restrict__ Wg, long long ldw, long long wstride,
                        const T* __restrict__ alpha_g, long long astride, const T* __restrict__ X, int d,
                        long long xstride, const double* __restrict__ theta, int tstride, double* __restrict__ partial,
                        T* __restrict__ G, long long ldg, long long gstride)
 {
-    __shared__ T Wi[2][CT_KC][CT_TILE];
-    __shared__ T Wj[2][CT_KC][CT_TILE];
+    // thread (ty, tx) of 16 x 16 owns rows i0 + {ty*4 .. +3, 64 + ty*4 .. +3} and the
+    // same pattern of columns: the k-loop reads them as 4-element runs (conflict free)
+    constexpr int CT_KC = ct_kc<T>();
+    __shared__ __align__(16) T Wi[2][CT_KC][CT_TILE];
+    __shared__ __align__(16) T Wj[2][CT_KC][CT_TILE];
     __shared__ double red[3][CT_NT / 32];
     const int m = blockIdx.y;
     const int tile = blockIdx.x;
@@ -185,20 +223,22 @@ __global__ void __launch_bounds__(CT_NT)
     const int i0 = ti * CT_TILE, j0 = tj * CT_TILE;
     const T* W = Wg + m * wstride;
     const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
-    T acc[4][4];
+    auto row_of = [&](int u) { return (u < 4 ? ty * 4 + u : 64 + ty * 4 + (u - 4)); };
+    auto col_of = [&](int v) { return (v < 4 ? tx * 4 + v : 64 + tx * 4 + (v - 4)); };
+    T acc[8][8];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < 8; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
+        for (int b = 0; b < 8; ++b) acc[a][b] = T(0);
     // k runs over [i0, n): W(k, i) = 0 for k < i.  DIRECT: Wg holds A^-1 itself.
     const int kbeg = i0, nk = n - kbeg;
     const int nch = DIRECT ? 0 : (nk + CT_KC - 1) / CT_KC;
     if constexpr (DIRECT) {
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < 8; ++u)
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const int i = i0 + ty * 4 + u, j = j0 + tx * 4 + v;
+            for (int v = 0; v < 8; ++v) {
+                const int i = i0 + row_of(u), j = j0 + col_of(v);
                 if (i < n && j <= i) acc[u][v] = W[i + (long long)j * ldw];
             }
     }
@@ -215,6 +255,23 @@ __global__ void __launch_bounds__(CT_NT)
     };
     if (nch > 0) stage(0, 0);
     cp_group_commit();
+    constexpr int VW = 16 / sizeof(T);
+    using V = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+    auto ld4 = [&](const T* p, T* out) {
+#pragma unroll
+        for (int h = 0; h < 4 / VW; ++h) {
+            const V w = reinterpret_cast<const V*>(p)[h];
+            if constexpr (VW == 2) {
+                out[2 * h] = w.x;
+                out[2 * h + 1] = w.y;
+            } else {
+                out[0] = w.x;
+                out[1] = w.y;
+                out[2] = w.z;
+                out[3] = w.w;
+            }
+        }
+    };
     for (int ch = 0; ch < nch; ++ch) {
         if (ch + 1 < nch) stage(ch + 1, (ch + 1) & 1);
         cp_group_commit();
@@ -223,16 +280,15 @@ __global__ void __launch_bounds__(CT_NT)
         const int buf = ch & 1;
 #pragma unroll
         for (int kk = 0; kk < CT_KC; ++kk) {
-            T a[4], b[4];
+            T a[8], b[8];
+            ld4(&Wi[buf][kk][ty * 4], a);
+            ld4(&Wi[buf][kk][64 + ty * 4], a + 4);
+            ld4(&Wj[buf][kk][tx * 4], b);
+            ld4(&Wj[buf][kk][64 + tx * 4], b + 4);
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                a[u] = Wi[buf][kk][ty * 4 + u];
-                b[u] = Wj[buf][kk][tx * 4 + u];
-            }
+            for (int u = 0; u < 8; ++u)
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-                for (int v = 0; v < 4; ++v) acc[u][v] = fma_(acc[u][v], a[u], b[v]);
+                for (int v = 0; v < 8; ++v) acc[u][v] = fma_(acc[u][v], a[u], b[v]);
         }
         __syncthreads();
     }
@@ -242,10 +298,10 @@ __global__ void __launch_bounds__(CT_NT)
     if constexpr (MODE == 1) {
         T* g = G + m * gstride;
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < 8; ++u)
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const int i = i0 + ty * 4 + u, j = j0 + tx * 4 + v;
+            for (int v = 0; v < 8; ++v) {
+                const int i = i0 + row_of(u), j = j0 + col_of(v);
                 if (i < n && j <= i) {
                     const T ab = T(0.5) * (acc[u][v] - al[i] * al[j]);
                     g[i + (long long)j * ldg] = ab;
@@ -259,12 +315,15 @@ __global__ void __launch_bounds__(CT_NT)
         const T* x = X + m * xstride;
         double g0 = 0.0, g1 = 0.0, g2 = 0.0;
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < 8; ++u) {
+            const int i = i0 + row_of(u);
+            if (i >= n) continue;
+            const double ai = (double)al[i];
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const int i = i0 + ty * 4 + u, j = j0 + tx * 4 + v;
-                if (i < n && j <= i) {
-                    const double ab = 0.5 * ((double)acc[u][v] - (double)al[i] * (double)al[j]);
+            for (int v = 0; v < 8; ++v) {
+                const int j = j0 + col_of(v);
+                if (j <= i) {
+                    const double ab = 0.5 * ((double)acc[u][v] - ai * (double)al[j]);
                     const double w = i == j ? 1.0 : 2.0;
                     double r2 = 0.0;
                     for (int c = 0; c < d; ++c) {
@@ -277,6 +336,7 @@ __global__ void __launch_bounds__(CT_NT)
                     if (i == j) g2 += ab;                 // dA/dsigma^2
                 }
             }
+        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             g0 += __shfl_xor_sync(0xffffffffu, g0, o);
@@ -290,9 +350,9 @@ __global__ void __launch_bounds__(CT_NT)
         }
         __syncthreads();
         if (t < 3) {
-            double s = 0.0;
-            for (int w = 0; w < CT_NT / 32; ++w) s += red[t][w];
-            partial[((long long)m * gridDim.x + tile) * 3 + t] = s;
+            double sum = 0.0;
+            for (int w = 0; w < CT_NT / 32; ++w) sum += red[t][w];
+            partial[((long long)m * gridDim.x + tile) * 3 + t] = sum;
         }
     }
 }

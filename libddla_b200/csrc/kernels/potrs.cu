@@ -96,7 +96,10 @@ __device__ __forceinline__ TX widen(TL v)
 // INV: the diagonal step multiplies by Dinv (TX, one RB x RB column-major block per
 // block row, entries (r, c) of inv(L_bb), zero outside the block) instead of
 // substituting; for the repeated solves of the refinement with one factor.
-template <class TL, class TX, bool UP, bool BT, bool INV = false>
+// ID: forward substitution only, on the identity (generated in place of B's
+// initial values): X = L^-1.  Chunk c's columns start at row c*RC, so block
+// rows above that one are zero and are neither computed nor waited for.
+template <class TL, class TX, bool UP, bool BT, bool INV = false, bool ID = false>
 __global__ void __launch_bounds__(NT) k_potrs_fused(const TL* __restrict__ A, long long lda, TX* B, long long ldb,
                                                     int n, int nrhs, int nchunks, int* flags, int* ticket,
                                                     int* status, const TX* __restrict__ Dinv)
@@ -118,11 +121,13 @@ __global__ void __launch_bounds__(NT) k_potrs_fused(const TL* __restrict__ A, lo
     const int t = s_t;
     const int chunk = t % nchunks;
     const int step = t / nchunks;
-    const bool fwd = step < N;
-    const int blk = fwd ? step : 2 * N - 1 - step;
+    const bool fwd = ID || step < N;
+    const int blk = ID ? step : (fwd ? step : 2 * N - 1 - step);
     int* cflags = flags + (size_t)chunk * 2 * N;  // [0,N) forward, [N,2N) backward
     const long long r0 = (long long)chunk * RC;
     const int nr = (int)((nrhs - r0) < RC ? (nrhs - r0) : RC);
+    const int jfirst = ID ? (int)(r0 / RB) : 0;  // first block row with a nonzero right-hand side
+    if (ID && blk < jfirst) return;
     const long long i0 = (long long)blk * RB;
     const int nrows = (int)((n - i0) < RB ? (n - i0) : RB);
     // raw tile element (i, k): A[(i0+i) + (j0+k)*lda] when p1, A[(j0+k) + (i0+i)*lda] otherwise;
@@ -135,8 +140,8 @@ __global__ void __launch_bounds__(NT) k_potrs_fused(const TL* __restrict__ A, lo
 
     // Visit the other block rows in publication order (forward 0, 1, ..; backward N-1, N-2, ..):
     // every wait but the last one is already satisfied when reached.
-    const int nvisit = fwd ? blk : N - 1 - blk;
-    auto visit = [&](int v) { return fwd ? v : N - 1 - v; };
+    const int nvisit = ID ? blk - jfirst : (fwd ? blk : N - 1 - blk);
+    auto visit = [&](int v) { return ID ? jfirst + v : (fwd ? v : N - 1 - v); };
     auto issue_tile = [&](int j, int buf) {
         const long long j0 = (long long)j * RB;
         const int ncols = (int)((n - j0) < RB ? (n - j0) : RB);
@@ -186,7 +191,10 @@ __global__ void __launch_bounds__(NT) k_potrs_fused(const TL* __restrict__ A, lo
 #pragma unroll
     for (int q = 0; q < RC / 4; ++q) {
         const int r = tg + 4 * q;
-        acc[q] = (tr < nrows && r < nr) ? x_ld_cg<T, BT>(B, ldb, i0 + tr, r0 + r) : zero<T>();
+        if constexpr (ID)
+            acc[q] = (tr < nrows && r < nr && i0 + tr == r0 + r) ? from_real<T>(R(1)) : zero<T>();
+        else
+            acc[q] = (tr < nrows && r < nr) ? x_ld_cg<T, BT>(B, ldb, i0 + tr, r0 + r) : zero<T>();
     }
 
     for (int v = 0; v < nvisit; ++v) {
@@ -329,26 +337,26 @@ __global__ void __launch_bounds__(NT) k_potrs_fused(const TL* __restrict__ A, lo
     if (threadIdx.x == 0) st_release(&cflags[fwd ? blk : N + blk], 1);
 }
 
-template <class T, bool UP, bool BT, class TL = T, bool INV = false>
+template <class T, bool UP, bool BT, class TL = T, bool INV = false, bool ID = false>
 cudaError_t potrs_launch(const TL* A, long long lda, T* B, long long ldb, int n, int nrhs, int* flags, int* ticket,
                          int* status, cudaStream_t st, const T* Dinv = nullptr)
 {
     const int N = (int)ceil_div(n, RB);
     const int nchunks = (int)ceil_div(nrhs, RC);
-    const long long grid = 2LL * N * nchunks;
+    const long long grid = (ID ? 1LL : 2LL) * N * nchunks;
     const size_t smem = potrs_smem_bytes<TL, T, INV>();
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_potrs_fused<TL, T, UP, BT, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_potrs_fused<TL, T, UP, BT, INV, ID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
         attr = true;
     }
     const double cf = Traits<T>::cplx ? 4.0 : 1.0;
     const double nd = n, rd = nrhs;
-    ProfScope ps(PK_POTRS_FUSED, st, cf * 2.0 * nd * nd * rd,
+    ProfScope ps(PK_POTRS_FUSED, st, ID ? cf * nd * nd * nd / 3.0 : cf * 2.0 * nd * nd * rd,
                  sizeof(TL) * nd * (nd + 1) + sizeof(T) * 4.0 * nd * rd);
-    k_potrs_fused<TL, T, UP, BT, INV><<<(unsigned)grid, NT, smem, st>>>(A, lda, B, ldb, n, nrhs, nchunks, flags,
-                                                                         ticket, status, Dinv);
+    k_potrs_fused<TL, T, UP, BT, INV, ID><<<(unsigned)grid, NT, smem, st>>>(A, lda, B, ldb, n, nrhs, nchunks, flags,
+                                                                             ticket, status, Dinv);
     note_launches(1);
     return cudaGetLastError();
 }
@@ -562,4 +570,26 @@ extern "C" int ddlak_potrs(char type, char uplo, char side, int n, int nrhs, con
     int* ticket = status + 1;
     int* flags = reinterpret_cast<int*>(static_cast<char*>(work) + 256);
     return (int)potrs_dispatch(type, uplo, side, n, nrhs, A, lda, B, ldb, flags, ticket, status, st);
+}
+
+// W = L^-1 for a lower factor: the fused forward substitution on the identity.
+extern "C" int ddlak_trtri_blocked(char type, int n, const void* L, long long ldl, void* W, long long ldw, void* work,
+                                   unsigned long long work_bytes, void* stream)
+{
+    using namespace ddlak;
+    if (n <= 0) return 0;
+    if (!L || !W || ldl < n || ldw < n || work_bytes < ddlak_potrs_workspace(n, n)) return (int)cudaErrorInvalidValue;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(work, 0, ddlak_potrs_workspace(n, n), st);
+    if (e != cudaSuccess) return (int)e;
+    int* status = static_cast<int*>(work);
+    int* ticket = status + 1;
+    int* flags = reinterpret_cast<int*>(static_cast<char*>(work) + 256);
+    if (type == 'd')
+        return (int)potrs_launch<double, false, false, double, false, true>(
+            static_cast<const double*>(L), ldl, static_cast<double*>(W), ldw, n, n, flags, ticket, status, st);
+    if (type == 's')
+        return (int)potrs_launch<float, false, false, float, false, true>(
+            static_cast<const float*>(L), ldl, static_cast<float*>(W), ldw, n, n, flags, ticket, status, st);
+    return (int)cudaErrorInvalidValue;
 }

@@ -49,12 +49,12 @@ def _handle_stream(handle):
 
 class _OnHandleStream:
     """Orders the handle's stream after torch's current stream on entry and
-    torch's after the handle's on exit; tensors touched by the library are
-    recorded on the handle's stream for the caching allocator."""
+    torch's after the handle's on exit.  The tensors are allocated on torch's
+    stream, which waits for the library's work before anything that follows,
+    so the caching allocator cannot hand their memory out while it is in use."""
 
     def __init__(self, handle, *tensors):
         self.handle = handle
-        self.tensors = [t for t in tensors if t is not None]
 
     def __enter__(self):
         torch = _torch()
@@ -64,8 +64,6 @@ class _OnHandleStream:
         return self
 
     def __exit__(self, *exc):
-        for t in self.tensors:
-            t.record_stream(self.hs)
         self.cur.wait_stream(self.hs)
 
 
