@@ -2,6 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--n 32768] [--nrhs 8] [--kappa 1e6] [--no-cpu] [--no-plain]
+                    [--no-batched] [--no-gp] [--no-gp-large] [--batched-count 4096]
 
 Workload: solve A X = B to FP64 accuracy for a double n x n SPD matrix
 A = U diag(s) U^T (U = product of 4 Householder reflectors with N(0,1)
@@ -13,6 +14,13 @@ uplo 'L'.  One step = one solve.  Two paths are timed:
   plain    : ddla_d_pposv (FP64 factor on the FP64 tensor cores + fused solve).
 TFLOP/s use the FP64 factor+solve count n^3/3 + 2 n^2 nrhs for both paths.
 The 8.6 GB matrix is larger than the 126 MB L2, so no L2 flush is needed.
+
+Two secondary figures ride on the same JSON line: "batched" (4096 uneven SPD
+matrices, n_i in [16, 512], factor + solve + log-determinant in one persistent
+graph-replayed launch, matrices/s, against a per-matrix loop of the plain
+path) and "gp" (256 Gaussian-process likelihoods of order 1024 with their
+hyperparameter gradients through the adjoint kernels, evaluations/s, against
+a per-matrix torch.linalg loop and torch's batched path).
 
 Device timing: CUDA events on the library handle's stream around each call,
 summed over the K steps; the plain path restores A from a pristine copy
@@ -218,6 +226,191 @@ def read_kernels(C):
     return out
 
 
+# ---------------------------------------------------------------------------
+# secondary legs: batched uneven SPD (factor+solve+logdet) and the GP likelihood
+# ---------------------------------------------------------------------------
+def batched_leg(args, torch, device, h, stream, C):
+    """4096 matrices, n_i uniform in [16, 512], A_i = G_i G_i^T / n_i + 0.1 I, b_i ~ N(0, 1):
+    one persistent launch replayed from a CUDA graph (VbatchedPlan) vs a per-matrix loop
+    of the plain path (ddla.pposv + ddla.diag_logdet) on a sample of the same matrices."""
+    from libddla_b200 import ddla
+    from libddla_b200.ddla import batched
+
+    out = {}
+    count = args.batched_count
+    g = torch.Generator(device=device).manual_seed(0xDD1A0004)
+    orders = np.random.default_rng(0xDD1A0004).integers(16, 513, size=count)
+    for tname, dt, code in (("f64", torch.float64, "d"), ("f32", torch.float32, "s")):
+        es = 8 if dt == torch.float64 else 4
+        sizes = (orders.astype(np.int64) ** 2 + 31) // 32 * 32
+        aoff = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+        voff = np.concatenate([[0], np.cumsum((orders.astype(np.int64) + 31) // 32 * 32)[:-1]])
+        mats = torch.zeros(int(sizes.sum()), dtype=dt, device=device)
+        rhs = torch.zeros(int(voff[-1] + 512), dtype=dt, device=device)
+        for nv in np.unique(orders):
+            idx = np.nonzero(orders == nv)[0]
+            G = torch.randn(len(idx), nv, nv, generator=g, device=device, dtype=torch.float64)
+            M = (G @ G.transpose(1, 2) / nv + 0.1 * torch.eye(nv, device=device, dtype=torch.float64)).to(dt)
+            for k, i in enumerate(idx):
+                mats[aoff[i]:aoff[i] + nv * nv] = M[k].reshape(-1)
+                rhs[voff[i]:voff[i] + nv] = torch.randn(nv, generator=g, device=device, dtype=torch.float64).to(dt)
+        pb = batched.PackedBatch(
+            dtype=np.dtype(np.float64 if dt == torch.float64 else np.float32), orders=orders.astype(np.int32),
+            a_offsets=aoff, b_offsets=voff, mats=mats, rhs=rhs,
+            d_n=torch.from_numpy(orders.astype(np.int32)).to(device),
+            d_lda=torch.from_numpy(orders.astype(np.int32)).to(device),
+            d_A=torch.from_numpy((mats.data_ptr() + aoff * es).astype(np.int64)).to(device),
+            d_B=torch.from_numpy((rhs.data_ptr() + voff * es).astype(np.int64)).to(device),
+            logdet=torch.zeros(count, dtype=torch.float64, device=device),
+            info=torch.zeros(count, dtype=torch.int32, device=device), max_n=512)
+        A0, B0 = mats.clone(), rhs.clone()
+        batched.autotune(h, code, 512)
+        plan = batched.VbatchedPlan(h, pb)
+        flops = plan.info()["flops"]
+
+        def restore():
+            with torch.cuda.stream(stream):
+                mats.copy_(A0)
+                rhs.copy_(B0)
+
+        for _ in range(args.warmup):
+            restore()
+            plan.run()
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(args.steps):
+            restore()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            plan.run()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        ms = statistics.median(times)
+        bad = int((pb.info != 0).sum())
+        plan.close()
+        # per-matrix loop of the plain path (device-resident inputs), on a sample
+        rs = np.random.default_rng(5)
+        sample = rs.choice(count, size=min(64, count), replace=False)
+        dev = []
+        for i in sample:
+            nv = int(orders[i])
+            Ai = A0[aoff[i]:aoff[i] + nv * nv].clone()
+            bi = B0[voff[i]:voff[i] + nv].clone()
+            dev.append((Ai, bi, ddla.DistributedMatrix.wrap(h, Ai.data_ptr(), nv, nv, nv, pb.dtype, mb=256, nb=256),
+                        ddla.DistributedMatrix.wrap(h, bi.data_ptr(), nv, 1, nv, pb.dtype, mb=256, nb=256)))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _, _, dA, dB in dev:
+            ddla.pposv(dA, dB)
+            ddla.diag_logdet(dA)
+        torch.cuda.synchronize()
+        loop_rate = len(dev) / (time.perf_counter() - t0)
+        rate = count / (ms * 1e-3)
+        out[tname] = {"value": rate, "unit": "matrices/s", "ms_per_step": ms, "tflops": flops / (ms * 1e-3) / 1e12,
+                      "failed": bad, "loop_value": loop_rate, "vs_loop": rate / loop_rate,
+                      "tuning": batched.tuning(h, code, 512)["variant"]}
+        del mats, rhs, A0, B0, pb, dev
+    return {"metric": "batched factor+solve+logdet matrices/s", "unit": "matrices/s",
+            "config": {"workload": f"{count} SPD matrices n_i ~ U[16,512], A_i = G_i G_i^T/n_i + 0.1 I, one rhs",
+                       "launch": "one persistent kernel per step, replayed from a CUDA graph",
+                       "loop": "per-matrix ddla.pposv + ddla.diag_logdet (plain path, device-resident), 64-matrix "
+                               "sample", "l2": "3 GB of matrices > 126 MB L2"},
+            **out}
+
+
+def gp_leg(args, torch, device):
+    """Batch of 256 GP likelihoods n=1024 (FP64), SE kernel on points in [0,1]^2, l=0.3,
+    sigma^2=1e-2: loss and dloss/dtheta per step through libddla_b200.ddla.autograd; against a
+    per-matrix torch.linalg (cuSOLVER) loop and torch's batched path.  Plus one n=16384 FP32."""
+    from libddla_b200.ddla import autograd as ag
+
+    g = torch.Generator(device=device).manual_seed(0xDD1A0005)
+    B, n = 256, 1024
+    X = torch.rand(B, n, 2, generator=g, device=device, dtype=torch.float64)
+    y = torch.randn(B, n, generator=g, device=device, dtype=torch.float64)
+    th = torch.tensor([0.3, 1.0, 1e-2], dtype=torch.float64, device=device, requires_grad=True)
+
+    def ours():
+        th.grad = None
+        loss = ag.gp_nll(X, y, th).sum()
+        loss.backward()
+        return loss
+
+    def se(Xb, t):
+        r2 = ((Xb[:, :, None, :] - Xb[:, None, :, :]) ** 2).sum(-1)
+        return t[1] * torch.exp(-r2 / (2 * t[0] ** 2)) + t[2] * torch.eye(Xb.shape[1], dtype=Xb.dtype, device=device)
+
+    def ref_one(b, t):
+        L = torch.linalg.cholesky(se(X[b:b + 1], t)[0])
+        a = torch.cholesky_solve(y[b].unsqueeze(-1), L).squeeze(-1)
+        return 0.5 * ((y[b] * a).sum() + 2 * torch.log(torch.diagonal(L)).sum())
+
+    def timed(fn, reps):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    ms = timed(ours, args.steps)
+    grad = th.grad.clone()
+    # torch reference gradient (FP64 autograd, batched) for the error line
+    t2 = th.detach().clone().requires_grad_(True)
+    K = se(X, t2)
+    L = torch.linalg.cholesky(K)
+    a = torch.cholesky_solve(y.unsqueeze(-1), L).squeeze(-1)
+    (0.5 * ((y * a).sum(-1) + 2 * torch.log(torch.diagonal(L, dim1=-2, dim2=-1)).sum(-1))).sum().backward()
+    rel = float(((grad - t2.grad).abs().max() / t2.grad.abs().max()).item())
+    del K, L, a
+
+    def torch_batched():
+        t = th.detach().clone().requires_grad_(True)
+        K = se(X, t)
+        Lb = torch.linalg.cholesky(K)
+        ab = torch.cholesky_solve(y.unsqueeze(-1), Lb).squeeze(-1)
+        (0.5 * ((y * ab).sum(-1) + 2 * torch.log(torch.diagonal(Lb, dim1=-2, dim2=-1)).sum(-1))).sum().backward()
+
+    tb = timed(torch_batched, 2)
+    nloop = 32
+
+    def torch_loop():
+        t = th.detach().clone().requires_grad_(True)
+        tot = sum(ref_one(b, t) for b in range(nloop))
+        tot.backward()
+
+    tl = timed(torch_loop, 2)
+    rate = B / (ms * 1e-3)
+    loop_rate = nloop / (tl * 1e-3)
+    # one large float32 problem (blocked kernels)
+    n2 = 16384
+    X2 = torch.rand(1, n2, 2, generator=g, device=device, dtype=torch.float32)
+    y2 = torch.randn(1, n2, generator=g, device=device, dtype=torch.float32)
+    th2 = torch.tensor([0.3, 1.0, 1e-2], dtype=torch.float64, device=device, requires_grad=True)
+
+    def big():
+        th2.grad = None
+        ag.gp_nll(X2, y2, th2).sum().backward()
+
+    ms_big = timed(big, 1) if not args.no_gp_large else None
+    return {"metric": "GP marginal likelihood logdet+grad evaluations/s", "value": rate, "unit": "1/s",
+            "ms_per_step": ms, "dtype": "f64",
+            "config": {"workload": f"{B} x n={n} SE-kernel GPs, points U[0,1]^2, l=0.3 sigma_f^2=1 sigma^2=1e-2, "
+                                   "loss = 1/2 (y^T A^-1 y + logdet A), dloss/dtheta by the adjoint kernels",
+                       "loop": f"torch.linalg.cholesky/cholesky_solve + autograd one matrix at a time "
+                               f"({nloop}-matrix sample)"},
+            "loop_value": loop_rate, "vs_loop": rate / loop_rate, "torch_batched_value": B / (tb * 1e-3),
+            "grad_rel_err_vs_torch_fp64": rel,
+            "single_n16384_f32_ms": ms_big}
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
     import torch
 
@@ -399,6 +592,10 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                                   "traffic": traffic.get("k_syrk_dmma", {}).get("bytes_per_launch_at_bench"),
                                   "peak_source": "cuBLAS DGEMM 8192^3 best-of-5 measured in this run"}
         line["speedup_mixed_over_plain"] = head["value"] / plain["value"]
+    if not args.no_batched:
+        line["batched"] = batched_leg(args, torch, device, h, stream, C)
+    if not args.no_gp:
+        line["gp"] = gp_leg(args, torch, device)
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu_tf, sample, info = cpu_sample(budget_s=12.0, nrhs=nrhs, kappa=args.kappa)
         line["cpu_baseline"] = {"value": cpu_tf, "unit": UNIT,
@@ -419,6 +616,10 @@ def main(argv=None):
     ap.add_argument("--kappa", type=float, default=1e6)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-gp", action="store_true")
+    ap.add_argument("--no-gp-large", action="store_true")
+    ap.add_argument("--batched-count", type=int, default=4096)
     args = ap.parse_args(argv)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
