@@ -2,7 +2,8 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--n 32768] [--nrhs 8] [--kappa 1e6] [--no-cpu] [--no-plain]
-                    [--no-batched] [--no-gp] [--no-gp-large] [--batched-count 4096]
+                    [--no-batched] [--no-gp] [--no-gp-large] [--batched-count 4096] [--gp-batch 256]
+                    [--only mixed-B|mixed-T|plain|batched|gp]
 
 Workload: solve A X = B to FP64 accuracy for a double n x n SPD matrix
 A = U diag(s) U^T (U = product of 4 Householder reflectors with N(0,1)
@@ -326,7 +327,7 @@ def gp_leg(args, torch, device):
     from libddla_b200.ddla import autograd as ag
 
     g = torch.Generator(device=device).manual_seed(0xDD1A0005)
-    B, n = 256, 1024
+    B, n = args.gp_batch, 1024
     X = torch.rand(B, n, 2, generator=g, device=device, dtype=torch.float64)
     y = torch.randn(B, n, generator=g, device=device, dtype=torch.float64)
     th = torch.tensor([0.3, 1.0, 1e-2], dtype=torch.float64, device=device, requires_grad=True)
@@ -379,7 +380,7 @@ def gp_leg(args, torch, device):
         (0.5 * ((y * ab).sum(-1) + 2 * torch.log(torch.diagonal(Lb, dim1=-2, dim2=-1)).sum(-1))).sum().backward()
 
     tb = timed(torch_batched, 2)
-    nloop = 32
+    nloop = min(32, B)
 
     def torch_loop():
         t = th.detach().clone().requires_grad_(True)
@@ -487,9 +488,21 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     tf = lambda total_ms: world * flops_pposv(n, nrhs) * args.steps / (total_ms * 1e-3) / 1e12
 
+    only = args.only
+    if only in ("batched", "gp"):
+        # one secondary leg alone (a profiling driver): its object is the line
+        leg = batched_leg(args, torch, device, h, stream, C) if only == "batched" else gp_leg(args, torch, device)
+        if rank == 0:
+            print(json.dumps({"only": only, only: leg}), flush=True)
+        h.destroy()
+        return
+
     # ---- mixed precision + refinement (headline) ----
     mixed = {}
-    for prec in ("B", "T"):
+    precs = ("B", "T") if only is None else ((only[-1],) if only.startswith("mixed-") else ())
+    if only == "plain":
+        precs = ()
+    for prec in precs:
         fell_back = [False]
 
         def solve_and_note(prec=prec):
@@ -509,12 +522,14 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         assert info == 0, (prec, info)
         mixed[prec] = {"value": tf(total), "ms_per_step": total / args.steps, "report": rep,
                        "backward_error": backward_error(X), "kernels": kern, "launches": launches, "clocks": clocks}
-    best = max(mixed, key=lambda p: mixed[p]["value"] if mixed[p]["report"]["iter"] >= 0 else -1)
-    head = mixed[best]
+    if only == "plain":
+        mixed = {}
+    best = max(mixed, key=lambda p: mixed[p]["value"] if mixed[p]["report"]["iter"] >= 0 else -1) if mixed else None
+    head = mixed[best] if mixed else None
 
     # ---- plain FP64 ----
     plain = None
-    if not args.no_plain:
+    if not args.no_plain and only in (None, "plain"):
         A = torch.empty_like(A0)
         dA = desc(A.data_ptr(), n, n)
 
@@ -532,6 +547,16 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         plain = {"value": tf(total), "ms_per_step": total / args.steps, "backward_error": backward_error(X),
                  "kernels": kern, "launches": launches}
         del A
+
+    if only is not None:
+        # one leg alone (a profiling driver): no e2e, CPU or secondary figures
+        if rank == 0:
+            print(json.dumps({"only": only, "mixed": {p: {k: v for k, v in d.items() if k != "kernels"}
+                                                      for p, d in mixed.items()},
+                              "plain": None if plain is None else {k: v for k, v in plain.items()
+                                                                   if k != "kernels"}}), flush=True)
+        h.destroy()
+        return
 
     # ---- e2e through the public API with host buffers (headline path) ----
     Ah = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
@@ -620,6 +645,9 @@ def main(argv=None):
     ap.add_argument("--no-gp", action="store_true")
     ap.add_argument("--no-gp-large", action="store_true")
     ap.add_argument("--batched-count", type=int, default=4096)
+    ap.add_argument("--gp-batch", type=int, default=256)
+    ap.add_argument("--only", choices=["mixed-B", "mixed-T", "plain", "batched", "gp"], default=None,
+                    help="run one leg alone (profiling driver); prints that leg's figures only")
     args = ap.parse_args(argv)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
