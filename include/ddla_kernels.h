@@ -87,7 +87,22 @@ int ddlak_inv_diag_blocks(int n, const void* L32, long long ldl, void* Dinv, voi
 int ddlak_potrs_mixed(int n, int nrhs, const void* L32, long long ldl, const void* Dinv, void* B, long long ldb,
                       void* work, unsigned long long work_bytes, void* stream);
 
-/* R = B - A X, A symmetric FP64 stored in its lower triangle; deterministic. */
+/* Refinement solves by inverted diagonal super-blocks of order ddlak_bis_block()
+ * (1024): ddlak_bis_inverse writes the FP64 inverses of the diagonal blocks of
+ * an FP32 factor (ddlak_bis_inverse_bytes(n) bytes, one BS x BS block per
+ * super-block; tmp is scratch of the same size); ddlak_bis_solve then solves
+ * L L^T X = B in place (FP64 B, nrhs <= 16, ldl a multiple of 4, L 16-byte
+ * aligned) in n/BS phases per direction of a diagonal-block product and a
+ * streaming panel update.  Scratch: ddlak_bis_solve_workspace(n, nrhs). */
+int ddlak_bis_block(void);
+unsigned long long ddlak_bis_inverse_bytes(int n);
+int ddlak_bis_inverse(int n, const void* L32, long long ldl, void* Dinv, void* tmp, void* stream);
+unsigned long long ddlak_bis_solve_workspace(int n, int nrhs);
+int ddlak_bis_solve(int n, int nrhs, const void* L32, long long ldl, const void* Dinv, void* B, long long ldb,
+                    void* work, unsigned long long work_bytes, void* stream);
+
+/* R = B - A X, A symmetric FP64 stored in its lower triangle, each lower tile read once
+ * (atomics fold the partial products into R: its last bits depend on their order). */
 int ddlak_symm_residual(int n, int nrhs, const void* A, long long lda, const void* X, long long ldx, const void* B,
                         long long ldb, void* R, long long ldr, void* stream);
 

@@ -23,10 +23,17 @@ std::size_t GmresIR::workspace_bytes(int n, int nrhs, int m)
            detail::padded_bytes<double>(nrhs);
 }
 
-GmresIR::GmresIR(const DdlaHandle_t& h, int n, int nrhs, const double* A, long long lda, const float* L32,
-                 long long ldl, const double* Dinv, void* solve_work, std::size_t solve_bytes, void* work, int m)
-    : h_(h), n_(n), nrhs_(nrhs), m_(m), A_(A), lda_(lda), L_(L32), ldl_(ldl), Dinv_(Dinv), swork_(solve_work),
-      sbytes_(solve_bytes)
+void MixedPreconditioner::apply(double* B, long long ldb) const
+{
+    if (blocked)
+        ck(ddlak_bis_solve(n, nrhs, L, ldl, Dinv, B, ldb, work, bytes, h->stream), "preconditioner");
+    else
+        ck(ddlak_potrs_mixed(n, nrhs, L, ldl, Dinv, B, ldb, work, bytes, h->stream), "preconditioner");
+}
+
+GmresIR::GmresIR(const DdlaHandle_t& h, int n, int nrhs, const double* A, long long lda, const MixedPreconditioner& M,
+                 void* work, int m)
+    : h_(h), n_(n), nrhs_(nrhs), m_(m), A_(A), lda_(lda), M_(M)
 {
     char* w = static_cast<char*>(work);
     V_ = detail::take<double>(w, (std::size_t)(m + 1) * 0 + (std::size_t)n * nrhs);
@@ -49,7 +56,7 @@ int GmresIR::solve(const double* R, double* D, int maxit)
 
     // V_0 = M^-1 r / ||M^-1 r||
     detail::cuda_check(cudaMemcpyAsync(Vi(0), R, sizeof(double) * n * nc, cudaMemcpyDeviceToDevice, st), "copy r");
-    ck(ddlak_potrs_mixed(n, nc, L_, ldl_, Dinv_, Vi(0), n, swork_, sbytes_, st), "preconditioner");
+    M_.apply(Vi(0), n);
     ck(ddlak_multidot(Vi(0), 0, 1, Vi(0), n, nc, nrm2_, st), "norm");
     std::vector<double> beta(nc);
     detail::cuda_check(cudaMemcpyAsync(beta.data(), nrm2_, sizeof(double) * nc, cudaMemcpyDeviceToHost, st), "norm");
@@ -77,7 +84,7 @@ int GmresIR::solve(const double* R, double* D, int maxit)
         if (all) break;
         // w = M^-1 A V_j  (the residual kernel gives 0 - A V_j; the solve is linear)
         ck(ddlak_symm_residual(n, nc, A_, lda_, Vi(j), n, Z_, n, Wv_, n, st), "A v");
-        ck(ddlak_potrs_mixed(n, nc, L_, ldl_, Dinv_, Wv_, n, swork_, sbytes_, st), "preconditioner");
+        M_.apply(Wv_, n);
         ck(ddlak_scale_cols(Wv_, Wv_, n, nc, -1.0, nullptr, st), "sign");
         // CGS2
         ck(ddlak_multidot(V_, vstride, j + 1, Wv_, n, nc, c1, st), "cgs dots");

@@ -15,14 +15,30 @@
 
 namespace ddla {
 
+// M^-1 = (L L^T)^-1 applied in place to an n x nrhs FP64 block, L the FP32
+// factor: by inverted diagonal super-blocks (ddlak_bis_solve) when `blocked`,
+// else by the fused chain solve (ddlak_potrs_mixed, Dinv = 64-row block inverses).
+struct MixedPreconditioner {
+    DdlaHandle_t h = nullptr;
+    int n = 0;
+    int nrhs = 0;
+    const float* L = nullptr;
+    long long ldl = 0;
+    const double* Dinv = nullptr;
+    bool blocked = false;
+    void* work = nullptr;
+    std::size_t bytes = 0;
+    void apply(double* B, long long ldb) const;
+};
+
 class GmresIR {
 public:
     static constexpr int kRestart = 30;
 
     static std::size_t workspace_bytes(int n, int nrhs, int m);
 
-    GmresIR(const DdlaHandle_t& h, int n, int nrhs, const double* A, long long lda, const float* L32, long long ldl,
-            const double* Dinv, void* solve_work, std::size_t solve_bytes, void* work, int m);
+    GmresIR(const DdlaHandle_t& h, int n, int nrhs, const double* A, long long lda, const MixedPreconditioner& M,
+            void* work, int m);
 
     // D = approximately A^-1 R (both n x nrhs, ld = n).  Runs at most maxit
     // Arnoldi steps, stopping early when every column's preconditioned
@@ -34,11 +50,7 @@ private:
     int n_, nrhs_, m_;
     const double* A_;
     long long lda_;
-    const float* L_;
-    long long ldl_;
-    const double* Dinv_;  // inverted diagonal blocks of L_ (ddlak_inv_diag_blocks)
-    void* swork_;
-    std::size_t sbytes_;
+    MixedPreconditioner M_;
     double* V_;      // (m+1) blocks of n x nrhs
     double* Wv_;     // n x nrhs
     double* Z_;      // zeros, n x nrhs (the B of A*v = -(0 - A v))

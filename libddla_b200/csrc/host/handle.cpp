@@ -126,6 +126,15 @@ static ddlaStatus_t set_impl(DdlaHandle_t handle, const MPI_Comm& comm, int npro
         handle->owns_stream = true;
         const cudaError_t e3 = cudaMallocHost(reinterpret_cast<void**>(&handle->host_word), 64);
         if (e3 != cudaSuccess) return from_cuda(e3);
+        // Workspace comes from the device's stream-ordered pool (cudaMallocAsync).
+        // Keep freed blocks in the pool instead of unmapping them at every
+        // synchronisation: the multi-GB workspaces of consecutive calls then reuse
+        // the same mapped memory.
+        cudaMemPool_t pool = nullptr;
+        if (cudaDeviceGetDefaultMemPool(&pool, handle->device) == cudaSuccess) {
+            unsigned long long keep = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
     }
     handle->comm = comm;
     handle->nprows_ = handle->npcols_ = 1;

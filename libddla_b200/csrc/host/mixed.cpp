@@ -86,14 +86,18 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
     // ---- workspace ----------------------------------------------------------
     const long long ldw = (n + 3) / 4 * 4;
     const std::size_t pbytes = ddlak_mixed_panel_bytes(n);
-    const std::size_t sbytes = ddlak_potrs_workspace(n, std::max(1, nrhs));
+    // refinement solves: inverted diagonal super-blocks for up to 16 right-hand
+    // sides, the fused chain with 64-row block inverses beyond
+    const bool blocked = nrhs <= 16;
+    const std::size_t sbytes = blocked ? ddlak_bis_solve_workspace(n, std::max(1, nrhs))
+                                       : ddlak_potrs_workspace(n, std::max(1, nrhs));
+    const std::size_t dinv_bytes = blocked ? ddlak_bis_inverse_bytes(n) : ddlak_inv_diag_bytes(n);
     const int kry = GmresIR::kRestart;
     const std::size_t bytes = detail::padded_bytes<float>((std::size_t)ldw * n) + 2 * pbytes +
                               3 * detail::padded_bytes<double>((std::size_t)n * std::max(1, nrhs)) +
                               detail::padded_bytes<double>(n) + detail::padded_bytes<Scalars>(1) +
                               2 * detail::padded_bytes<double>(std::max(1, nrhs)) + sbytes +
-                              GmresIR::workspace_bytes(n, std::max(1, nrhs), kry) +
-                              (std::size_t)ddlak_inv_diag_bytes(n) + 256;
+                              GmresIR::workspace_bytes(n, std::max(1, nrhs), kry) + dinv_bytes + 256;
     detail::DeviceScratch ws(h, bytes);
     char* w = ws.data();
     float* W = detail::take<float>(w, (std::size_t)ldw * n);
@@ -105,7 +109,7 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
     double* D = detail::take<double>(w, (std::size_t)n * std::max(1, nrhs));
     double* Bc = detail::take<double>(w, (std::size_t)n * std::max(1, nrhs));
     double* colsum = detail::take<double>(w, n);
-    double* Dinv = detail::take<double>(w, ddlak_inv_diag_bytes(n) / sizeof(double));
+    double* Dinv = detail::take<double>(w, dinv_bytes / sizeof(double));
     Scalars* sc = detail::take<Scalars>(w, 1);
     double* xn = detail::take<double>(w, std::max(1, nrhs));
     double* rn = detail::take<double>(w, std::max(1, nrhs));
@@ -149,8 +153,23 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
     detail::cuda_check(cudaMemcpy2DAsync(X, ldx * sizeof(double), Bc, n * sizeof(double), n * sizeof(double), nrhs,
                                          cudaMemcpyDeviceToDevice, st),
                        "copy B to X");
-    ck(ddlak_inv_diag_blocks(n, W, ldw, Dinv, st), "diagonal block inverses");
-    ck(ddlak_potrs_mixed(n, nrhs, W, ldw, Dinv, X, ldx, swork, sbytes, st), "initial solve");
+    if (blocked) {
+        detail::DeviceScratch tmp(h, ddlak_bis_inverse_bytes(n));
+        ck(ddlak_bis_inverse(n, W, ldw, Dinv, tmp.data(), st), "diagonal block inverses");
+    } else {
+        ck(ddlak_inv_diag_blocks(n, W, ldw, Dinv, st), "diagonal block inverses");
+    }
+    MixedPreconditioner M;
+    M.h = h;
+    M.n = n;
+    M.nrhs = nrhs;
+    M.L = W;
+    M.ldl = ldw;
+    M.Dinv = Dinv;
+    M.blocked = blocked;
+    M.work = swork;
+    M.bytes = sbytes;
+    M.apply(X, ldx);
 
     std::vector<double> hx(nrhs), hr(nrhs);
     auto residual_check = [&](double& worst) -> bool {
@@ -174,7 +193,7 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
     double worst = 0, prev = INFINITY;
     int sweeps = 0;
     bool use_gmres = false;
-    GmresIR gmres(h, n, nrhs, A, lda, W, ldw, Dinv, swork, sbytes, gwork, kry);
+    GmresIR gmres(h, n, nrhs, A, lda, M, gwork, kry);
     while (true) {
         const bool ok = residual_check(worst);
         rep.backward_error = worst;
@@ -194,7 +213,7 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
         } else {
             detail::cuda_check(cudaMemcpyAsync(D, R, sizeof(double) * n * nrhs, cudaMemcpyDeviceToDevice, st),
                                "copy residual");
-            ck(ddlak_potrs_mixed(n, nrhs, W, ldw, Dinv, D, n, swork, sbytes, st), "correction solve");
+            M.apply(D, n);
             ++sweeps;
         }
         ck(ddlak_axpy(n, nrhs, 1.0, D, n, X, ldx, st), "update x");

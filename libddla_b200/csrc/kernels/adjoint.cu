@@ -5,7 +5,7 @@
 // matrices laid out with fixed strides:
 //   k_gp_build        A = K(theta) + sigma^2 I (squared-exponential kernel on
 //                     points in R^d), lower triangle only (all the factorization reads);
-//   k_trtri_batched   W = L^-1 (lower), one CTA per matrix (order <= 1024):
+//   k_trtri_batched   W = L^-1 (lower), one CTA per matrix and block-column range (order <= 1024):
 //                     block columns of width B; for each 32-row block the rows'
 //                     partial results are staged in shared memory, all warps solve
 //                     them against the 32 x 32 diagonal block of L (a few columns
@@ -86,8 +86,18 @@ __global__ void __launch_bounds__(TR_NT, 1)
     const T* L = Lg + blockIdx.x * lstride;
     T* W = Wg + blockIdx.x * wstride;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    // block columns of W are independent: part p of gridDim.y takes the range
+    // [jb, je) holding about 1/P of the work ((n - J)^3 / 3 beyond column J)
+    const int P = gridDim.y, p = blockIdx.y;
+    auto jstart = [&](int q) -> int {
+        if (q <= 0) return 0;
+        if (q >= P) return n;
+        const double f = 1.0 - cbrt((double)(P - q) / (double)P);
+        return min(n, (int)(f * n) / B * B);
+    };
+    const int jb = jstart(p), je = jstart(p + 1);
     int step = 0;
-    for (int J = 0; J < n; J += B) {
+    for (int J = jb; J < je; J += B) {
         const int nb = min(B, n - J);
         T acc[RPT][B];
 #pragma unroll
@@ -213,8 +223,10 @@ __global__ void __launch_bounds__(CT_NT, 1)
     // thread (ty, tx) of 16 x 16 owns rows i0 + {ty*4 .. +3, 64 + ty*4 .. +3} and the
     // same pattern of columns: the k-loop reads them as 4-element runs (conflict free)
     constexpr int CT_KC = ct_kc<T>();
-    __shared__ __align__(16) T Wi[2][CT_KC][CT_TILE];
-    __shared__ __align__(16) T Wj[2][CT_KC][CT_TILE];
+    // rows padded by 4 elements: the staging stores (consecutive k in consecutive
+    // threads) then fall in different banks
+    __shared__ __align__(16) T Wi[2][CT_KC][CT_TILE + 4];
+    __shared__ __align__(16) T Wj[2][CT_KC][CT_TILE + 4];
     __shared__ double red[3][CT_NT / 32];
     const int m = blockIdx.y;
     const int tile = blockIdx.x;
@@ -422,8 +434,13 @@ template <class T>
 int trtri_t(int batch, int n, const void* L, long long ldl, long long lstride, void* W, long long ldw,
             long long wstride, cudaStream_t st)
 {
-    k_trtri_batched<T><<<batch, TR_NT, 0, st>>>(n, static_cast<const T*>(L), ldl, lstride, static_cast<T*>(W), ldw,
-                                                wstride);
+    // split each matrix over block-column ranges until the launch covers the SMs twice
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int parts = 1;
+    while (parts < 8 && (long long)batch * parts < 2LL * sms && n / TrWidth<T>::B >= 4 * parts) parts *= 2;
+    k_trtri_batched<T><<<dim3(batch, parts), TR_NT, 0, st>>>(n, static_cast<const T*>(L), ldl, lstride,
+                                                             static_cast<T*>(W), ldw, wstride);
     note_launches(1);
     return (int)cudaGetLastError();
 }

@@ -16,6 +16,7 @@
 #include <cuda_bf16.h>
 
 #include <mutex>
+#include <type_traits>
 
 #include "common.cuh"
 #include "ddla_kernels_internal.h"
@@ -41,11 +42,10 @@ __global__ void __launch_bounds__(256) k_convert_lower(const double* __restrict_
     int I, J;
     tile_of_tri(blockIdx.x, I, J);
     const long long ri = (long long)I * 64, rj = (long long)J * 64;
-    __shared__ double csum[64];
+    __shared__ double csw[8][16];   // per warp: column sums of its 32 rows
     __shared__ double rsum[4][64];
     const int r = threadIdx.x & 63, cg = threadIdx.x >> 6;
-    if (threadIdx.x < 64) csum[threadIdx.x] = 0.0;
-    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double rs = 0.0;
     double vals[16];
 #pragma unroll
@@ -56,19 +56,23 @@ __global__ void __launch_bounds__(256) k_convert_lower(const double* __restrict_
 #pragma unroll
     for (int u = 0; u < 16; ++u) {
         const long long i = ri + r, j = rj + cg + 4 * u;
+        const double a = vals[u];
         if (i < n && j < n && i >= j) {
-            const double a = vals[u];
             W[i + j * ldw] = (float)(i == j ? a * diag_scale : a);
-            const double aa = fabs(a);
-            atomicAdd(&csum[cg + 4 * u], aa);
-            if (i != j) rs += aa;
+            if (i != j) rs += fabs(a);
         }
+        // column cg + 4u: sum of |a| over this warp's 32 rows
+        double v = fabs(a);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) csw[warp][u] = v;
     }
     rsum[cg][r] = rs;
     __syncthreads();
     if (threadIdx.x < 64) {
-        const int t = threadIdx.x;
-        if (rj + t < n && csum[t] != 0.0) atomicAdd(&colsum[rj + t], csum[t]);
+        const int t = threadIdx.x, tcg = t & 3, tu = t >> 2;  // column t = tcg + 4 tu
+        const double cs = csw[2 * tcg][tu] + csw[2 * tcg + 1][tu];
+        if (rj + t < n && cs != 0.0) atomicAdd(&colsum[rj + t], cs);
         const double rt = rsum[0][t] + rsum[1][t] + rsum[2][t] + rsum[3][t];
         if (ri + t < n && rt != 0.0) atomicAdd(&colsum[ri + t], rt);
     }
@@ -261,96 +265,123 @@ __global__ void __launch_bounds__(128, 2) k_mixed_update(const __grid_constant__
 }
 
 // ---------------------------------------------------------------------------
-// R = B - A X for symmetric A stored in its lower triangle (FP64), up to 16
-// right-hand sides per chunk (grid.z).  Block row I of the result needs the
-// row strip A(I, 0..I) and the column strip A(I+1.., I) (used transposed); the
-// strip is split over grid.y CTAs that stream their tiles through a 3-stage
-// cp.async ring and fold their partial sums into R with atomics (R holds B on
-// entry), so small n still fills every SM.
+// R = B - A X for symmetric A stored in its lower triangle (FP64), NC (8 or 16)
+// right-hand sides per chunk (grid.y).  Every lower tile A(I, J), I >= J, is
+// read from HBM once and used twice: A(I,J) X(J) goes to R(I) and A(I,J)^T X(I)
+// to R(J).  CTA (J, c) walks tiles I = J + c*SR_CPT .. of column strip J through
+// a double-buffered cp.async ring: the first product is folded into R(I) with
+// atomics after each tile, the second accumulates in registers and is folded
+// into R(J) at the end (R holds B on entry).  The tile is stored rotated,
+// element (r, col) at T[col][(r + col) mod 64], so both the row walk of the
+// first product and the column walk of the second are conflict free.  The
+// atomics make the last bits of R depend on the order the tiles finish.
 // ---------------------------------------------------------------------------
 constexpr int SR = 64;
-constexpr int SR_STAGES = 3;
+constexpr int SR_CPT = 8;  // tiles per CTA
+
+template <int NC>
+constexpr size_t symm_residual_smem()
+{
+    return sizeof(double) * (2 * SR * SR + 3 * SR * (NC + 1));
+}
+
+template <int NC>
 __global__ void __launch_bounds__(256) k_symm_residual(const double* __restrict__ A, long long lda, int n, int nrhs,
                                                        const double* __restrict__ X, long long ldx,
-                                                       double* __restrict__ R, long long ldr, int per_split)
+                                                       double* __restrict__ R, long long ldr, int chunks)
 {
+    constexpr int QN = NC / 4;  // columns per thread
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double (*Tb)[SR][SR + 1] = reinterpret_cast<double (*)[SR][SR + 1]>(smem_raw);  // raw tiles [col][row]
-    double (*Xs)[17] = reinterpret_cast<double (*)[17]>(smem_raw + sizeof(double) * SR_STAGES * SR * (SR + 1));
-    const int I = blockIdx.x;
+    double* Tb = reinterpret_cast<double*>(smem_raw);                       // [2][SR cols][SR]
+    double (*XJ)[NC + 1] = reinterpret_cast<double (*)[NC + 1]>(Tb + 2 * SR * SR);
+    double (*XI)[SR][NC + 1] = reinterpret_cast<double (*)[SR][NC + 1]>(Tb + 2 * SR * SR + SR * (NC + 1));
     const int N = (int)ceil_div(n, SR);
-    const int vbeg = blockIdx.y * per_split;
-    const int vend = (vbeg + per_split) < N ? (vbeg + per_split) : N;
-    if (vbeg >= vend) return;
-    const long long i0 = (long long)I * SR;
-    const int nrows = (int)((n - i0) < SR ? (n - i0) : SR);
-    const int r0 = blockIdx.z * 16;
-    const int nr = nrhs - r0 < 16 ? nrhs - r0 : 16;
+    const int J = blockIdx.x / chunks, c = blockIdx.x % chunks;
+    if (J >= N) return;
+    const int tbeg = J + c * SR_CPT;
+    if (tbeg >= N) return;
+    const int tend = (tbeg + SR_CPT) < N ? (tbeg + SR_CPT) : N;
+    const long long j0 = (long long)J * SR;
+    const int ncols = (int)((n - j0) < SR ? (n - j0) : SR);
+    const int r0 = blockIdx.y * NC;
+    const int nr = nrhs - r0 < NC ? nrhs - r0 : NC;
     const int tr = threadIdx.x & 63, tg = threadIdx.x >> 6;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    // visit v: for v <= I the row-strip tile A(I, v) (raw rows of I, cols of v),
-    // for v > I the column-strip tile A(v, I) (raw rows of v, cols of I), used transposed
-    auto issue = [&](int v, int buf) {
-        const long long rr = v <= I ? i0 : (long long)v * SR;
-        const long long cc = v <= I ? (long long)v * SR : i0;
-        const int nrr = (int)((n - rr) < SR ? (n - rr) : SR);
-        const int ncc = (int)((n - cc) < SR ? (n - cc) : SR);
+
+    auto issue = [&](int I, int buf) {
+        const long long i0 = (long long)I * SR;
+        const int nrows = (int)((n - i0) < SR ? (n - i0) : SR);
+        double* T = Tb + buf * SR * SR;
         for (int idx = threadIdx.x; idx < SR * SR; idx += blockDim.x) {
-            const int rrow = idx % SR, ccol = idx / SR;
-            const bool valid = rrow < nrr && ccol < ncc && (rr + rrow >= cc + ccol);
-            cp_async_elem<8>(&Tb[buf][ccol][rrow], valid ? A + (rr + rrow) + (cc + ccol) * lda : A, valid);
+            const int r = idx & 63, col = idx >> 6;
+            const bool valid = r < nrows && col < ncols && (I != J || r >= col);
+            cp_async_elem<8>(&T[col * SR + ((r + col) & 63)], valid ? A + (i0 + r) + (j0 + col) * lda : A, valid);
+        }
+        for (int idx = threadIdx.x; idx < SR * NC; idx += blockDim.x) {
+            const int k = idx % SR, q = idx / SR;
+            const bool valid = k < nrows && q < nr;
+            cp_async_elem<8>(&XI[buf][k][q], valid ? X + (i0 + k) + (r0 + q) * ldx : X, valid);
         }
     };
-#pragma unroll
-    for (int s = 0; s < SR_STAGES - 1; ++s) {
-        if (vbeg + s < vend) issue(vbeg + s, s);
-        asm volatile("cp.async.commit_group;" ::: "memory");
+    for (int idx = threadIdx.x; idx < SR * NC; idx += blockDim.x) {
+        const int k = idx % SR, q = idx / SR;
+        XJ[k][q] = (k < ncols && q < nr) ? X[(j0 + k) + (r0 + q) * ldx] : 0.0;
     }
-    for (int v = vbeg; v < vend; ++v) {
-        const int slot = (v - vbeg) % SR_STAGES;
-        const int pre = v + SR_STAGES - 1;
-        if (pre < vend) issue(pre, (pre - vbeg) % SR_STAGES);
-        asm volatile("cp.async.commit_group;" ::: "memory");
-        const long long j0 = (long long)v * SR;
-        const int ncols = (int)((n - j0) < SR ? (n - j0) : SR);
-        for (int idx = threadIdx.x; idx < SR * 16; idx += blockDim.x) {
-            const int k = idx % SR, r = idx / SR;
-            Xs[k][r] = (k < ncols && r < nr) ? X[(j0 + k) + (r0 + r) * ldx] : 0.0;
-        }
-        asm volatile("cp.async.wait_group %0;" ::"n"(SR_STAGES - 1) : "memory");
+    issue(tbeg, 0);
+    cp_group_commit();
+    double accb[QN], accb2[QN];
+#pragma unroll
+    for (int q = 0; q < QN; ++q) accb[q] = accb2[q] = 0.0;
+    for (int I = tbeg; I < tend; ++I) {
+        const int buf = (I - tbeg) & 1;
+        if (I + 1 < tend) issue(I + 1, buf ^ 1);
+        cp_group_commit();
+        cp_group_wait<1>();
         __syncthreads();
-        const double (*Tt)[SR + 1] = Tb[slot];
-        if (v < I) {
-#pragma unroll 8
-            for (int k = 0; k < SR; ++k) {
-                const double a = Tt[k][tr];
+        const double* T = Tb + buf * SR * SR;
+        double acca[QN], acca2[QN];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) acc[q] = fma(a, Xs[k][tg + 4 * q], acc[q]);
-            }
-        } else if (v == I) {
-            // symmetric diagonal tile from its lower half: A(tr, k) = T[k][tr] (tr >= k) or T[tr][k]
-#pragma unroll 8
-            for (int k = 0; k < SR; ++k) {
-                const double a = tr >= k ? Tt[k][tr] : Tt[tr][k];
+        for (int q = 0; q < QN; ++q) acca[q] = acca2[q] = 0.0;
+        if (I != J) {
+            // R(I) -= A(I,J) X(J)  (row tr);  R(J) -= A(I,J)^T X(I)  (column tr)
+#pragma unroll 4
+            for (int k = 0; k < SR; k += 2) {
+                const double a0 = T[k * SR + ((tr + k) & 63)], a1 = T[(k + 1) * SR + ((tr + k + 1) & 63)];
+                const double b0 = T[tr * SR + ((k + tr) & 63)], b1 = T[tr * SR + ((k + 1 + tr) & 63)];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) acc[q] = fma(a, Xs[k][tg + 4 * q], acc[q]);
+                for (int q = 0; q < QN; ++q) {
+                    const int col = tg + 4 * q;
+                    acca[q] = fma(a0, XJ[k][col], acca[q]);
+                    acca2[q] = fma(a1, XJ[k + 1][col], acca2[q]);
+                    accb[q] = fma(b0, XI[buf][k][col], accb[q]);
+                    accb2[q] = fma(b1, XI[buf][k + 1][col], accb2[q]);
+                }
             }
         } else {
-#pragma unroll 8
+            // diagonal tile: the symmetric product from its lower half, into R(J) only
+#pragma unroll 4
             for (int k = 0; k < SR; ++k) {
-                const double a = Tt[tr][k];  // A(row k of block v, col tr of block I)
+                const double a = tr >= k ? T[k * SR + ((tr + k) & 63)] : T[tr * SR + ((k + tr) & 63)];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) acc[q] = fma(a, Xs[k][tg + 4 * q], acc[q]);
+                for (int q = 0; q < QN; ++q) acca[q] = fma(a, XJ[k][tg + 4 * q], acca[q]);
             }
         }
+        const long long i0 = (long long)I * SR;
+        if (i0 + tr < n)
+#pragma unroll
+            for (int q = 0; q < QN; ++q) {
+                const int col = tg + 4 * q;
+                if (col < nr) atomicAdd(&R[(i0 + tr) + (r0 + col) * ldr], -(acca[q] + acca2[q]));
+            }
         __syncthreads();
     }
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    cp_group_wait<0>();
+    if (tr < ncols)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int r = tg + 4 * q;
-        if (tr < nrows && r < nr) atomicAdd(&R[(i0 + tr) + (r0 + r) * ldr], -acc[q]);
-    }
+        for (int q = 0; q < QN; ++q) {
+            const int col = tg + 4 * q;
+            const double v = accb[q] + accb2[q];
+            if (col < nr && v != 0.0) atomicAdd(&R[(j0 + tr) + (r0 + col) * ldr], -v);
+        }
 }
 
 // out[j] = max_i |M(i,j)| (out zeroed by the caller; atomics on the bit pattern of non-negative doubles)
@@ -643,22 +674,25 @@ extern "C" int ddlak_symm_residual(int n, int nrhs, const void* A, long long lda
                                                 nrhs, cudaMemcpyDeviceToDevice, st);
         if (e != cudaSuccess) return (int)e;
     }
-    const size_t smem = sizeof(double) * (SR_STAGES * SR * (SR + 1) + SR * 17);
-    static std::once_flag once;
-    std::call_once(once, [&] {
-        cudaFuncSetAttribute(k_symm_residual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    });
     const int N = (int)ceil_div(n, SR);
-    int nsplit = (int)ceil_div(4 * 148, N);
-    nsplit = nsplit < 1 ? 1 : (nsplit > N ? N : nsplit);
-    const int per = (int)ceil_div(N, nsplit);
-    nsplit = (int)ceil_div(N, per);
-    dim3 grid((unsigned)N, (unsigned)nsplit, (unsigned)ceil_div(nrhs, 16));
-    {
-        ProfScope ps(PK_SYMM_RESIDUAL, st, 2.0 * (double)n * n * nrhs, 8.0 * (double)n * (n + 1));
-        k_symm_residual<<<grid, 256, smem, st>>>(static_cast<const double*>(A), lda, n, nrhs,
-                                                 static_cast<const double*>(X), ldx, static_cast<double*>(R), ldr, per);
-    }
+    const int chunks = (int)ceil_div(N, SR_CPT);
+    auto launch = [&](auto nc_tag) -> void {
+        constexpr int NC = decltype(nc_tag)::value;
+        const size_t smem = symm_residual_smem<NC>();
+        static std::once_flag once;
+        std::call_once(once, [&] {
+            cudaFuncSetAttribute(k_symm_residual<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        });
+        dim3 grid((unsigned)(N * chunks), (unsigned)ceil_div(nrhs, NC));
+        ProfScope ps(PK_SYMM_RESIDUAL, st, 2.0 * (double)n * n * nrhs, 4.0 * (double)n * (n + 1));
+        k_symm_residual<NC><<<grid, 256, smem, st>>>(static_cast<const double*>(A), lda, n, nrhs,
+                                                    static_cast<const double*>(X), ldx, static_cast<double*>(R), ldr,
+                                                    chunks);
+    };
+    if (nrhs <= 8)
+        launch(std::integral_constant<int, 8>{});
+    else
+        launch(std::integral_constant<int, 16>{});
     note_launches(1);
     return (int)cudaGetLastError();
 }

@@ -115,6 +115,7 @@ __global__ void __launch_bounds__(NT) k_potrs_fused(const TL* __restrict__ A, lo
     R* Rinv = reinterpret_cast<R*>(Acc + RB);
     __shared__ int s_t;
     __shared__ int s_abort;
+    __shared__ int s_next;
     if (threadIdx.x == 0) { s_t = atomicAdd(ticket, 1); s_abort = 0; }
     __syncthreads();
     const int N = (int)ceil_div(n, RB);
@@ -197,25 +198,54 @@ __global__ void __launch_bounds__(NT) k_potrs_fused(const TL* __restrict__ A, lo
             acc[q] = (tr < nrows && r < nr) ? x_ld_cg<T, BT>(B, ldb, i0 + tr, r0 + r) : zero<T>();
     }
 
+    // The solved block of the next visit is fetched into registers (L2 loads) while
+    // the current tile is multiplied whenever its flag is already set, so only the
+    // visits that really wait (the last ones) pay the load latency after the wait.
+    constexpr int XE = RB * RC / NT;
+    T xr[XE];
+    bool pre = false;
+    auto load_x = [&](int jj) {
+        const long long jj0 = (long long)jj * RB;
+        const int nc = (int)((n - jj0) < RB ? (n - jj0) : RB);
+#pragma unroll
+        for (int e = 0; e < XE; ++e) {
+            const int idx = threadIdx.x + e * NT;
+            const int k = idx % RB, r = idx / RB;
+            xr[e] = (k < nc && r < nr) ? x_ld_cg<T, BT>(B, ldb, jj0 + k, r0 + r) : zero<T>();
+        }
+    };
     for (int v = 0; v < nvisit; ++v) {
         const int j = visit(v);
-        const long long j0 = (long long)j * RB;
-        const int ncols = (int)((n - j0) < RB ? (n - j0) : RB);
         if (v + 1 < nvisit) issue_tile(visit(v + 1), (v + 1) & 1);
         else issue_diag((v + 1) & 1);
         cp_commit();
-        if (threadIdx.x == 0) {
-            if (!bounded_wait_geq(&cflags[fwd ? j : N + j], 1, status)) s_abort = 1;
-            __threadfence();
+        if (!pre) {
+            if (threadIdx.x == 0) {
+                if (!bounded_wait_geq(&cflags[fwd ? j : N + j], 1, status)) s_abort = 1;
+                __threadfence();
+            }
+            __syncthreads();
+            if (s_abort) { cp_wait<0>(); return; }
+            load_x(j);
         }
-        __syncthreads();
-        if (s_abort) { cp_wait<0>(); return; }
-        for (int idx = threadIdx.x; idx < RB * RC; idx += NT) {
-            const int k = idx % RB, r = idx / RB;
-            Xs[k][r] = (k < ncols && r < nr) ? x_ld_cg<T, BT>(B, ldb, j0 + k, r0 + r) : zero<T>();
+#pragma unroll
+        for (int e = 0; e < XE; ++e) {
+            const int idx = threadIdx.x + e * NT;
+            Xs[idx % RB][idx / RB] = xr[e];
+        }
+        if (threadIdx.x == 0) {
+            bool ready = false;
+            if (v + 1 < nvisit) {
+                const int jn = visit(v + 1);
+                ready = ld_acquire(&cflags[fwd ? jn : N + jn]) >= 1;
+                if (ready) __threadfence();
+            }
+            s_next = ready ? 1 : 0;
         }
         cp_wait<1>();
         __syncthreads();
+        pre = s_next != 0;
+        if (pre) load_x(visit(v + 1));
         const TL (*Lt)[RB + 1] = Lbuf[v & 1];
         if (p1) {
 #pragma unroll 8

@@ -112,16 +112,18 @@ __device__ void vb_matrix(int n, T* __restrict__ A, long long lda, T* __restrict
             cp_group_wait<1>();
             __syncthreads();
             const T* src = Ls + (size_t)(ch & 1) * VB_KC * LDS;
+            // a warp whose rows of set r all lie past the block column's last row skips them
+            bool live[RPT];
 #pragma unroll
-            for (int kk = 0; kk < VB_KC; ++kk) {
-                T li[RPT];
+            for (int r = 0; r < RPT; ++r) live[r] = (t - lane) + r * VB_NT < mJ;
 #pragma unroll
-                for (int r = 0; r < RPT; ++r) li[r] = src[kk * LDS + t + r * VB_NT];
+            for (int r = 0; r < RPT; ++r) {
+                if (!live[r]) continue;
 #pragma unroll
-                for (int q = 0; q < W; ++q) {
-                    const T lq = src[kk * LDS + q];
+                for (int kk = 0; kk < VB_KC; ++kk) {
+                    const T li = src[kk * LDS + t + r * VB_NT];
 #pragma unroll
-                    for (int r = 0; r < RPT; ++r) c[r][q] = fms(c[r][q], li[r], lq);
+                    for (int q = 0; q < W; ++q) c[r][q] = fms(c[r][q], li, src[kk * LDS + q]);
                 }
             }
             __syncthreads();
