@@ -12,7 +12,8 @@
 // Additions beside the reference path (no reference counterpart):
 //   pposv_mixed     FP64-accurate solve from a low-precision tensor-core factor
 //                   plus iterative refinement / GMRES-IR (LAPACK ?sposv shape);
-//   potrf_batched_solve_logdet / gp_nll_batched: see ddla_batched.h.
+//   posvVbatched / VbatchedPlan / vbatchedAutotune (batched uneven SPD) and
+//   cholNll* / gpNll* (likelihood and its adjoint): see ddla_batched.h.
 #ifndef DDLA_H
 #define DDLA_H
 
@@ -91,15 +92,16 @@ void ppotrs_run(const DdlaHandle_t& handle, char side, char uplo, char trans, in
 // with classical iterative refinement, switching to GMRES-IR preconditioned by
 // the low-precision factor when refinement stagnates.  precision 'D' factors
 // in FP64 directly.  uplo 'L' only.
-//   On success A is unchanged, X holds the solution and iter > 0 is the number
-//   of refinement sweeps (GMRES iterations count one each).  If neither scheme
+//   On success A is unchanged, X holds the solution and iter >= 0 is the number
+//   of refinement sweeps (GMRES iterations count one each; 0 when the first
+//   solve already passes the stopping test).  If neither scheme
 //   reaches the LAPACK ?sposv stopping test (||r|| <= ||x|| ||A|| eps sqrt(n))
 //   within the iteration budget, the routine falls back to ppotrf/ppotrs in
 //   FP64 (A then holds the FP64 factor) and sets iter = -(sweeps + 1).
 //   info is ppotrf's info of whichever factorization produced X.
 // ---------------------------------------------------------------------------
 struct MixedReport {
-    int iter = 0;            // refinement sweeps (> 0), or -(sweeps+1) after FP64 fallback
+    int iter = 0;            // refinement sweeps (>= 0), or -(sweeps+1) after the FP64 fallback
     int gmres = 0;           // 1 if GMRES-IR was used
     double shift = 0;        // diagonal shift applied to the low-precision factor (relative)
     double backward_error = 0;  // final max_j ||b_j - A x_j||_inf / (||A||_inf ||x_j||_inf)

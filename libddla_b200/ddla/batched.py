@@ -161,3 +161,23 @@ def tuning(handle, dtype: str, max_n: int) -> dict:
                                           ctypes.byref(t)), "vbatched tuning")
     nb = (512 if max_n <= 512 else 1024) // 16
     return {"grid": g.value, "widths": [w[0], w[1]], "variant": [v[i] for i in range(nb)], "tuned": bool(t.value)}
+
+
+def shard_lpt(orders, world: int):
+    """Partition a batch over `world` ranks by longest-processing-time on the
+    factorization cost n^3 (each matrix to the least-loaded rank, largest first).
+    Returns one sorted index list per rank; every index appears exactly once and
+    the loads differ by at most the cost of one matrix."""
+    import heapq
+
+    if world < 1:
+        raise ValueError("shard_lpt: world must be >= 1")
+    orders = [int(n) for n in orders]
+    order = sorted(range(len(orders)), key=lambda i: (-orders[i], i))
+    heap = [(0.0, r) for r in range(world)]
+    shards = [[] for _ in range(world)]
+    for i in order:
+        load, r = heapq.heappop(heap)
+        shards[r].append(i)
+        heapq.heappush(heap, (load + float(orders[i]) ** 3, r))
+    return [sorted(s) for s in shards]
