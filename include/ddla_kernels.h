@@ -72,7 +72,9 @@ int ddlak_convert_lower(int n, const void* A, long long lda, void* W, long long 
 /* Cholesky of the FP32 matrix W (lower) with tensor-core trailing updates:
  * precision 'B' (BF16 operands) or 'T' (TF32 operands), FP32 accumulation,
  * FP64 diagonal blocks.  P0/P1: two buffers of ddlak_mixed_panel_bytes(n).
- * *dinfo as ddlak_potrf; *status nonzero if a tensor-core pipeline wait gave up. */
+ * *dinfo as ddlak_potrf; *status nonzero if a tensor-core pipeline wait gave up.
+ * The strictly upper triangle of W's leading n x n is used as scratch (the
+ * update writes whole 128 x 128 tiles); ldw must be a multiple of 4. */
 int ddlak_potrf_mixed(char precision, int n, void* W, long long ldw, void* P0, void* P1, int* dinfo, int* status,
                       void* stream);
 

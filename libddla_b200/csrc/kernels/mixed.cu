@@ -163,16 +163,17 @@ constexpr int MU_STAGES = 2;
 constexpr int MU_TILE_BYTES = 128 * 128;  // 128 rows x 128 bytes
 constexpr size_t MU_SMEM = (size_t)MU_STAGES * 2 * MU_TILE_BYTES + 1024;
 
-enum : int { MU_ERR_EMPTY = 0x21, MU_ERR_FULL = 0x22, MU_ERR_DONE = 0x23 };
+enum : int { MU_ERR_EMPTY = 0x21, MU_ERR_FULL = 0x22, MU_ERR_DONE = 0x23, MU_ERR_CTILE = 0x24 };
 
 template <bool TF32>
-__global__ void __launch_bounds__(128, 2) k_mixed_update(const __grid_constant__ CUtensorMap pmap,
+__global__ void __launch_bounds__(128, 3) k_mixed_update(const __grid_constant__ CUtensorMap pmap,
+                                                         const __grid_constant__ CUtensorMap wmap,
                                                          float* __restrict__ W, long long ldw, int n, long long t0,
                                                          long long pr0, int cols, int nkb,
                                                          const int* __restrict__ info, int* __restrict__ status)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t full[MU_STAGES], empty[MU_STAGES], done;
+    __shared__ __align__(8) uint64_t full[MU_STAGES], empty[MU_STAGES], done, cbar;
     __shared__ uint32_t s_tmem;
     if (*(volatile const int*)info != 0) return;
     int I, J;
@@ -184,7 +185,6 @@ __global__ void __launch_bounds__(128, 2) k_mixed_update(const __grid_constant__
         I = blockIdx.x / nct;
         if (I < J) return;
     }
-    const long long cend = cols == 0 ? (long long)n : t0 + cols;
     const long long ri = t0 + (long long)I * 128, rj = t0 + (long long)J * 128;
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -195,6 +195,7 @@ __global__ void __launch_bounds__(128, 2) k_mixed_update(const __grid_constant__
             tc::mbar_init(&empty[s], 1);
         }
         tc::mbar_init(&done, 1);
+        tc::mbar_init(&cbar, 1);
         tc::mbar_fence_init();
     }
     if (warp == 0) tc::tmem_alloc(&s_tmem, 128);
@@ -233,27 +234,37 @@ __global__ void __launch_bounds__(128, 2) k_mixed_update(const __grid_constant__
     }
     __syncwarp();
 
-    // epilogue
+    // epilogue: once the MMAs are done the operand stages are free; the 128 x 128
+    // FP32 tile of W comes in by TMA (64 KB, one request), the accumulator is
+    // subtracted in shared memory and the tile goes back by a TMA bulk store.
+    // Out-of-range rows and columns are zero-filled on the load and clipped on
+    // the store; the upper triangle of a diagonal tile is written too (W's upper
+    // triangle is scratch nothing reads).
     bool ok = tc::mbar_wait(&done, 0, status, MU_ERR_DONE);
     ok = __all_sync(0xffffffffu, ok);
     tc::tc_fence_after();
-    if (ok) {
-        const long long i = ri + 32 * warp + lane;
+    float* ct = reinterpret_cast<float*>(base);  // [128 cols][128 rows]
+    if (__syncthreads_and(ok)) {
+        if (threadIdx.x == 0) {
+            tc::mbar_expect_tx(&cbar, 128 * 128 * 4);
+            tc::tma_load_2d(ct, &wmap, &cbar, (int)ri, (int)rj);
+        }
+        ok = tc::mbar_wait(&cbar, 0, status, MU_ERR_CTILE);
+        ok = __all_sync(0xffffffffu, ok);
+        if (ok) {
+            const int r = 32 * warp + lane;
 #pragma unroll 1
-        for (int c = 0; c < 4; ++c) {
-            float v[32];
-            tc::tmem_ld_32x32b_x32(tmem + ((uint32_t)(32 * warp) << 16) + 32 * c, v);
-            float w[32];
+            for (int c = 0; c < 4; ++c) {
+                float v[32];
+                tc::tmem_ld_32x32b_x32(tmem + ((uint32_t)(32 * warp) << 16) + 32 * c, v);
 #pragma unroll
-            for (int e = 0; e < 32; ++e) {
-                const long long j = rj + 32 * c + e;
-                w[e] = (i < n && j < cend && i >= j) ? __ldcg(W + i + j * ldw) : 0.f;
+                for (int e = 0; e < 32; ++e) ct[(32 * c + e) * 128 + r] -= v[e];
             }
-#pragma unroll
-            for (int e = 0; e < 32; ++e) {
-                const long long j = rj + 32 * c + e;
-                if (i < n && j < cend && i >= j) W[i + j * ldw] = w[e] - v[e];
-            }
+            tc::fence_proxy_async_smem();
+        }
+        if (__syncthreads_and(ok) && threadIdx.x == 0) {
+            tc::tma_store_2d(&wmap, ct, (int)ri, (int)rj);
+            tc::tma_store_wait_read();
         }
     }
     tc::tc_fence_before();
@@ -504,6 +515,21 @@ bool encode_panel_map(CUtensorMap* map, const void* P, long long rows, int kp, b
     return r == CUDA_SUCCESS;
 }
 
+// W (FP32, n x n, leading dimension ldw, a multiple of 4) as 128 x 128 tiles, no swizzle
+bool encode_w_map(CUtensorMap* map, const float* W, int n, long long ldw)
+{
+    EncodeFn fn = encode_fn();
+    if (!fn) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)n};
+    const cuuint64_t strides[1] = {(cuuint64_t)ldw * 4};
+    const cuuint32_t box[2] = {128u, 128u};
+    const cuuint32_t estr[2] = {1u, 1u};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(W), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 struct MixedStreams {
     cudaStream_t hi = nullptr;
     cudaEvent_t start = nullptr, panel = nullptr, rest = nullptr;
@@ -537,13 +563,16 @@ cudaError_t mixed_update(float* W, long long ldw, int n, long long t0, long long
     });
     CUtensorMap map;
     if (!encode_panel_map(&map, P, (long long)n - pr0, nbk, TF32)) return cudaErrorInvalidValue;
+    CUtensorMap wmap;
+    if (!encode_w_map(&wmap, W, n, ldw)) return cudaErrorInvalidValue;
     const long long t = ceil_div(m, 128);
     const long long grid = cols == 0 ? t * (t + 1) / 2 : t * ceil_div(cols, 128);
     const int nkb = nbk / (TF32 ? 32 : 64);
     const double md = (double)m, cw = cols ? (double)cols : md;
     const double fl = cols ? 2.0 * nbk * (md * cw - cw * (cw - 1) / 2) : md * (md + 1) * nbk;
     ProfScope ps(PK_MIXED_UPDATE, st, fl, 4.0 * (cols ? 2.0 * md * cw : md * (md + 1)));
-    k_mixed_update<TF32><<<(unsigned)grid, 128, MU_SMEM, st>>>(map, W, ldw, n, t0, pr0, cols, nkb, dinfo, status);
+    k_mixed_update<TF32><<<(unsigned)grid, 128, MU_SMEM, st>>>(map, wmap, W, ldw, n, t0, pr0, cols, nkb, dinfo,
+                                                               status);
     note_launches(1);
     return cudaGetLastError();
 }
