@@ -395,6 +395,125 @@ __global__ void __launch_bounds__(256) k_symm_residual(const double* __restrict_
         }
 }
 
+// The same residual with the tiles of A and the blocks of X brought in by TMA
+// (one 32 KB request per tile instead of 4096 element copies); the tile stays
+// unrotated in shared memory, element (r, col) at T[col*64 + r], and the column
+// walk of the transposed product visits row (k + col) mod 64 at step k so that
+// the threads of a warp still hit different banks.  Requires A and X with even
+// leading dimensions and 16-byte aligned (the host falls back otherwise).  If a
+// tile's arrival wait gives up, NaN is folded into the affected rows of R, which
+// the refinement treats as a failed residual.
+__device__ int g_sr_status;
+
+template <int NC>
+constexpr size_t symm_residual_tma_smem()
+{
+    return 1024 + sizeof(double) * (2 * SR * SR + 2 * NC * SR + SR * (NC + 1));
+}
+
+template <int NC>
+__global__ void __launch_bounds__(256, 2) k_symm_residual_tma(const __grid_constant__ CUtensorMap amap,
+                                                              const __grid_constant__ CUtensorMap xmap, int n,
+                                                              int nrhs, const double* __restrict__ X, long long ldx,
+                                                              double* __restrict__ R, long long ldr, int chunks)
+{
+    constexpr int QN = NC / 4;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[2];
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    double* Tb = reinterpret_cast<double*>(base);  // [2][64 cols][64 rows]
+    double* XIb = Tb + 2 * SR * SR;                // [2][NC][64]
+    double (*XJ)[NC + 1] = reinterpret_cast<double (*)[NC + 1]>(XIb + 2 * NC * SR);
+    const int N = (int)ceil_div(n, SR);
+    const int J = blockIdx.x / chunks, c = blockIdx.x % chunks;
+    if (J >= N) return;
+    const int tbeg = J + c * SR_CPT;
+    if (tbeg >= N) return;
+    const int tend = (tbeg + SR_CPT) < N ? (tbeg + SR_CPT) : N;
+    const long long j0 = (long long)J * SR;
+    const int ncols = (int)((n - j0) < SR ? (n - j0) : SR);
+    const int r0 = blockIdx.y * NC;
+    const int nr = nrhs - r0 < NC ? nrhs - r0 : NC;
+    const int tr = threadIdx.x & 63, tg = threadIdx.x >> 6;
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&full[0], 1);
+        tc::mbar_init(&full[1], 1);
+        tc::mbar_fence_init();
+    }
+    for (int idx = threadIdx.x; idx < SR * NC; idx += blockDim.x) {
+        const int k = idx % SR, q = idx / SR;
+        XJ[k][q] = (k < ncols && q < nr) ? X[(j0 + k) + (r0 + q) * ldx] : 0.0;
+    }
+    __syncthreads();
+    constexpr uint32_t bytes = (uint32_t)(sizeof(double) * (SR * SR + NC * SR));
+    auto issue = [&](int I, int buf) {
+        if (threadIdx.x == 0) {
+            tc::mbar_expect_tx(&full[buf], bytes);
+            tc::tma_load_2d(Tb + buf * SR * SR, &amap, &full[buf], I * SR, (int)j0);
+            tc::tma_load_2d(XIb + buf * NC * SR, &xmap, &full[buf], I * SR, r0);
+        }
+    };
+    issue(tbeg, 0);
+    double accb[QN], accb2[QN];
+#pragma unroll
+    for (int q = 0; q < QN; ++q) accb[q] = accb2[q] = 0.0;
+    bool all_ok = true;
+    for (int I = tbeg; I < tend; ++I) {
+        const int k_ = I - tbeg, buf = k_ & 1;
+        if (I + 1 < tend) issue(I + 1, buf ^ 1);
+        const bool ok = __syncthreads_and(tc::mbar_wait(&full[buf], (k_ >> 1) & 1, &g_sr_status, 0x31));
+        all_ok = all_ok && ok;
+        const double* T = Tb + buf * SR * SR;
+        const double* XI = XIb + buf * NC * SR;
+        double acca[QN], acca2[QN];
+#pragma unroll
+        for (int q = 0; q < QN; ++q) acca[q] = acca2[q] = 0.0;
+        if (!ok) {
+#pragma unroll
+            for (int q = 0; q < QN; ++q) acca[q] = __longlong_as_double(0x7ff8000000000000LL);
+        } else if (I != J) {
+            // R(I) -= A(I,J) X(J)  (row tr);  R(J) -= A(I,J)^T X(I)  (column tr, rows visited rotated)
+#pragma unroll 4
+            for (int k = 0; k < SR; k += 2) {
+                const double a0 = T[k * SR + tr], a1 = T[(k + 1) * SR + tr];
+                const int kr0 = (k + tr) & 63, kr1 = (k + 1 + tr) & 63;
+                const double b0 = T[tr * SR + kr0], b1 = T[tr * SR + kr1];
+#pragma unroll
+                for (int q = 0; q < QN; ++q) {
+                    const int col = tg + 4 * q;
+                    acca[q] = fma(a0, XJ[k][col], acca[q]);
+                    acca2[q] = fma(a1, XJ[k + 1][col], acca2[q]);
+                    accb[q] = fma(b0, XI[col * SR + kr0], accb[q]);
+                    accb2[q] = fma(b1, XI[col * SR + kr1], accb2[q]);
+                }
+            }
+        } else {
+            // diagonal tile: the symmetric product from its lower half, into R(J) only
+#pragma unroll 4
+            for (int k = 0; k < SR; ++k) {
+                const double a = tr >= k ? T[k * SR + tr] : T[tr * SR + k];
+#pragma unroll
+                for (int q = 0; q < QN; ++q) acca[q] = fma(a, XJ[k][tg + 4 * q], acca[q]);
+            }
+        }
+        const long long i0 = (long long)I * SR;
+        if (i0 + tr < n)
+#pragma unroll
+            for (int q = 0; q < QN; ++q) {
+                const int col = tg + 4 * q;
+                if (col < nr) atomicAdd(&R[(i0 + tr) + (r0 + col) * ldr], -(acca[q] + acca2[q]));
+            }
+        __syncthreads();
+    }
+    if (tr < ncols)
+#pragma unroll
+        for (int q = 0; q < QN; ++q) {
+            const int col = tg + 4 * q;
+            const double v = all_ok ? accb[q] + accb2[q] : __longlong_as_double(0x7ff8000000000000LL);
+            if (col < nr && v != 0.0) atomicAdd(&R[(j0 + tr) + (r0 + col) * ldr], -v);
+        }
+}
+
 // out[j] = max_i |M(i,j)| (out zeroed by the caller; atomics on the bit pattern of non-negative doubles)
 __global__ void __launch_bounds__(256) k_colmax(const double* __restrict__ M, long long ld, int n, int ncol,
                                                 double* __restrict__ out)
@@ -525,6 +644,23 @@ bool encode_w_map(CUtensorMap* map, const float* W, int n, long long ldw)
     const cuuint32_t box[2] = {128u, 128u};
     const cuuint32_t estr[2] = {1u, 1u};
     const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(W), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+// FP64 column-major matrix (rows x cols, leading dimension ld, even) as box_rows x
+// box_cols tiles, no swizzle; out-of-range elements read as zero
+bool encode_f64_map(CUtensorMap* map, const double* P, long long rows, long long cols, long long ld, int box_rows,
+                    int box_cols)
+{
+    EncodeFn fn = encode_fn();
+    if (!fn || (ld & 1) || (reinterpret_cast<uintptr_t>(P) & 15)) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)rows, (cuuint64_t)cols};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 8};
+    const cuuint32_t box[2] = {(cuuint32_t)box_rows, (cuuint32_t)box_cols};
+    const cuuint32_t estr[2] = {1u, 1u};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(P), dims, strides, box, estr,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
@@ -707,6 +843,21 @@ extern "C" int ddlak_symm_residual(int n, int nrhs, const void* A, long long lda
     const int chunks = (int)ceil_div(N, SR_CPT);
     auto launch = [&](auto nc_tag) -> void {
         constexpr int NC = decltype(nc_tag)::value;
+        CUtensorMap amap, xmap;
+        if (encode_f64_map(&amap, static_cast<const double*>(A), n, n, lda, SR, SR) &&
+            encode_f64_map(&xmap, static_cast<const double*>(X), n, nrhs, ldx, SR, NC)) {
+            const size_t smem = symm_residual_tma_smem<NC>();
+            static std::once_flag once_t;
+            std::call_once(once_t, [&] {
+                cudaFuncSetAttribute(k_symm_residual_tma<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem);
+            });
+            dim3 grid((unsigned)(N * chunks), (unsigned)ceil_div(nrhs, NC));
+            ProfScope ps(PK_SYMM_RESIDUAL, st, 2.0 * (double)n * n * nrhs, 4.0 * (double)n * (n + 1));
+            k_symm_residual_tma<NC><<<grid, 256, smem, st>>>(amap, xmap, n, nrhs, static_cast<const double*>(X),
+                                                              ldx, static_cast<double*>(R), ldr, chunks);
+            return;
+        }
         const size_t smem = symm_residual_smem<NC>();
         static std::once_flag once;
         std::call_once(once, [&] {
