@@ -514,6 +514,133 @@ __global__ void __launch_bounds__(256, 2) k_symm_residual_tma(const __grid_const
         }
 }
 
+// The residual for up to 8 right-hand sides on the FP64 tensor cores
+// (mma.sync m8n8k4 f64): with n = 8 = the right-hand sides, A(I,J) X(J) is
+// 8 x 16 fragments of the tile times the 16 fragments of X(J), and
+// A(I,J)^T X(I) the transposed fragments times those of X(I); the k sum runs
+// inside the instruction, so no partial sums cross threads.  Warp w owns rows
+// 8w..8w+7 of the first product (accumulated per tile, folded into R(I) with
+// atomics) and columns 8w..8w+7 of the second (accumulated over the CTA's tiles,
+// folded into R(J) at the end); X(J)'s fragments stay in registers for the
+// CTA's life.  The tile arrives by one TMA load of a 68 x 64 box: its column
+// stride of 68 doubles (4 rows beyond the tile, never read) puts the 32
+// elements of every fragment of either orientation, and of X(I)'s fragments, on
+// 16 distinct 8-byte bank pairs, two wavefronts per load, where the dense
+// 64-double stride gives 4-way (row walk) and 8-way (column walk) conflicts.
+// Two stages per CTA, two CTAs per SM.  Same preconditions and timeout
+// behaviour as k_symm_residual_tma.
+// ---------------------------------------------------------------------------
+constexpr int SRD_LD = SR + 4;                                      // smem column stride (doubles)
+constexpr int SRD_TILE = SRD_LD * SR;                               // A tile, doubles
+constexpr int SRD_XI = SRD_LD * 8;                                  // X(I) block, doubles
+constexpr int SRD_STAGE = ((SRD_TILE + SRD_XI) * 8 + 1023) / 1024 * 1024;  // bytes, 1024-aligned
+constexpr int SRD_NSTAGE = 2;
+constexpr size_t symm_residual_dmma_smem() { return 1024 + (size_t)SRD_NSTAGE * SRD_STAGE; }
+
+__device__ __forceinline__ void dmma_f64(double& d0, double& d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(256, 2) k_symm_residual_dmma(const __grid_constant__ CUtensorMap amap,
+                                                               const __grid_constant__ CUtensorMap xmap, int n,
+                                                               int nrhs, const double* __restrict__ X, long long ldx,
+                                                               double* __restrict__ R, long long ldr, int chunks)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[SRD_NSTAGE];
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int N = (int)ceil_div(n, SR);
+    const int J = blockIdx.x / chunks, c = blockIdx.x % chunks;
+    if (J >= N) return;
+    const int tbeg = J + c * SR_CPT;
+    if (tbeg >= N) return;
+    const int tend = (tbeg + SR_CPT) < N ? (tbeg + SR_CPT) : N;
+    const long long j0 = (long long)J * SR;
+    const int r0 = blockIdx.y * 8;
+    const int nr = nrhs - r0 < 8 ? nrhs - r0 : 8;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = lane >> 2, q = lane & 3;  // fragment row / column within the 8x4 (4x8) block
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < SRD_NSTAGE; ++s) tc::mbar_init(&full[s], 1);
+        tc::mbar_fence_init();
+    }
+    __syncthreads();
+    constexpr uint32_t bytes = (uint32_t)(sizeof(double) * (SRD_TILE + SRD_XI));
+    auto issue = [&](int I, int s) {
+        if (threadIdx.x == 0) {
+            double* T = reinterpret_cast<double*>(base + s * SRD_STAGE);
+            tc::mbar_expect_tx(&full[s], bytes);
+            tc::tma_load_2d(T, &amap, &full[s], I * SR, (int)j0);
+            tc::tma_load_2d(T + SRD_TILE, &xmap, &full[s], I * SR, r0);
+        }
+    };
+    for (int s = 0; s < SRD_NSTAGE && tbeg + s < tend; ++s) issue(tbeg + s, s);
+    // B fragments of X(J): element (k = 4kb + q, rhs = g)
+    double xj[16];
+#pragma unroll
+    for (int kb = 0; kb < 16; ++kb) {
+        const long long row = j0 + 4 * kb + q;
+        xj[kb] = (row < n && g < nr) ? X[row + (r0 + g) * ldx] : 0.0;
+    }
+    double cb0 = 0.0, cb1 = 0.0, cb2 = 0.0, cb3 = 0.0;  // second product, rows 8w+g of R(J), two k parities
+    bool all_ok = true;
+    for (int I = tbeg; I < tend; ++I) {
+        const int k_ = I - tbeg, s = k_ % SRD_NSTAGE;
+        const bool ok = __syncthreads_and(tc::mbar_wait(&full[s], (k_ / SRD_NSTAGE) & 1, &g_sr_status, 0x32));
+        all_ok = all_ok && ok;
+        const double* T = reinterpret_cast<const double*>(base + s * SRD_STAGE);
+        const double* XI = T + SRD_TILE;
+        double ca0 = 0.0, ca1 = 0.0, ca2 = 0.0, ca3 = 0.0;
+        if (I != J) {
+            // A(I,J) X(J): A fragment (row 8w+g, k 4kb+q) at T[k*68 + row]
+            // A(I,J)^T X(I): A fragment (col 8w+g, k 4kb+q) at T[col*68 + k], B fragment X(I)(4kb+q, g)
+#pragma unroll
+            for (int kb = 0; kb < 16; kb += 2) {
+                const double a0 = T[(4 * kb + q) * SRD_LD + 8 * w + g];
+                const double a1 = T[(4 * kb + 4 + q) * SRD_LD + 8 * w + g];
+                const double t0 = T[(8 * w + g) * SRD_LD + 4 * kb + q];
+                const double t1 = T[(8 * w + g) * SRD_LD + 4 * kb + 4 + q];
+                const double x0 = XI[g * SRD_LD + 4 * kb + q];
+                const double x1 = XI[g * SRD_LD + 4 * kb + 4 + q];
+                dmma_f64(ca0, ca1, a0, xj[kb]);
+                dmma_f64(ca2, ca3, a1, xj[kb + 1]);
+                dmma_f64(cb0, cb1, t0, x0);
+                dmma_f64(cb2, cb3, t1, x1);
+            }
+        } else {
+            // diagonal tile: the symmetric product from its lower half, into R(J) only
+#pragma unroll
+            for (int kb = 0; kb < 16; kb += 2) {
+                const int r = 8 * w + g, k0 = 4 * kb + q, k1 = k0 + 4;
+                const double a0 = r >= k0 ? T[k0 * SRD_LD + r] : T[r * SRD_LD + k0];
+                const double a1 = r >= k1 ? T[k1 * SRD_LD + r] : T[r * SRD_LD + k1];
+                dmma_f64(ca0, ca1, a0, xj[kb]);
+                dmma_f64(ca2, ca3, a1, xj[kb + 1]);
+            }
+        }
+        __syncthreads();  // stage s consumed by every warp
+        if (I + SRD_NSTAGE < tend) issue(I + SRD_NSTAGE, s);
+        // C fragment: row 8w+g, right-hand sides 2q and 2q+1
+        const long long row = (long long)I * SR + 8 * w + g;
+        const double nanv = __longlong_as_double(0x7ff8000000000000LL);
+        const double v0 = ok ? ca0 + ca2 : nanv, v1 = ok ? ca1 + ca3 : nanv;
+        if (row < n) {
+            if (2 * q < nr) atomicAdd(&R[row + (r0 + 2 * q) * ldr], -v0);
+            if (2 * q + 1 < nr) atomicAdd(&R[row + (r0 + 2 * q + 1) * ldr], -v1);
+        }
+    }
+    const long long row = j0 + 8 * w + g;
+    if (row < n) {
+        const double nanv = __longlong_as_double(0x7ff8000000000000LL);
+        const double v0 = all_ok ? cb0 + cb2 : nanv, v1 = all_ok ? cb1 + cb3 : nanv;
+        if (2 * q < nr && v0 != 0.0) atomicAdd(&R[row + (r0 + 2 * q) * ldr], -v0);
+        if (2 * q + 1 < nr && v1 != 0.0) atomicAdd(&R[row + (r0 + 2 * q + 1) * ldr], -v1);
+    }
+}
+
 // out[j] = max_i |M(i,j)| (out zeroed by the caller; atomics on the bit pattern of non-negative doubles)
 __global__ void __launch_bounds__(256) k_colmax(const double* __restrict__ M, long long ld, int n, int ncol,
                                                 double* __restrict__ out)
@@ -841,6 +968,22 @@ extern "C" int ddlak_symm_residual(int n, int nrhs, const void* A, long long lda
     }
     const int N = (int)ceil_div(n, SR);
     const int chunks = (int)ceil_div(N, SR_CPT);
+    if (nrhs <= 8) {
+        CUtensorMap amap, xmap;
+        if (encode_f64_map(&amap, static_cast<const double*>(A), n, n, lda, SRD_LD, SR) &&
+            encode_f64_map(&xmap, static_cast<const double*>(X), n, nrhs, ldx, SRD_LD, 8)) {
+            const size_t smem = symm_residual_dmma_smem();
+            static std::once_flag once_d;
+            std::call_once(once_d, [&] {
+                cudaFuncSetAttribute(k_symm_residual_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            });
+            ProfScope ps(PK_SYMM_RESIDUAL, st, 2.0 * (double)n * n * nrhs, 4.0 * (double)n * (n + 1));
+            k_symm_residual_dmma<<<dim3((unsigned)(N * chunks), 1), 256, smem, st>>>(
+                amap, xmap, n, nrhs, static_cast<const double*>(X), ldx, static_cast<double*>(R), ldr, chunks);
+            note_launches(1);
+            return (int)cudaGetLastError();
+        }
+    }
     auto launch = [&](auto nc_tag) -> void {
         constexpr int NC = decltype(nc_tag)::value;
         CUtensorMap amap, xmap;

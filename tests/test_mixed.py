@@ -41,11 +41,17 @@ def _k(name, *argtypes):
     return f
 
 
-@pytest.mark.parametrize("n,nrhs", [(200, 3), (777, 20), (1030, 8)])
-def test_symm_residual_matches_numpy(handle, n, nrhs):
+@pytest.mark.parametrize("n,nrhs,pad", [(200, 3, 0), (777, 20, 0), (1030, 8, 0), (1, 1, 1), (64, 8, 0), (67, 1, 1),
+                                        (68, 7, 2), (131, 8, 5), (2049, 5, 1), (4100, 8, 12), (333, 16, 1),
+                                        (500, 9, 0)])
+def test_symm_residual_matches_numpy(handle, n, nrhs, pad):
+    """Every residual kernel: DMMA (nrhs <= 8, even leading dimensions), TMA
+    (nrhs <= 16), element copies (odd leading dimensions); ragged last tiles."""
     rng = np.random.default_rng(n)
     A = _spd(rng, n)
-    Al = np.asfortranarray(np.tril(A) + np.triu(np.full((n, n), np.nan), 1))  # upper poisoned: never read
+    ld = n + pad
+    Al = np.full((ld, n), np.nan, order="F")  # upper triangle and padding poisoned: never read
+    Al[:n, :n] = np.tril(A) + np.triu(np.full((n, n), np.nan), 1)
     X = np.asfortranarray(rng.standard_normal((n, nrhs)))
     B = np.asfortranarray(rng.standard_normal((n, nrhs)))
     vp, i, ll = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong
@@ -53,11 +59,12 @@ def test_symm_residual_matches_numpy(handle, n, nrhs):
     dA, dX, dB = _dev(handle, Al), _dev(handle, X), _dev(handle, B)
     dR = handle.malloc(B.nbytes)
     try:
-        assert f(n, nrhs, dA, n, dX, n, dB, n, dR, n, _stream(handle)) == 0
+        assert f(n, nrhs, dA, ld, dX, n, dB, n, dR, n, _stream(handle)) == 0
         R = np.empty_like(B)
         handle.memcpy(R.ctypes.data, dR, R.nbytes)
         handle.synchronize()
         ref = B - A @ X
+        assert np.all(np.isfinite(R))
         assert np.max(np.abs(R - ref)) <= 1e-12 * np.max(np.abs(A)) * np.max(np.abs(X)) * n
     finally:
         for p in (dA, dX, dB, dR):
