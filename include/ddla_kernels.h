@@ -92,16 +92,25 @@ int ddlak_potrs_mixed(int n, int nrhs, const void* L32, long long ldl, const voi
 /* Refinement solves by inverted diagonal super-blocks of order ddlak_bis_block()
  * (1024): ddlak_bis_inverse writes the FP64 inverses of the diagonal blocks of
  * an FP32 factor (ddlak_bis_inverse_bytes(n) bytes, one BS x BS block per
- * super-block; tmp is scratch of the same size); ddlak_bis_solve then solves
- * L L^T X = B in place (FP64 B, nrhs <= 16, ldl a multiple of 4, L 16-byte
- * aligned) in n/BS phases per direction of a diagonal-block product and a
- * streaming panel update.  Scratch: ddlak_bis_solve_workspace(n, nrhs). */
+ * super-block, the strictly lower part mirrored into the upper half; tmp is
+ * scratch of the same size); ddlak_bis_inverse_narrow rounds them to FP32
+ * (half the bytes).  ddlak_bis_solve solves L L^T X = B in place (FP64 B,
+ * nrhs <= 16, ldl a multiple of 4, L and Dinv 16-byte aligned) with FP64
+ * arithmetic and the FP64 inverses; ddlak_bis_solve_f32 with FP32 arithmetic
+ * and the FP32 inverses (the single-precision solve of ?sposv).  Each is one
+ * persistent launch per 8 right-hand sides over the n/BS diagonal-block
+ * products and streaming panel updates of both directions; if one of its
+ * bounded waits gives up, X is NaN.  Scratch: ddlak_bis_solve_workspace(n,
+ * nrhs) for either. */
 int ddlak_bis_block(void);
 unsigned long long ddlak_bis_inverse_bytes(int n);
 int ddlak_bis_inverse(int n, const void* L32, long long ldl, void* Dinv, void* tmp, void* stream);
+int ddlak_bis_inverse_narrow(int n, const void* Dinv, void* Dinv32, void* stream);
 unsigned long long ddlak_bis_solve_workspace(int n, int nrhs);
 int ddlak_bis_solve(int n, int nrhs, const void* L32, long long ldl, const void* Dinv, void* B, long long ldb,
                     void* work, unsigned long long work_bytes, void* stream);
+int ddlak_bis_solve_f32(int n, int nrhs, const void* L32, long long ldl, const void* Dinv32, void* B, long long ldb,
+                        void* work, unsigned long long work_bytes, void* stream);
 
 /* R = B - A X, A symmetric FP64 stored in its lower triangle, each lower tile read once
  * (atomics fold the partial products into R: its last bits depend on their order). */

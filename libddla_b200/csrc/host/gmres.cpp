@@ -25,7 +25,9 @@ std::size_t GmresIR::workspace_bytes(int n, int nrhs, int m)
 
 void MixedPreconditioner::apply(double* B, long long ldb) const
 {
-    if (blocked)
+    if (blocked && single)
+        ck(ddlak_bis_solve_f32(n, nrhs, L, ldl, Dinv32, B, ldb, work, bytes, h->stream), "preconditioner");
+    else if (blocked)
         ck(ddlak_bis_solve(n, nrhs, L, ldl, Dinv, B, ldb, work, bytes, h->stream), "preconditioner");
     else
         ck(ddlak_potrs_mixed(n, nrhs, L, ldl, Dinv, B, ldb, work, bytes, h->stream), "preconditioner");
@@ -35,6 +37,7 @@ GmresIR::GmresIR(const DdlaHandle_t& h, int n, int nrhs, const double* A, long l
                  void* work, int m)
     : h_(h), n_(n), nrhs_(nrhs), m_(m), A_(A), lda_(lda), M_(M)
 {
+    M_.single = false;  // the Krylov basis needs the preconditioner applied in FP64
     char* w = static_cast<char*>(work);
     V_ = detail::take<double>(w, (std::size_t)(m + 1) * 0 + (std::size_t)n * nrhs);
     for (int i = 1; i <= m; ++i) (void)detail::take<double>(w, (std::size_t)n * nrhs);

@@ -16,8 +16,9 @@
 namespace ddla {
 
 // M^-1 = (L L^T)^-1 applied in place to an n x nrhs FP64 block, L the FP32
-// factor: by inverted diagonal super-blocks (ddlak_bis_solve) when `blocked`,
-// else by the fused chain solve (ddlak_potrs_mixed, Dinv = 64-row block inverses).
+// factor: by inverted diagonal super-blocks when `blocked` (FP32 arithmetic
+// with the FP32 inverses Dinv32 when `single`, else FP64 arithmetic), else by
+// the fused chain solve (ddlak_potrs_mixed, Dinv = 64-row block inverses).
 struct MixedPreconditioner {
     DdlaHandle_t h = nullptr;
     int n = 0;
@@ -25,7 +26,9 @@ struct MixedPreconditioner {
     const float* L = nullptr;
     long long ldl = 0;
     const double* Dinv = nullptr;
+    const float* Dinv32 = nullptr;
     bool blocked = false;
+    bool single = false;
     void* work = nullptr;
     std::size_t bytes = 0;
     void apply(double* B, long long ldb) const;

@@ -7,7 +7,9 @@
 //      operands, FP32 accumulation and storage, FP64 diagonal blocks); when the
 //      low-precision factorization breaks down, W is rebuilt with the diagonal
 //      scaled by 1 + c*u (a relative shift) and factored again;
-//   3. X = L^-T L^-1 B (FP32 factor, FP64 vectors);
+//   3. X = L^-T L^-1 B with the FP32 factor (FP32 solves by inverted diagonal
+//      super-blocks for up to 16 right-hand sides, as ?sposv's single-precision
+//      solves; the fused chain with FP64 vectors beyond);
 //   4. refinement: R = B - A X in FP64 against the untouched A, D = L^-T L^-1 R,
 //      X += D, until every column meets ||r|| <= ||x|| ||A|| eps sqrt(n) (the
 //      ?sposv test); when a sweep fails to halve the scaled residual the
@@ -92,12 +94,13 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
     const std::size_t sbytes = blocked ? ddlak_bis_solve_workspace(n, std::max(1, nrhs))
                                        : ddlak_potrs_workspace(n, std::max(1, nrhs));
     const std::size_t dinv_bytes = blocked ? ddlak_bis_inverse_bytes(n) : ddlak_inv_diag_bytes(n);
+    const std::size_t dinv32_bytes = blocked ? detail::padded_bytes<float>(ddlak_bis_inverse_bytes(n) / 8) : 0;
     const int kry = GmresIR::kRestart;
     const std::size_t bytes = detail::padded_bytes<float>((std::size_t)ldw * n) + 2 * pbytes +
                               3 * detail::padded_bytes<double>((std::size_t)n * std::max(1, nrhs)) +
                               detail::padded_bytes<double>(n) + detail::padded_bytes<Scalars>(1) +
                               2 * detail::padded_bytes<double>(std::max(1, nrhs)) + sbytes +
-                              GmresIR::workspace_bytes(n, std::max(1, nrhs), kry) + dinv_bytes + 256;
+                              GmresIR::workspace_bytes(n, std::max(1, nrhs), kry) + dinv_bytes + dinv32_bytes + 256;
     detail::DeviceScratch ws(h, bytes);
     char* w = ws.data();
     float* W = detail::take<float>(w, (std::size_t)ldw * n);
@@ -110,6 +113,7 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
     double* Bc = detail::take<double>(w, (std::size_t)n * std::max(1, nrhs));
     double* colsum = detail::take<double>(w, n);
     double* Dinv = detail::take<double>(w, dinv_bytes / sizeof(double));
+    float* Dinv32 = blocked ? detail::take<float>(w, ddlak_bis_inverse_bytes(n) / 8) : nullptr;
     Scalars* sc = detail::take<Scalars>(w, 1);
     double* xn = detail::take<double>(w, std::max(1, nrhs));
     double* rn = detail::take<double>(w, std::max(1, nrhs));
@@ -156,6 +160,7 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
     if (blocked) {
         detail::DeviceScratch tmp(h, ddlak_bis_inverse_bytes(n));
         ck(ddlak_bis_inverse(n, W, ldw, Dinv, tmp.data(), st), "diagonal block inverses");
+        ck(ddlak_bis_inverse_narrow(n, Dinv, Dinv32, st), "FP32 diagonal block inverses");
     } else {
         ck(ddlak_inv_diag_blocks(n, W, ldw, Dinv, st), "diagonal block inverses");
     }
@@ -166,7 +171,9 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
     M.L = W;
     M.ldl = ldw;
     M.Dinv = Dinv;
+    M.Dinv32 = Dinv32;
     M.blocked = blocked;
+    M.single = blocked;  // classic sweeps: FP32 solves; GmresIR keeps its copy in FP64
     M.work = swork;
     M.bytes = sbytes;
     M.apply(X, ldx);

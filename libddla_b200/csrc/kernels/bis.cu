@@ -1,32 +1,60 @@
 // Triangular solves of the mixed refinement by inverted diagonal super-blocks.
 //
-// The refinement solves L L^T x = b many times with one FP32 factor L (FP64
-// vectors).  A chain of 64-row block rows is bound by the latency of its n/64
-// sequential links; here the diagonal blocks of order BS = 1024 are inverted
-// once (in FP64, by the batched W = L^-1 kernel on widened copies) and each
-// direction is n/BS phases of two wide kernels:
-//   forward,  phase s:  y_s = inv(L_ss) b_s;          b_i -= L_is y_s   (i > s)
-//   backward, phase s:  x_s = inv(L_ss)^T y_s;        y_j -= L_sj^T x_s (j < s)
-// The panel kernels stream the FP32 factor once per direction with 16-byte loads
-// (HBM-bound), split along the 1024-long inner dimension when a phase has few
-// row (column) tiles, the partial sums folded in with FP64 atomics.  The
-// inverse blocks are mirrored into their unused upper halves so that both
-// diagonal-block products read contiguous columns.  y lives in a scratch
-// vector Y; b is overwritten by x.  nrhs <= 16.
+// The refinement solves L L^T x = b many times with one FP32 factor L.  The
+// diagonal blocks of order BS = 1024 are inverted once (in FP64, by the batched
+// W = L^-1 kernel on widened copies), and each solve is then
+//   forward,  phase s = 0..S-1:   y_s = inv(L_ss) b_s;        b_i -= L_is y_s   (i > s)
+//   backward, phase s = S-1..0:   x_s = inv(L_ss)^T y_s;      y_j -= L_sj^T x_s (j < s)
+// run by ONE persistent kernel (k_bis_chain) over a queue of units in that
+// order.  A unit is a 64-row (or 64-column) tile times one 256-wide slice of
+// the inner dimension (KS): at most 64 KB of FP32 matrix, two 32 KB chunks that
+// TMA streams into shared memory while the unit waits for its inputs.  A phase
+// lists its diagonal units (64-row parts x slices) and then its panel units,
+// the tiles the next diagonal block needs first.  A CTA takes the next unit
+// from an atomic counter, starts its matrix loads, waits (bounded) on the
+// counters its inputs are published on, computes, folds its partial product
+// into the target vector with atomics and counts itself done:
+//   cnt_f[t]   forward panel units applied to tile t of b    (complete at 4 per earlier phase)
+//   ydone[p]   forward diagonal units done for 64-row part p of y
+//   fdone      forward units done (the backward pass starts when all are)
+//   cnt_b[t]   backward panel units applied to tile t of y
+//   xdone[p]   backward diagonal units done for part p of x
+// Every wait is on units earlier in the queue, held by running CTAs, so the
+// queue cannot deadlock.  Splitting the inner dimension puts four CTAs on each
+// tile of the chain from one diagonal block to the next, and because the
+// contributions to a tile commute, the bulk of each panel never waits for
+// another phase.  The atomics make the last bits of the result depend on the
+// order the units finish.
+//
+// Arithmetic type T: float for the classic refinement sweeps (the FP32 factor
+// with FP32 solves, as LAPACK ?sposv: the solve's rounding is far below the
+// factor's), double for the GMRES preconditioner.  Vectors are held row-major,
+// 8 right-hand sides per row (32 or 64 bytes), the inverse blocks in T with
+// their strictly lower part mirrored into the upper half so that both the
+// product with inv(L_ss) and with its transpose read 4 contiguous rows per
+// load.  nrhs <= 16 (two passes of 8 beyond 8).  If a wait gives up, the
+// status word is set, every CTA leaves, and the solution is returned as NaN,
+// which the refinement treats as a failed sweep.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <mutex>
 
 #include <ddla_kernels.h>
 
 #include "common.cuh"
 #include "profile.h"
+#include "tc_common.cuh"
 
 namespace ddlak {
 namespace {
 
 constexpr int BS = 1024;  // super-block order
-constexpr int BIS_NT = 256;
+constexpr int CT = 64;    // rows of a vector tile
+constexpr int TPB = BS / CT;
+constexpr int CQ = 8;     // right-hand sides per pass
+constexpr int CH_NT = 512;
 
 // tmp[s] (BS x BS, ld BS) = FP64 copy of the lower triangle of the diagonal block s of L32
 __global__ void k_bis_widen(int n, const float* __restrict__ L, long long ldl, double* __restrict__ tmp)
@@ -41,8 +69,7 @@ __global__ void k_bis_widen(int n, const float* __restrict__ L, long long ldl, d
 }
 
 // Mirror the strictly lower part of every inverse block into its upper half:
-// D[k + i BS] = D[i + k BS] for k < i.  Column i then holds row i of the
-// inverse in rows 0..i and column i in rows i..: both products read columns.
+// D[k + i BS] = D[i + k BS] for k < i.
 __global__ void k_bis_mirror(double* __restrict__ Dinv)
 {
     __shared__ double t[32][33];
@@ -56,241 +83,623 @@ __global__ void k_bis_mirror(double* __restrict__ Dinv)
     if (i > k) D[k + (long long)i * BS] = t[tx][ty];
 }
 
-// y_s = inv(L_ss) b_s (FWD) or x_s = inv(L_ss)^T y_s: one warp per output row i,
-// lanes over column i of the mirrored inverse (rows 0..i, or i..bsz-1)
-template <int NQ, bool FWD>
-__global__ void __launch_bounds__(BIS_NT) k_bis_diag(int n, int nrhs, int s, const double* __restrict__ Dinv,
-                                                     const double* __restrict__ Vin, long long ldin,
-                                                     double* __restrict__ Vout, long long ldout)
+__global__ void k_bis_narrow(long long count, const double* __restrict__ src, float* __restrict__ dst)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* vs = reinterpret_cast<double*>(smem_raw);  // [NQ][BS]
-    const long long s0 = (long long)s * BS;
-    const int bsz = (int)((n - s0) < BS ? (n - s0) : BS);
-    const double* D = Dinv + (long long)s * BS * BS;
-    for (int e = threadIdx.x; e < bsz * NQ; e += BIS_NT) {
-        const int k = e % bsz, q = e / bsz;
-        vs[q * BS + k] = q < nrhs ? Vin[(s0 + k) + q * ldin] : 0.0;
-    }
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i = blockIdx.x * (BIS_NT / 32) + warp;
-    if (i >= bsz) return;
-    double acc[NQ];
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
-    const double* col = D + (long long)i * BS;
-    const int kb = FWD ? 0 : i, ke = FWD ? i + 1 : bsz;
-#pragma unroll 4
-    for (int k = kb + lane; k < ke; k += 32) {
-        const double d = col[k];
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) acc[q] = fma(d, vs[q * BS + k], acc[q]);
-    }
-#pragma unroll
-    for (int q = 0; q < NQ; ++q)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
-    if (lane == 0)
-#pragma unroll
-        for (int q = 0; q < NQ; ++q)
-            if (q < nrhs) Vout[(s0 + i) + q * ldout] = acc[q];
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count; e += (long long)gridDim.x * blockDim.x)
+        dst[e] = (float)src[e];
 }
 
-// b_i -= L(i, s-block k-range) y_s for the rows below block s, in 64-row tiles
-// (tile bx, bx + gridDim.x, ...: the staged y range is reused) and the k-range of
-// blockIdx.y (the range split over gridDim.y, partial sums folded in with atomics).
-// thread (g: rows 4g..4g+3 of the tile read as float4, ks: one of 16 k-slices)
-template <int NQ>
-__global__ void __launch_bounds__(BIS_NT) k_bis_panel(int n, int nrhs, int s, const float* __restrict__ L,
-                                                      long long ldl, const double* __restrict__ Y,
-                                                      double* __restrict__ B, long long ldb)
+// ---------------------------------------------------------------------------
+// the persistent chain
+// ---------------------------------------------------------------------------
+struct Chain {
+    int n, S, Tt;
+    long long nf, total;
+    const float* L;
+    long long ldl;
+    int* ctl;  // [0] status, [1] fdone, [2..3] queue head (64-bit)
+    int* cnt_f;
+    int* ydone;
+    int* cnt_b;
+    int* xdone;
+};
+
+constexpr int KS = 256;  // inner-dimension slice of a unit
+constexpr int QPB = BS / KS;
+
+__host__ __device__ __forceinline__ int blk_size(int n, int s)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int kseg = BS / gridDim.y;
-    double (*ys)[NQ + 1] = reinterpret_cast<double (*)[NQ + 1]>(smem_raw);  // [kseg][NQ+1]
-    double (*red)[64][NQ] = reinterpret_cast<double (*)[64][NQ]>(smem_raw + sizeof(double) * BS * (NQ + 1));
-    const long long s0 = (long long)s * BS;
-    const long long r0 = s0 + BS;  // first row below a full block s
-    const long long tiles = ceil_div(n - r0, 64);
-    const int kb0 = blockIdx.y * kseg;
-    for (int e = threadIdx.x; e < kseg * NQ; e += BIS_NT) {
-        const int k = e % kseg, q = e / kseg;
-        ys[k][q] = q < nrhs ? Y[(s0 + kb0 + k) + q * (long long)n] : 0.0;
-    }
-    const int g = threadIdx.x & 15, ks = threadIdx.x >> 4;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int kper = kseg / 16;
-    const int kb = ks * kper, ke = kb + kper;
-    for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const long long i0 = r0 + tile * 64;
-        const long long ir = i0 + 4 * g;
-        __syncthreads();  // ys staged / red of the previous tile consumed
-        double acc[4][NQ];
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) acc[u][q] = 0.0;
-        if (ir + 3 < n) {
-            const float* base = L + ir + (s0 + kb0 + kb) * ldl;
-#pragma unroll 8
-            for (int k = kb; k < ke; ++k, base += ldl) {
-                const float4 l = *reinterpret_cast<const float4*>(base);
-#pragma unroll
-                for (int q = 0; q < NQ; ++q) {
-                    const double y = ys[k][q];
-                    acc[0][q] = fma((double)l.x, y, acc[0][q]);
-                    acc[1][q] = fma((double)l.y, y, acc[1][q]);
-                    acc[2][q] = fma((double)l.z, y, acc[2][q]);
-                    acc[3][q] = fma((double)l.w, y, acc[3][q]);
-                }
-            }
-        } else {
-            for (int k = kb; k < ke; ++k)
-#pragma unroll
-                for (int u = 0; u < 4; ++u)
-                    if (ir + u < n) {
-                        const double l = L[(ir + u) + (s0 + kb0 + k) * ldl];
-#pragma unroll
-                        for (int q = 0; q < NQ; ++q) acc[u][q] = fma(l, ys[k][q], acc[u][q]);
-                    }
-        }
-        // reduce the 16 k-slices: pairs in-warp (lane ^ 16), then 8 partials through shared memory
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) acc[u][q] += __shfl_xor_sync(0xffffffffu, acc[u][q], 16);
-        if (lane < 16)
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-                for (int q = 0; q < NQ; ++q) red[warp][4 * g + u][q] = acc[u][q];
-        __syncthreads();
-        for (int e = threadIdx.x; e < 64 * NQ; e += BIS_NT) {
-            const int r = e & 63, q = e >> 6;
-            if (q < nrhs && i0 + r < n) {
-                double sum = 0.0;
-#pragma unroll
-                for (int w = 0; w < BIS_NT / 32; ++w) sum += red[w][r][q];
-                atomicAdd(&B[(i0 + r) + q * ldb], -sum);
-            }
-        }
-    }
+    const long long r = (long long)n - (long long)s * BS;
+    return r < BS ? (int)r : BS;
+}
+__host__ __device__ __forceinline__ int blk_parts(int n, int s) { return (blk_size(n, s) + CT - 1) / CT; }
+__host__ __device__ __forceinline__ int blk_slices(int n, int s) { return (blk_size(n, s) + KS - 1) / KS; }
+// slices of the forward diagonal part p (columns 0 .. min((p+1)*64, bsz)) and of the backward one (p*64 .. bsz)
+__host__ __device__ __forceinline__ int fdiag_slices(int bsz, int p)
+{
+    const int ke = (p + 1) * CT < bsz ? (p + 1) * CT : bsz;
+    return (ke + KS - 1) / KS;
+}
+__host__ __device__ __forceinline__ int bdiag_slices(int bsz, int p) { return (bsz + KS - 1) / KS - (p * CT) / KS; }
+__host__ __device__ __forceinline__ int fdiag_units(int bsz)
+{
+    int u = 0;
+    for (int p = 0; p < (bsz + CT - 1) / CT; ++p) u += fdiag_slices(bsz, p);
+    return u;
+}
+__host__ __device__ __forceinline__ int bdiag_units(int bsz)
+{
+    int u = 0;
+    for (int p = 0; p < (bsz + CT - 1) / CT; ++p) u += bdiag_slices(bsz, p);
+    return u;
 }
 
-// y_j -= sum_{i in block s, row range of blockIdx.y} L(i, j) x_i for columns j < s*BS:
-// one thread per column j (tiles of 256 columns, bx, bx + gridDim.x, ...), the
-// column's rows read as float4 and its dot products kept in registers; x of the
-// row range staged row-major so that its values are 128-bit broadcast reads.
-template <int NQ>
-__global__ void __launch_bounds__(BIS_NT) k_bis_panel_t(int n, int nrhs, int s, const float* __restrict__ L,
-                                                        long long ldl, const double* __restrict__ B, long long ldb,
-                                                        double* __restrict__ Y)
+// Queue order.  Forward group g = 0..S-1: the diagonal slices of block g
+// (kind 0), the sliced panel units of phase g on the tiles of blocks g+1..g+LA
+// (kind 1: the next diagonal blocks' inputs), then the bulk of phase g-LAG: one
+// unit per tile of blocks g-LAG+LA+1.. over the whole inner range (kind 4).
+// Backward group g = S-1..0: the diagonal slices of block g (kind 2), the
+// sliced panel units of phase g on the column tiles of blocks g-1..g-LA
+// (kind 3), then the bulk of phase g+LAG on the column tiles of blocks
+// < g+LAG-LA (kind 5).  A phase's bulk is taken LAG groups after its diagonal
+// block, when its inputs are long complete, and its first tiles are needed
+// LA-LAG+1 groups later, so the chain from one diagonal block to the next
+// neither queues behind the bulk nor waits for it.
+constexpr int LA = 3;
+constexpr int LAG = 2;
+static_assert(LAG <= LA, "a bulk unit must precede every diagonal block it feeds");
+
+__host__ __device__ __forceinline__ long long group_units(int n, int S, int Tt, bool fwd, int g)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const long long s0 = (long long)s * BS;
-    const int bsz = (int)((n - s0) < BS ? (n - s0) : BS);
-    const int iseg = BS / gridDim.y;
-    const int ib0 = blockIdx.y * iseg;
-    if (ib0 >= bsz) return;
-    const int ie = (ib0 + iseg) < bsz ? (ib0 + iseg) : bsz;
-    const int cnt = ie - ib0;
-    double (*xs)[NQ] = reinterpret_cast<double (*)[NQ]>(smem_raw);  // [iseg][NQ]
-    for (int e = threadIdx.x; e < iseg * NQ; e += BIS_NT) {
-        const int k = e / NQ, q = e % NQ;
-        xs[k][q] = (q < nrhs && k < cnt) ? B[(s0 + ib0 + k) + q * ldb] : 0.0;
-    }
-    __syncthreads();
-    const long long tiles = ceil_div(s0, BIS_NT);
-    const int c4 = cnt & ~3;
-    for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const long long j = tile * BIS_NT + threadIdx.x;
-        if (j >= s0) continue;
-        const float* col = L + s0 + ib0 + j * ldl;
-        double acc[NQ];
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
-#pragma unroll 4
-        for (int i = 0; i < c4; i += 4) {
-            const float4 l = __ldg(reinterpret_cast<const float4*>(col + i));
-#pragma unroll
-            for (int q = 0; q < NQ; ++q)
-                acc[q] = fma((double)l.x, xs[i][q],
-                             fma((double)l.y, xs[i + 1][q], fma((double)l.z, xs[i + 2][q], fma((double)l.w, xs[i + 3][q], acc[q]))));
+    const int nq = blk_slices(n, g);
+    if (fwd) {
+        long long u = fdiag_units(blk_size(n, g));
+        const long long ce = (long long)(g + LA + 1) * TPB < Tt ? (long long)(g + LA + 1) * TPB : Tt;
+        if (ce > (long long)(g + 1) * TPB) u += (ce - (long long)(g + 1) * TPB) * nq;
+        if (g >= LAG) {
+            const long long b0 = (long long)(g - LAG + LA + 1) * TPB;
+            if (Tt > b0) u += Tt - b0;
         }
-        for (int i = c4; i < cnt; ++i) {
-            const double l = col[i];
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) acc[q] = fma(l, xs[i][q], acc[q]);
-        }
-#pragma unroll
-        for (int q = 0; q < NQ; ++q)
-            if (q < nrhs) atomicAdd(&Y[j + q * (long long)n], -acc[q]);
+        return u;
     }
+    long long u = bdiag_units(blk_size(n, g));
+    u += (long long)(g - (g > LA ? g - LA : 0)) * TPB * nq;
+    if (g + LAG <= S - 1 && g + LAG - LA > 0) u += (long long)(g + LAG - LA) * TPB;
+    return u;
 }
 
-// the smallest power-of-two split (<= cap) giving at least `want` CTAs
-int split_for(long long tiles, int cap, long long want)
+// unit v of group g -> (kind, phase, index, slice); index = diagonal part
+// (kinds 0, 2), row tile (1, 4) or column tile (3, 5)
+__host__ __device__ void decode_in_group(const Chain& c, bool fwd, int g, long long v, int& kind, int& s, int& idx,
+                                         int& kq)
 {
-    int k = 1;
-    while (k < cap && tiles * k < want) k *= 2;
-    return k;
+    const int bsz = blk_size(c.n, g), dp = blk_parts(c.n, g), nq = blk_slices(c.n, g);
+    kq = 0;
+    if (fwd) {
+        for (int p = 0; p < dp; ++p) {
+            const int k = fdiag_slices(bsz, p);
+            if (v < k) { kind = 0; s = g; idx = p; kq = (int)v; return; }
+            v -= k;
+        }
+        const long long ce = (long long)(g + LA + 1) * TPB < c.Tt ? (long long)(g + LA + 1) * TPB : c.Tt;
+        const long long nc = ce > (long long)(g + 1) * TPB ? (ce - (long long)(g + 1) * TPB) * nq : 0;
+        if (v < nc) { kind = 1; s = g; idx = (g + 1) * TPB + (int)(v / nq); kq = (int)(v % nq); return; }
+        v -= nc;
+        kind = 4;
+        s = g - LAG;
+        idx = (g - LAG + LA + 1) * TPB + (int)v;
+        return;
+    }
+    for (int p = dp - 1; p >= 0; --p) {
+        const int k = bdiag_slices(bsz, p);
+        if (v < k) { kind = 2; s = g; idx = p; kq = (p * CT) / KS + (int)v; return; }
+        v -= k;
+    }
+    const long long nc = (long long)(g - (g > LA ? g - LA : 0)) * TPB * nq;
+    if (v < nc) { kind = 3; s = g; idx = g * TPB - 1 - (int)(v / nq); kq = (int)(v % nq); return; }
+    v -= nc;
+    kind = 5;
+    s = g + LAG;
+    idx = (g + LAG - LA) * TPB - 1 - (int)v;
 }
 
-template <int NQ>
-cudaError_t bis_solve_t(int n, int nrhs, const float* L, long long ldl, const double* Dinv, double* B, long long ldb,
-                        double* Y, cudaStream_t st)
+// unit u -> group by a forward scan (the checker's reference; the kernel keeps a cursor)
+__host__ __device__ void decode_unit(const Chain& c, long long u, int& kind, int& s, int& idx, int& kq)
 {
-    const int S = (int)ceil_div(n, BS);
-    const size_t sm_panel = sizeof(double) * (BS * (NQ + 1) + (BIS_NT / 32) * 64 * NQ);
-    const size_t sm_vec = sizeof(double) * BS * (NQ + 1);
-    static bool attr = [&] {
-        cudaFuncSetAttribute(k_bis_panel<NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_panel);
-        cudaFuncSetAttribute(k_bis_panel_t<NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_vec);
-        cudaFuncSetAttribute(k_bis_diag<NQ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_vec);
-        cudaFuncSetAttribute(k_bis_diag<NQ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_vec);
-        return true;
-    }();
-    (void)attr;
-    int sms = 148;
+    long long base = 0;
+    for (int g = 0; g < c.S; ++g) {
+        const long long gu = group_units(c.n, c.S, c.Tt, true, g);
+        if (u < base + gu) { decode_in_group(c, true, g, u - base, kind, s, idx, kq); return; }
+        base += gu;
+    }
+    for (int g = c.S - 1; g >= 0; --g) {
+        const long long gu = group_units(c.n, c.S, c.Tt, false, g);
+        if (u < base + gu) { decode_in_group(c, false, g, u - base, kind, s, idx, kq); return; }
+        base += gu;
+    }
+    kind = -1;
+    s = idx = kq = 0;
+}
+
+// A CTA takes increasing unit numbers, so its group is found by moving forward.
+struct Cursor {
+    bool fwd = true;
+    int g = 0;
+    long long base = 0;
+    __host__ __device__ void decode(const Chain& c, long long u, int& kind, int& s, int& idx, int& kq)
     {
-        int dev = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        while (true) {
+            if (fwd ? g >= c.S : g < 0) { kind = -1; s = idx = kq = 0; return; }
+            const long long gu = group_units(c.n, c.S, c.Tt, fwd, g);
+            if (u < base + gu) { decode_in_group(c, fwd, g, u - base, kind, s, idx, kq); return; }
+            base += gu;
+            if (fwd && g == c.S - 1) { fwd = false; g = c.S - 1; }
+            else g += fwd ? 1 : -1;
+        }
     }
-    const long long want = 3LL * sms;  // CTAs of a phase: resident CTAs on every SM
+};
+
+template <class T> struct VecIO;
+template <> struct VecIO<float> {
+    static __device__ __forceinline__ void ld8(const float* p, float (&v)[CQ])
+    {
+        const float4 a = *reinterpret_cast<const float4*>(p), b = *reinterpret_cast<const float4*>(p + 4);
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    }
+    static __device__ __forceinline__ void ld4(const float* p, float (&a)[4])
+    {
+        const float4 v = *reinterpret_cast<const float4*>(p);
+        a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w;
+    }
+};
+template <> struct VecIO<double> {
+    static __device__ __forceinline__ void ld8(const double* p, double (&v)[CQ])
+    {
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const double2 a = *reinterpret_cast<const double2*>(p + 2 * h);
+            v[2 * h] = a.x;
+            v[2 * h + 1] = a.y;
+        }
+    }
+    static __device__ __forceinline__ void ld4(const double* p, double (&a)[4])
+    {
+        const double2 v0 = *reinterpret_cast<const double2*>(p), v1 = *reinterpret_cast<const double2*>(p + 2);
+        a[0] = v0.x; a[1] = v0.y; a[2] = v1.x; a[3] = v1.y;
+    }
+};
+
+// Every unit streams its matrix through shared memory in 64 KB chunks, one
+// TMA box each: a 64-row x KC-column box of L or of the inverse blocks for the
+// row units (KC = 256 for FP32, 128 for FP64), a 256-row x 64-column box of L
+// for the column units.  A TMA box costs a CTA about half a microsecond however
+// large it is, so the boxes are as large as two stages of shared memory allow;
+// a sliced unit is one box, prefetched in full while the unit waits.
+constexpr int CHUNK = 65536;
+constexpr int NSTAGE = 2;
+template <class MT> constexpr int chunk_cols() { return CHUNK / (CT * (int)sizeof(MT)); }
+constexpr int PT_ROWS = CHUNK / (CT * 4);  // rows of a column-unit chunk (256)
+
+// Row unit, one chunk: acc(4g+u, q) += sum over this thread's columns of the
+// chunk (k-slice ks of 32) of M(4g+u, k) V(k, q), M(r, k) at tile[k*64 + r]
+// (column k of the chunk = block column kb + j*KC + k), V(k, q) at
+// vs[(j*KC + k)*CQ + q].  Columns at or past ke, and (MASK 1) past the row or
+// (MASK 2) before it, contribute 0.
+template <class T, class MT, int MASK>
+__device__ __forceinline__ void row_chunk(const MT* tile, const T* vs, int j, int kb, int ke, int rloc, int g, int ks,
+                                          T (&acc)[4][CQ])
+{
+    constexpr int KC = chunk_cols<MT>(), KT = KC / 32;
+    const int r4 = 4 * g;
+#pragma unroll 2
+    for (int kk = 0; kk < KT; ++kk) {
+        const int kc = ks * KT + kk;
+        const int kabs = kb + j * KC + kc;
+        MT a[4];
+        VecIO<MT>::ld4(tile + kc * CT + r4, a);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int row = rloc + r4 + u;
+            const bool ok = kabs < ke && (MASK != 1 || kabs <= row) && (MASK != 2 || kabs >= row);
+            if (!ok) a[u] = MT(0);
+        }
+        T v[CQ];
+        VecIO<T>::ld8(vs + (j * KC + kc) * CQ, v);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int q = 0; q < CQ; ++q) acc[u][q] = fma((T)a[u], v[q], acc[u][q]);
+    }
+}
+
+// Column unit, one chunk (rows j*256 .. j*256+255 of the unit, 64 columns,
+// tile[c*256 + r]): warp w owns columns 4w..4w+3, lane l the rows 4l..4l+3 and
+// 128+4l..128+4l+3, so the 32 lanes read 512 contiguous bytes of a column.
+// xq holds the vector q-major (xq[q*XQ + row]), read the same way.  The sum
+// over the lanes is taken once per unit (col_reduce).
+constexpr int XQ = BS + PT_ROWS;  // rows of the q-major vector
+template <class T>
+__device__ __forceinline__ void col_chunk(const float* tile, const T* xq, int j, T (&acc)[4][CQ])
+{
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int step = 0; step < 2; ++step) {
+        const int r = step * 128 + 4 * lane;
+        T x[CQ][4];
+#pragma unroll
+        for (int q = 0; q < CQ; ++q) VecIO<T>::ld4(xq + q * XQ + j * PT_ROWS + r, x[q]);
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) {
+            const float4 l = *reinterpret_cast<const float4*>(tile + (4 * w + cc) * PT_ROWS + r);
+#pragma unroll
+            for (int q = 0; q < CQ; ++q)
+                acc[cc][q] = fma((T)l.w, x[q][3], fma((T)l.z, x[q][2], fma((T)l.y, x[q][1], fma((T)l.x, x[q][0], acc[cc][q]))));
+        }
+    }
+}
+
+// Sum v[0..7] over the 32 lanes of a warp in 9 shuffles: halves of the values
+// are exchanged at distances 16, 8, 4, then the last value at 2 and 1.  Lane l
+// ends with the total of value ((l >> 4) & 1)*4 + ((l >> 3) & 1)*2 + ((l >> 2) & 1).
+template <class T>
+__device__ __forceinline__ T warp_sum8(T (&v)[CQ])
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int m = 16, len = CQ; m >= 4; m >>= 1, len >>= 1) {
+        const bool up = (lane & m) != 0;
+        const int half = len / 2;
+#pragma unroll
+        for (int i = 0; i < half; ++i) {
+            const T send = up ? v[i] : v[i + half];
+            const T keep = up ? v[i + half] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, m);
+        }
+    }
+    T r = v[0];
+    r += __shfl_xor_sync(0xffffffffu, r, 2);
+    r += __shfl_xor_sync(0xffffffffu, r, 1);
+    return r;
+}
+
+constexpr int VS_ROWS = BS + 256;  // staged row-major vector rows: a block plus the overhang of the last chunk
+
+// the reduction of a unit's partial sums (16 warps x 64 x CQ) reuses the stages
+template <class T>
+constexpr size_t chain_smem()
+{
+    static_assert((size_t)NSTAGE * CHUNK >= sizeof(T) * (CH_NT / 32) * CT * CQ, "reduction does not fit the stages");
+    static_assert(VS_ROWS * CQ >= XQ * CQ, "vector staging");
+    return 1024 + (size_t)NSTAGE * CHUNK + sizeof(T) * (size_t)VS_ROWS * CQ;
+}
+
+// Thread 0's wait list for a unit, polled by the lanes of warp 0 in parallel.
+__device__ __forceinline__ bool wait_inputs(const Chain& c, int kind, int s, int kb, int ke, int bsz, int* status)
+{
+    const int lane = threadIdx.x & 31;
+    bool ok = true;
+    const int lo = kb / CT, hi = (ke - 1) / CT;  // tiles or 64-row parts of block s the unit reads
+    for (int i = lo + lane; i <= hi && ok; i += 32) {
+        if (kind == 0) ok = bounded_wait_geq(&c.cnt_f[s * TPB + i], QPB * s, status);
+        else if (kind == 1) ok = bounded_wait_geq(&c.ydone[s * TPB + i], fdiag_slices(bsz, i), status);
+        else if (kind == 2) {
+            const int need = s == c.S - 1 ? 0 : QPB * (c.S - 2 - s) + blk_slices(c.n, c.S - 1);
+            ok = bounded_wait_geq(&c.cnt_b[s * TPB + i], need, status);
+        } else ok = bounded_wait_geq(&c.xdone[s * TPB + i], bdiag_slices(bsz, i), status);
+    }
+    if (kind == 2 && s == c.S - 1 && lane == 31 && ok) ok = bounded_wait_geq(c.ctl + 1, (int)c.nf, status);
+    return __all_sync(0xffffffffu, ok);
+}
+
+template <class T>
+__global__ void __launch_bounds__(CH_NT, 1) k_bis_chain(const __grid_constant__ CUtensorMap mapL,
+                                                        const __grid_constant__ CUtensorMap mapLt,
+                                                        const __grid_constant__ CUtensorMap mapD, Chain c,
+                                                        T* Bv, T* Y, T* X)
+{
+    constexpr int NS = NSTAGE;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    T* vs = reinterpret_cast<T*>(base + NS * CHUNK);
+    T* red = reinterpret_cast<T*>(base);  // after a unit's last chunk
+    __shared__ __align__(8) uint64_t full[NS];
+    __shared__ long long s_u;
+    __shared__ int s_ok;
+    int* status = c.ctl;
+    int* fdone = c.ctl + 1;
+    unsigned long long* head = reinterpret_cast<unsigned long long*>(c.ctl + 2);
+    const int tid = threadIdx.x;
+    constexpr int KCD = chunk_cols<T>();      // inverse-block columns per chunk
+    constexpr int KCL = chunk_cols<float>();  // factor columns per chunk (row units)
+    if (tid == 0) {
+        for (int s = 0; s < NS; ++s) tc::mbar_init(&full[s], 1);
+        tc::mbar_fence_init();
+        tc::prefetch_tmap(&mapL);
+        tc::prefetch_tmap(&mapLt);
+        tc::prefetch_tmap(&mapD);
+    }
+    __syncthreads();
+    unsigned long long seq = 0;  // chunks this CTA has consumed
+    __shared__ int s_unit[4];
+    Cursor cur;                  // thread 0's
+    while (true) {
+        if (tid == 0) {
+            s_u = (long long)atomicAdd(head, 1ULL);
+            if (s_u < c.total) cur.decode(c, s_u, s_unit[0], s_unit[1], s_unit[2], s_unit[3]);
+        }
+        __syncthreads();
+        const long long u = s_u;
+        if (u >= c.total) break;
+        const int unit_kind = s_unit[0], s = s_unit[1], idx = s_unit[2], kq = s_unit[3];
+        const bool bulk = unit_kind >= 4;  // a whole-block panel unit (kinds 4, 5 compute as 1, 3)
+        const int kind = unit_kind == 4 ? 1 : (unit_kind == 5 ? 3 : unit_kind);
+        const int bsz = blk_size(c.n, s);
+        const long long s0 = (long long)s * BS;
+        // rows (parts / tiles) and the inner range [kb, ke) of the block the unit covers
+        int nch, kb = kq * KS, ke, rloc = 0;
+        const T* vsrc;
+        if (kind == 0) {
+            rloc = idx * CT;
+            ke = min(min(kb + KS, rloc + CT), bsz);
+            nch = (ke - kb + KCD - 1) / KCD;
+            vsrc = Bv + (s0 + kb) * CQ;
+        } else if (kind == 1) {
+            ke = bulk ? bsz : min(kb + KS, bsz);
+            nch = (ke - kb + KCL - 1) / KCL;
+            vsrc = Y + (s0 + kb) * CQ;
+        } else if (kind == 2) {
+            rloc = idx * CT;
+            kb = max(kb, rloc);
+            ke = min(kq * KS + KS, bsz);
+            nch = (ke - kb + KCD - 1) / KCD;
+            vsrc = Y + (s0 + kb) * CQ;
+        } else {
+            ke = bulk ? bsz : min(kb + KS, bsz);
+            nch = (ke - kb + PT_ROWS - 1) / PT_ROWS;
+            vsrc = X + (s0 + kb) * CQ;
+        }
+        auto issue = [&](int j) {
+            const int st = (int)((seq + j) % NS);
+            unsigned char* dst = base + st * CHUNK;
+            tc::mbar_expect_tx(&full[st], CHUNK);
+            if (kind == 0 || kind == 2)
+                tc::tma_load_2d(dst, &mapD, &full[st], rloc, s * BS + kb + j * KCD);
+            else if (kind == 1)
+                tc::tma_load_2d(dst, &mapL, &full[st], idx * CT, (int)(s0 + kb + j * KCL));
+            else
+                tc::tma_load_2d(dst, &mapLt, &full[st], (int)(s0 + kb + j * PT_ROWS), idx * CT);
+        };
+        auto prefetch = [&](int j) {
+            if (kind == 0 || kind == 2)
+                tc::tma_prefetch_l2_2d(&mapD, rloc, s * BS + kb + j * KCD);
+            else if (kind == 1)
+                tc::tma_prefetch_l2_2d(&mapL, idx * CT, (int)(s0 + kb + j * KCL));
+            else
+                tc::tma_prefetch_l2_2d(&mapLt, (int)(s0 + kb + j * PT_ROWS), idx * CT);
+        };
+        const int npro = nch < NS ? nch : NS;
+        if (tid == 0) {
+            // the matrix is read-only: its chunks stream in while the unit waits for its inputs
+            tc::fence_proxy_async_smem();  // the previous unit's reduction wrote the stages
+            for (int j = 0; j < npro; ++j) issue(j);
+            for (int j = npro; j < nch; ++j) prefetch(j);  // the rest of the unit heads for L2 now
+        }
+        if (tid < 32) {
+            const bool ok = kind >= 0 && wait_inputs(c, kind, s, kb, ke, bsz, status);
+            if (tid == 0) s_ok = ok;
+        }
+        __syncthreads();
+        if (!s_ok) {
+            // a wait gave up (status set): let the chunks in flight land (bounded), then leave
+            for (int j = 0; j < npro; ++j)
+                (void)tc::mbar_wait(&full[(seq + j) % NS], (uint32_t)(((seq + j) / NS) & 1), status, 0x52);
+            break;
+        }
+        // stage the vector rows kb .. kb + nch*chunk of the block (zeros past the block): row-major
+        // for the row units, q-major for the column units
+        const int vavail = bsz - kb;
+        if (kind != 3) {
+            const int vlen = nch * (kind == 1 ? KCL : KCD);
+            constexpr int PER = CQ * (int)sizeof(T) / 16;  // 16-byte pieces per row
+            const float4* src = reinterpret_cast<const float4*>(vsrc);
+            float4* dst = reinterpret_cast<float4*>(vs);
+#pragma unroll 4
+            for (int e = tid; e < vlen * PER; e += CH_NT)
+                dst[e] = (e / PER) < vavail ? __ldcg(src + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+        } else {
+            constexpr int QP = 16 / (int)sizeof(T);  // right-hand sides per 16-byte piece
+            const int vlen = nch * PT_ROWS;
+            const float4* src = reinterpret_cast<const float4*>(vsrc);
+            for (int e = tid; e < vlen * (CQ / QP); e += CH_NT) {
+                const int row = e / (CQ / QP), q0 = (e % (CQ / QP)) * QP;
+                const float4 v = row < vavail ? __ldcg(src + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+                const T* pv = reinterpret_cast<const T*>(&v);
+#pragma unroll
+                for (int i = 0; i < QP; ++i) vs[(q0 + i) * XQ + row] = pv[i];
+            }
+        }
+        __syncthreads();
+        T acc[4][CQ];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int q = 0; q < CQ; ++q) acc[a][q] = T(0);
+        const int g = tid & 15, ks = tid >> 4;
+        bool ok = true;
+        int j = 0;
+        for (; j < nch; ++j) {
+            const int st = (int)((seq + j) % NS);
+            const uint32_t par = (uint32_t)(((seq + j) / NS) & 1);
+            ok = __syncthreads_and(tc::mbar_wait(&full[st], par, status, 0x51));
+            if (!ok) break;
+            const unsigned char* tile = base + st * CHUNK;
+            if (kind == 0)
+                row_chunk<T, T, 1>(reinterpret_cast<const T*>(tile), vs, j, kb, ke, rloc, g, ks, acc);
+            else if (kind == 1)
+                row_chunk<T, float, 0>(reinterpret_cast<const float*>(tile), vs, j, kb, ke, rloc, g, ks, acc);
+            else if (kind == 2)
+                row_chunk<T, T, 2>(reinterpret_cast<const T*>(tile), vs, j, kb, ke, rloc, g, ks, acc);
+            else
+                col_chunk<T>(reinterpret_cast<const float*>(tile), vs, j, acc);
+            __syncthreads();  // stage consumed by every thread
+            if (tid == 0 && j + NS < nch) issue(j + NS);
+        }
+        if (!ok) {
+            // an arrival wait gave up: wait (bounded) for the chunks still in flight, then leave
+            for (int jj = j; jj < nch && jj < j + NS; ++jj)
+                (void)tc::mbar_wait(&full[(seq + jj) % NS], (uint32_t)(((seq + jj) / NS) & 1), status, 0x52);
+            break;
+        }
+        seq += nch;
+        // reduce to the unit's 512 outputs: (row or column e >> 3, right-hand side e & 7)
+        const int w = tid >> 5, lane = tid & 31;
+        T o = T(0);
+        if (kind != 3) {
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int q = 0; q < CQ; ++q) acc[a][q] += __shfl_xor_sync(0xffffffffu, acc[a][q], 16);
+            if (lane < 16)
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int q = 0; q < CQ; ++q) red[(w * CT + 4 * g + a) * CQ + q] = acc[a][q];
+            __syncthreads();
+#pragma unroll
+            for (int ww = 0; ww < CH_NT / 32; ++ww) o += red[ww * CT * CQ + tid];
+        } else {
+            const int q = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) {
+                const T sum = warp_sum8<T>(acc[cc]);
+                if ((lane & 3) == 0) red[(4 * w + cc) * CQ + q] = sum;
+            }
+            __syncthreads();
+            o = red[tid];
+        }
+        const int r = tid >> 3;
+        if (kind == 0) {
+            if (rloc + r < bsz) atomicAdd(&Y[(s0 + rloc) * CQ + tid], o);
+        } else if (kind == 1) {
+            if ((long long)idx * CT + r < c.n) atomicAdd(&Bv[(long long)idx * CT * CQ + tid], -o);
+        } else if (kind == 2) {
+            if (rloc + r < bsz) atomicAdd(&X[(s0 + rloc) * CQ + tid], o);
+        } else {
+            atomicAdd(&Y[(long long)idx * CT * CQ + tid], -o);
+        }
+        __syncthreads();  // every update of the unit issued; vs / red free
+        if (tid == 0) {
+            // release: the unit's updates (ordered before by the barrier) precede the count
+            const int applied = bulk ? blk_slices(c.n, s) : 1;  // a bulk unit counts as all slices of its phase
+            if (kind == 0) red_release_add(&c.ydone[s * TPB + idx], 1);
+            else if (kind == 1) red_release_add(&c.cnt_f[idx], applied);
+            else if (kind == 2) red_release_add(&c.xdone[s * TPB + idx], 1);
+            else red_release_add(&c.cnt_b[idx], applied);
+            if (kind <= 1) red_release_add(fdone, 1);
+        }
+    }
+}
+
+// Bv(i, q) = B(i, q) for q < nr, 0 beyond (row-major, CQ per row)
+template <class T>
+__global__ void k_bis_pack(int n, int nr, const double* __restrict__ B, long long ldb, T* __restrict__ Bv)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)n * CQ;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long i = e / CQ;
+        const int q = (int)(e % CQ);
+        Bv[e] = q < nr ? (T)B[i + q * ldb] : T(0);
+    }
+}
+
+// B(i, q) = Bv(i, q), or NaN when a wait of the chain gave up
+template <class T>
+__global__ void k_bis_unpack(int n, int nr, const T* __restrict__ Bv, double* __restrict__ B, long long ldb,
+                             const int* __restrict__ status)
+{
+    const bool bad = *status != DDLAK_OK;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)n * nr;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long i = e % n;
+        const int q = (int)(e / n);
+        B[i + q * ldb] = bad ? __longlong_as_double(0x7ff8000000000000LL) : (double)__ldcg(Bv + i * CQ + q);
+    }
+}
+
+struct ChainLayout {
+    int S, Tt;
+    long long nf, nb;
+    size_t flag_bytes, vec_bytes;
+};
+
+ChainLayout chain_layout(int n, size_t elem)
+{
+    ChainLayout l{};
+    l.S = (int)ceil_div(n, BS);
+    l.Tt = (int)ceil_div(n, CT);
+    for (int g = 0; g < l.S; ++g) {
+        l.nf += group_units(n, l.S, l.Tt, true, g);
+        l.nb += group_units(n, l.S, l.Tt, false, g);
+    }
+    l.flag_bytes = ((size_t)(64 + 2 * l.Tt + 2 * l.S * TPB) * sizeof(int) + 255) / 256 * 256;
+    l.vec_bytes = ((size_t)n * CQ * elem + 255) / 256 * 256;
+    return l;
+}
+
+// workspace: [flags][Y][X][Bv]; the flags, Y and X start at zero
+template <class T>
+cudaError_t bis_chain_solve(int n, int nrhs, const float* L, long long ldl, const T* Dinv, double* B, long long ldb,
+                            void* work, cudaStream_t st)
+{
+    if (n > (1 << 30) / 2) return cudaErrorInvalidValue;  // TMA coordinates are 32-bit
+    const ChainLayout lay = chain_layout(n, sizeof(T));
+    char* w = static_cast<char*>(work);
+    int* ctl = reinterpret_cast<int*>(w);
+    T* Yv = reinterpret_cast<T*>(w + lay.flag_bytes);
+    T* Xv = reinterpret_cast<T*>(w + lay.flag_bytes + lay.vec_bytes);
+    T* Bv = reinterpret_cast<T*>(w + lay.flag_bytes + 2 * lay.vec_bytes);
+    Chain c{};
+    c.n = n;
+    c.S = lay.S;
+    c.Tt = lay.Tt;
+    c.nf = lay.nf;
+    c.total = lay.nf + lay.nb;
+    c.L = L;
+    c.ldl = ldl;
+    c.ctl = ctl;
+    c.cnt_f = ctl + 64;
+    c.ydone = c.cnt_f + lay.Tt;
+    c.cnt_b = c.ydone + lay.S * TPB;
+    c.xdone = c.cnt_b + lay.Tt;
+    const size_t smem = chain_smem<T>();
+    CUtensorMap mapL, mapLt, mapD;
+    const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    if (!tc::encode_colmajor_2d(&mapL, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, L, n, n, ldl, CT, chunk_cols<float>(),
+                                CU_TENSOR_MAP_SWIZZLE_NONE) ||
+        !tc::encode_colmajor_2d(&mapLt, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, L, n, n, ldl, PT_ROWS, CT,
+                                CU_TENSOR_MAP_SWIZZLE_NONE) ||
+        !tc::encode_colmajor_2d(&mapD, dt, (int)sizeof(T), Dinv, BS, (long long)lay.S * BS, BS, CT, chunk_cols<T>(),
+                                CU_TENSOR_MAP_SWIZZLE_NONE))
+        return cudaErrorInvalidValue;
+    static int grid = [&] {
+        cudaFuncSetAttribute(k_bis_chain<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int dev = 0, sms = 148, per = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bis_chain<T>, CH_NT, smem);
+        return sms * (per > 0 ? per : 1);
+    }();
+    const unsigned g = (unsigned)std::min<long long>(grid, c.total);
+    const unsigned gv = (unsigned)std::min<long long>(ceil_div((long long)n * CQ, 256), 1184);
     int launches = 0;
-    // forward: L y = b (y into Y)
-    for (int s = 0; s < S; ++s) {
-        const long long s0 = (long long)s * BS;
-        const int bsz = (int)((n - s0) < BS ? (n - s0) : BS);
-        k_bis_diag<NQ, true><<<(unsigned)ceil_div(bsz, BIS_NT / 32), BIS_NT, sm_vec, st>>>(n, nrhs, s, Dinv, B, ldb,
-                                                                                          Y, n);
-        ++launches;
-        const long long rest = n - s0 - bsz;
-        if (rest > 0) {
-            const long long tiles = ceil_div(rest, 64);
-            const int ks = split_for(tiles, 16, want);
-            const long long gx = tiles < ceil_div(want, ks) ? tiles : ceil_div(want, ks);
-            k_bis_panel<NQ><<<dim3((unsigned)gx, (unsigned)ks), BIS_NT, sm_panel, st>>>(n, nrhs, s, L, ldl, Y, B,
-                                                                                        ldb);
-            ++launches;
-        }
-    }
-    // backward: L^T x = y (x into B)
-    for (int s = S - 1; s >= 0; --s) {
-        const long long s0 = (long long)s * BS;
-        const int bsz = (int)((n - s0) < BS ? (n - s0) : BS);
-        k_bis_diag<NQ, false><<<(unsigned)ceil_div(bsz, BIS_NT / 32), BIS_NT, sm_vec, st>>>(n, nrhs, s, Dinv, Y, n,
-                                                                                           B, ldb);
-        ++launches;
-        if (s0 > 0) {
-            const long long tiles = ceil_div(s0, BIS_NT);
-            const int is = split_for(tiles, 16, want);
-            const long long gx = tiles < ceil_div(want, is) ? tiles : ceil_div(want, is);
-            k_bis_panel_t<NQ><<<dim3((unsigned)gx, (unsigned)is), BIS_NT, sm_vec, st>>>(n, nrhs, s, L, ldl, B, ldb,
-                                                                                        Y);
-            ++launches;
-        }
+    for (int r0 = 0; r0 < nrhs; r0 += CQ) {
+        const int nr = std::min(CQ, nrhs - r0);
+        cudaError_t e = cudaMemsetAsync(ctl, 0, lay.flag_bytes + 2 * lay.vec_bytes, st);
+        if (e != cudaSuccess) return e;
+        k_bis_pack<T><<<gv, 256, 0, st>>>(n, nr, B + r0 * ldb, ldb, Bv);
+        k_bis_chain<T><<<g, CH_NT, smem, st>>>(mapL, mapLt, mapD, c, Bv, Yv, Xv);
+        k_bis_unpack<T><<<gv, 256, 0, st>>>(n, nr, Xv, B + r0 * ldb, ldb, ctl);
+        launches += 3;
     }
     note_launches(launches);
     return cudaGetLastError();
@@ -337,26 +746,61 @@ extern "C" int ddlak_bis_inverse(int n, const void* L32, long long ldl, void* Di
     return (int)cudaGetLastError();
 }
 
+extern "C" int ddlak_bis_inverse_narrow(int n, const void* Dinv, void* Dinv32, void* stream)
+{
+    using namespace ddlak;
+    if (n <= 0) return 0;
+    if (!Dinv || !Dinv32) return (int)cudaErrorInvalidValue;
+    const long long count = (long long)ceil_div(n, BS) * BS * BS;
+    k_bis_narrow<<<1184, 256, 0, static_cast<cudaStream_t>(stream)>>>(count, static_cast<const double*>(Dinv),
+                                                                      static_cast<float*>(Dinv32));
+    note_launches(1);
+    return (int)cudaGetLastError();
+}
+
 extern "C" unsigned long long ddlak_bis_solve_workspace(int n, int nrhs)
 {
-    return ((unsigned long long)(n > 0 ? n : 0) * (nrhs > 0 ? nrhs : 0) * sizeof(double) + 255) / 256 * 256;
+    using namespace ddlak;
+    (void)nrhs;
+    if (n <= 0) return 256;
+    const ChainLayout l = chain_layout(n, sizeof(double));
+    return l.flag_bytes + 3 * l.vec_bytes;
 }
+
+namespace {
+int bis_check(int n, int nrhs, const void* L32, long long ldl, const void* Dinv, const void* B, long long ldb,
+              unsigned long long work_bytes)
+{
+    if (nrhs > 16 || !L32 || !Dinv || !B || ldb < n || ldl < n || (ldl & 3) ||
+        (reinterpret_cast<uintptr_t>(L32) & 15) || (reinterpret_cast<uintptr_t>(Dinv) & 15) ||
+        work_bytes < ddlak_bis_solve_workspace(n, nrhs))
+        return (int)cudaErrorInvalidValue;
+    return 0;
+}
+}  // namespace
 
 extern "C" int ddlak_bis_solve(int n, int nrhs, const void* L32, long long ldl, const void* Dinv, void* B,
                                long long ldb, void* work, unsigned long long work_bytes, void* stream)
 {
     using namespace ddlak;
     if (n <= 0 || nrhs <= 0) return 0;
-    if (nrhs > 16 || !L32 || !Dinv || !B || ldb < n || ldl < n || (ldl & 3) ||
-        (reinterpret_cast<uintptr_t>(L32) & 15) || work_bytes < ddlak_bis_solve_workspace(n, nrhs))
-        return (int)cudaErrorInvalidValue;
+    if (int r = bis_check(n, nrhs, L32, ldl, Dinv, B, ldb, work_bytes)) return r;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const double nd = n, rd = nrhs;
     ProfScope ps(PK_POTRS_FUSED, st, 2.0 * nd * nd * rd, 4.0 * nd * (nd + 1));
-    const float* L = static_cast<const float*>(L32);
-    const double* D = static_cast<const double*>(Dinv);
-    double* b = static_cast<double*>(B);
-    double* Y = static_cast<double*>(work);
-    if (nrhs <= 8) return (int)bis_solve_t<8>(n, nrhs, L, ldl, D, b, ldb, Y, st);
-    return (int)bis_solve_t<16>(n, nrhs, L, ldl, D, b, ldb, Y, st);
+    return (int)bis_chain_solve<double>(n, nrhs, static_cast<const float*>(L32), ldl, static_cast<const double*>(Dinv),
+                                        static_cast<double*>(B), ldb, work, st);
+}
+
+extern "C" int ddlak_bis_solve_f32(int n, int nrhs, const void* L32, long long ldl, const void* Dinv32, void* B,
+                                   long long ldb, void* work, unsigned long long work_bytes, void* stream)
+{
+    using namespace ddlak;
+    if (n <= 0 || nrhs <= 0) return 0;
+    if (int r = bis_check(n, nrhs, L32, ldl, Dinv32, B, ldb, work_bytes)) return r;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const double nd = n, rd = nrhs;
+    ProfScope ps(PK_POTRS_FUSED, st, 2.0 * nd * nd * rd, 4.0 * nd * (nd + 1));
+    return (int)bis_chain_solve<float>(n, nrhs, static_cast<const float*>(L32), ldl, static_cast<const float*>(Dinv32),
+                                       static_cast<double*>(B), ldb, work, st);
 }

@@ -125,6 +125,12 @@ __device__ __forceinline__ void st_release(int* p, int v)
     asm volatile("st.release.gpu.global.b32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
 
+// *p += v with release semantics at GPU scope (no return value)
+__device__ __forceinline__ void red_release_add(int* p, int v)
+{
+    asm volatile("red.release.gpu.global.add.s32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
+
 // Spin (one thread) until *flag >= want or the budget runs out.  Returns false
 // on timeout after recording DDLAK_WAIT_TIMEOUT in *status.
 __device__ __forceinline__ bool bounded_wait_geq(const int* flag, int want, int* status)

@@ -21,6 +21,34 @@ namespace tc {
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
+// Host: a 2-D tiled TMA map over a column-major matrix (rows contiguous):
+// `rows` x `cols` elements of `esize` bytes, columns `ld` elements apart, box
+// box_rows x box_cols, zero fill outside.  False when the driver entry point
+// is missing or the encoding is rejected (base not 16-byte aligned, ld*esize
+// not a multiple of 16, box inner extent not a multiple of 16 bytes, ...).
+inline bool encode_colmajor_2d(CUtensorMap* map, CUtensorMapDataType dt, int esize, const void* p, long long rows,
+                               long long cols, long long ld, int box_rows, int box_cols, CUtensorMapSwizzle sw)
+{
+    using Fn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+                            const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                            CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static Fn fn = [] {
+        void* q = nullptr;
+        cudaDriverEntryPointQueryResult r;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &q, cudaEnableDefault, &r) == cudaSuccess &&
+            r == cudaDriverEntryPointSuccess)
+            return reinterpret_cast<Fn>(q);
+        return static_cast<Fn>(nullptr);
+    }();
+    if (!fn || (reinterpret_cast<uintptr_t>(p) & 15) || ((ld * esize) & 15) || rows < 1 || cols < 1) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)rows, (cuuint64_t)cols};
+    const cuuint64_t strides[1] = {(cuuint64_t)(ld * esize)};
+    const cuuint32_t box[2] = {(cuuint32_t)box_rows, (cuuint32_t)box_cols};
+    const cuuint32_t estr[2] = {1u, 1u};
+    return fn(map, dt, 2, const_cast<void*>(p), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // ---- mbarrier ---------------------------------------------------------------
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
 {
@@ -61,6 +89,13 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
             smem_u32(dst)),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
         : "memory");
+}
+// Prefetch a 2-D box into L2 (no shared-memory destination, no completion)
+__device__ __forceinline__ void tma_prefetch_l2_2d(const CUtensorMap* map, int x, int y)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y)
+                 : "memory");
 }
 // TMA store of a 2-D box from shared memory (bulk group; no multicast)
 __device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void* src, int x, int y)
