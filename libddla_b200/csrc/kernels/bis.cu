@@ -6,12 +6,12 @@
 //   forward,  phase s = 0..S-1:   y_s = inv(L_ss) b_s;        b_i -= L_is y_s   (i > s)
 //   backward, phase s = S-1..0:   x_s = inv(L_ss)^T y_s;      y_j -= L_sj^T x_s (j < s)
 // run by ONE persistent kernel (k_bis_chain) over a queue of units in that
-// order.  A unit is a 64-row (or 64-column) tile times one 256-wide slice of
-// the inner dimension (KS): at most 64 KB of FP32 matrix, two 32 KB chunks that
-// TMA streams into shared memory while the unit waits for its inputs.  A phase
-// lists its diagonal units (64-row parts x slices) and then its panel units,
-// the tiles the next diagonal block needs first.  A CTA takes the next unit
-// from an atomic counter, starts its matrix loads, waits (bounded) on the
+// order.  A unit on the chain from one diagonal block to the next is a 64-row
+// (or 64-column) tile times one 256-wide slice of the inner dimension (KS):
+// 64 KB of FP32 matrix, one TMA box streamed into shared memory while the unit
+// waits for its inputs; the rest of each panel goes in whole-block bulk units
+// (four boxes) that trail the chain (queue order below).  A CTA takes the next
+// unit from an atomic counter, starts its matrix loads, waits (bounded) on the
 // counters its inputs are published on, computes, folds its partial product
 // into the target vector with atomics and counts itself done:
 //   cnt_f[t]   forward panel units applied to tile t of b    (complete at 4 per earlier phase)
