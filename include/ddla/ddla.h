@@ -49,11 +49,32 @@ void pposv(const DdlaHandle_t& handle, char side, char uplo, char trans, int n, 
 template <typename T>
 void potrf(const DdlaHandle_t& handle, char uplo, int n, T* A, int lda, int* info);
 
+// Cholesky from the bottom-right corner (reference ddla.h:1090-1093, 1117-1121):
+// uplo 'U' computes A = U*U^H in the upper triangle, 'L' A = L^H*L in the
+// lower one; the other triangle and the padding rows are left as they were.
+// info is 0 or the (1-based) index of the first pivot, counted from the bottom,
+// that is not positive; A's selected triangle is then unspecified.  Both
+// return with the handle's stream synchronised.  potrf_bottom_right throws
+// std::runtime_error on a bad argument (potrf_bottom_right.cpp:171-187);
+// ppotrf_bottom_right validates the descriptor like ppotrf and throws
+// std::invalid_argument (ppotrf_bottom_right.cpp:62-70).
+template <typename T>
+void potrf_bottom_right(char uplo, int n, T* A, int lda, int& info, const DdlaHandle_t& handle);
+template <typename T>
+void ppotrf_bottom_right(const DdlaHandle_t& handle, char uplo, int n, T* A, const int* descA, int& info);
+
 // Principal log of prod(A(i,i)), i < n, as (log magnitude, phase in (-pi, pi]).
 // Zero diagonal -> (-inf, 0); nonfinite diagonal throws std::domain_error and
 // leaves result unchanged.  Completes before returning.
 template <typename T>
 void diag_logdet(const DdlaHandle_t& handle, int n, const T* A, int lda, std::complex<real_type_t<T>>& result);
+
+// The same through an int[9] descriptor (reference ddla.h:2914-2915,
+// src/PBLAS/pdiag_logdet.cpp:11-48): n <= M_, N_, leading dimension LLD_;
+// std::invalid_argument for a bad order or a null local matrix.
+template <typename T>
+void pdiag_logdet(const DdlaHandle_t& handle, int n, const T* A, const int* descA,
+                  std::complex<real_type_t<T>>& result);
 
 // ppotrs<double> that allocates nothing (no reference counterpart): for callers
 // that cannot allocate device memory while running.  The solve's flags live in
@@ -77,6 +98,13 @@ void ppotrf_run(const DdlaHandle_t& handle, char uplo, int n, T* A, int ia, int 
 template <typename T>
 void ppotrs_workspace_size(const DdlaHandle_t& handle, char side, int n, int nrhs, const int* descA,
                            const int* descB, std::size_t* backend_bytes, std::size_t* host_bytes);
+// (src/Cholesky/cholesky_workspace.h:163-200)
+template <typename T>
+void ppotrf_bottom_right_workspace_size(const DdlaHandle_t& handle, char uplo, int n, T* A, const int* descA,
+                                        std::size_t* backend_bytes, std::size_t* host_bytes);
+template <typename T>
+void ppotrf_bottom_right_run(const DdlaHandle_t& handle, char uplo, int n, T* A, const int* descA, int& info,
+                             void* backend_work, std::size_t backend_bytes, void* host_work, std::size_t host_bytes);
 template <typename T>
 void ppotrs_run(const DdlaHandle_t& handle, char side, char uplo, char trans, int n, int nrhs, const T* A,
                 const int* descA, T* B, const int* descB, void* backend_work, std::size_t backend_bytes,

@@ -100,6 +100,18 @@ int ddla_d_potrf(void* handle, char uplo, int n, void* A, int lda, void* info);
 int ddla_c_potrf(void* handle, char uplo, int n, void* A, int lda, void* info);
 int ddla_z_potrf(void* handle, char uplo, int n, void* A, int lda, void* info);
 
+/* ddla_c_api.cpp:1191-1225: bottom-right Cholesky, A = U*U^H ('U') or L^H*L ('L');
+ * info (host int*) is 0 or the failed pivot's index */
+int ddla_s_potrf_bottom_right(void* handle, char uplo, int n, void* A, int lda, int* info);
+int ddla_d_potrf_bottom_right(void* handle, char uplo, int n, void* A, int lda, int* info);
+int ddla_c_potrf_bottom_right(void* handle, char uplo, int n, void* A, int lda, int* info);
+int ddla_z_potrf_bottom_right(void* handle, char uplo, int n, void* A, int lda, int* info);
+/* ddla_c_api.cpp:1227-1261: the same through an int[9] descriptor (1x1 grid) */
+int ddla_s_ppotrf_bottom_right(void* handle, char uplo, int n, void* A, const int* descA, int* info);
+int ddla_d_ppotrf_bottom_right(void* handle, char uplo, int n, void* A, const int* descA, int* info);
+int ddla_c_ppotrf_bottom_right(void* handle, char uplo, int n, void* A, const int* descA, int* info);
+int ddla_z_ppotrf_bottom_right(void* handle, char uplo, int n, void* A, const int* descA, int* info);
+
 /* diag_logdet has no C export in the reference (its C++ template is
  * include/ddla/ddla.h:2900-2902); these add one.  result receives two reals
  * of the matrix's real type: log magnitude, phase in (-pi, pi]. */
@@ -107,6 +119,12 @@ int ddla_s_diag_logdet(void* handle, int n, const void* A, int lda, void* result
 int ddla_d_diag_logdet(void* handle, int n, const void* A, int lda, void* result);
 int ddla_c_diag_logdet(void* handle, int n, const void* A, int lda, void* result);
 int ddla_z_diag_logdet(void* handle, int n, const void* A, int lda, void* result);
+/* pdiag_logdet (reference include/ddla/ddla.h:2914-2915, no C export there):
+ * the same through an int[9] descriptor, leading dimension LLD_ */
+int ddla_s_pdiag_logdet(void* handle, int n, const void* A, const int* descA, void* result);
+int ddla_d_pdiag_logdet(void* handle, int n, const void* A, const int* descA, void* result);
+int ddla_c_pdiag_logdet(void* handle, int n, const void* A, const int* descA, void* result);
+int ddla_z_pdiag_logdet(void* handle, int n, const void* A, const int* descA, void* result);
 
 /* The reference's internal check / size / run split of ppotrf and ppotrs
  * (src/Cholesky/cholesky_workspace.h:133-154, 207-222) exported so a caller can

@@ -26,6 +26,15 @@ extern "C" {
  * and then to the order of the first non-positive-definite leading minor. */
 int ddlak_potrf(char type, char uplo, int n, void* A, long long lda, int* dinfo, void* stream);
 
+/* In place A <- J A J on the leading n x n (element (i, j) trades places with
+ * (n-1-i, n-1-j); J the order-reversing permutation).  With it the bottom-right
+ * factorization of src/Cholesky/potrf_bottom_right.cpp:208-256 (A = U U^H or
+ * L^H L from the last column; its per-block reverse packing,
+ * potrf_bottom_right_transform.cpp:18-47) is ddlak_potrf of the opposite
+ * triangle between two swaps.  The opposite triangle and rows n..lda-1 are
+ * permuted and restored, never altered. */
+int ddlak_reverse_swap(char type, int n, void* A, long long lda, void* stream);
+
 /* Bytes of device scratch ddlak_potrs needs for (n, nrhs). */
 unsigned long long ddlak_potrs_workspace(int n, int nrhs);
 

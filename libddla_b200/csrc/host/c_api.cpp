@@ -122,6 +122,20 @@ int diag_logdet_impl(void* handle, int n, const void* A, int lda, void* result)
 }
 
 template <class T>
+int pdiag_logdet_impl(void* handle, int n, const void* A, const int* descA, void* result)
+{
+    using R = ddla::real_type_t<T>;
+    return run(handle, [&](ddla::DdlaHandle_t h) -> int {
+        if (result == nullptr) return ST_INVALID_VALUE;
+        std::complex<R> r;
+        std::memcpy(&r, result, sizeof(r));
+        ddla::pdiag_logdet<T>(h, n, static_cast<const T*>(A), descA, r);
+        std::memcpy(result, &r, sizeof(r));
+        return ST_SUCCESS;
+    });
+}
+
+template <class T>
 int ppotrf_ws_impl(void* handle, char uplo, int n, const int* descA, long long* bytes)
 {
     return run(handle, [&](ddla::DdlaHandle_t h) -> int {
@@ -361,9 +375,29 @@ int ddla_c_bcast_dims(int, int* m, int* n, int* type_char, int root)
             return ST_SUCCESS;                                                                                       \
         });                                                                                                          \
     }                                                                                                                \
+    int ddla_##P##_potrf_bottom_right(void* handle, char uplo, int n, void* A, int lda, int* info)                 \
+    {                                                                                                                \
+        return run(handle, [&](ddla::DdlaHandle_t h) -> int {                                                        \
+            if (!info) return ST_INVALID_VALUE;                                                                      \
+            ddla::potrf_bottom_right<T>(uplo, n, static_cast<T*>(A), lda, *info, h);                                 \
+            return ST_SUCCESS;                                                                                       \
+        });                                                                                                          \
+    }                                                                                                                \
+    int ddla_##P##_ppotrf_bottom_right(void* handle, char uplo, int n, void* A, const int* descA, int* info)       \
+    {                                                                                                                \
+        return run(handle, [&](ddla::DdlaHandle_t h) -> int {                                                        \
+            if (!info) return ST_INVALID_VALUE;                                                                      \
+            ddla::ppotrf_bottom_right<T>(h, uplo, n, static_cast<T*>(A), descA, *info);                              \
+            return ST_SUCCESS;                                                                                       \
+        });                                                                                                          \
+    }                                                                                                                \
     int ddla_##P##_diag_logdet(void* handle, int n, const void* A, int lda, void* result)                          \
     {                                                                                                                \
         return diag_logdet_impl<T>(handle, n, A, lda, result);                                                       \
+    }                                                                                                                \
+    int ddla_##P##_pdiag_logdet(void* handle, int n, const void* A, const int* descA, void* result)                \
+    {                                                                                                                \
+        return pdiag_logdet_impl<T>(handle, n, A, descA, result);                                                    \
     }                                                                                                                \
     int ddla_##P##_ppotrf_workspace_size(void* handle, char uplo, int n, const int* descA, long long* bytes)       \
     {                                                                                                                \

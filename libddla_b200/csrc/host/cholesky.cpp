@@ -69,6 +69,28 @@ void pposv_check(const DdlaHandle_t& h, char side, char uplo, char trans, int n,
     if (ib != 1 || jb != 1) throw std::invalid_argument("pposv: offsets must be one");
 }
 
+// potrf_bottom_right_check (src/Cholesky/potrf_bottom_right.cpp:171-187): real throws, runtime_error
+void potrf_bottom_right_check(const DdlaHandle_t& h, char uplo, int n, const void* A, int lda)
+{
+    detail::require_gpu(h, "potrf_bottom_right");
+    if (uplo != 'U' && uplo != 'L') throw std::runtime_error("potrf_bottom_right: uplo must be 'U' or 'L'");
+    if (n < 0) throw std::runtime_error("potrf_bottom_right: negative matrix size");
+    if (n == 0) return;
+    if (A == nullptr) throw std::runtime_error("potrf_bottom_right: null A");
+    if (lda < n) throw std::runtime_error("potrf_bottom_right: lda too small");
+}
+
+// ppotrf_bottom_right_check (src/Cholesky/ppotrf_bottom_right.cpp:62-70) on a 1x1 grid
+void ppotrf_bottom_right_check(const DdlaHandle_t& h, char uplo, int n, const void* A, const int* d)
+{
+    detail::check_desc(d, h);
+    detail::require_gpu(h, "ppotrf_bottom_right");
+    if ((uplo != 'L' && uplo != 'U') || n < 0 || n > d[DDLA_M_] || n > d[DDLA_N_] || d[DDLA_MB_] != d[DDLA_NB_] ||
+        h->nprows_ != h->npcols_)
+        throw std::invalid_argument("ppotrf_bottom_right: invalid triangle, dimensions, blocks or grid");
+    if (n && !A) throw std::invalid_argument("ppotrf_bottom_right: null local matrix");
+}
+
 int read_device_int(const DdlaHandle_t& h, const int* dptr)
 {
     detail::cuda_check(cudaMemcpyAsync(h->host_word, dptr, sizeof(int), cudaMemcpyDeviceToHost, h->stream),
@@ -130,6 +152,70 @@ void ppotrs_run(const DdlaHandle_t& h, char side, char uplo, char, int n, int nr
 }
 
 }  // namespace cholesky_impl
+
+namespace cholesky_impl {
+
+// The bottom-right factorization (src/Cholesky/potrf_bottom_right.cpp:208-256 on one
+// rank): J A J (J reverses the order) is factored by the standard kernels on the
+// opposite triangle, then swapped back.  A pivot that fails at reversed position k
+// is the pivot n - k + 1 counted from the top, the reference's
+// global_offset + n - solver_info + 1 (potrf_bottom_right.cpp:97).
+template <typename T>
+void bottom_right_core(const DdlaHandle_t& h, char uplo, int n, T* A, long long lda, int& info, void* backend_work,
+                       std::size_t backend_bytes)
+{
+    info = 0;
+    if (n == 0) return;
+    if (backend_bytes < detail::padded_bytes<int>(1) || backend_work == nullptr)
+        throw std::invalid_argument("ppotrf_bottom_right: workspace smaller than ppotrf_bottom_right_workspace_size");
+    char* w = static_cast<char*>(backend_work);
+    int* dinfo = detail::take<int>(w, 1);
+    detail::kernel_check(ddlak_reverse_swap(tcode<T>(), n, A, lda, h->stream), "reverse swap");
+    detail::kernel_check(ddlak_potrf(tcode<T>(), uplo == 'U' ? 'L' : 'U', n, A, lda, dinfo, h->stream),
+                         "potrf kernels");
+    detail::kernel_check(ddlak_reverse_swap(tcode<T>(), n, A, lda, h->stream), "reverse swap");
+    const int r = read_device_int(h, dinfo);
+    info = r == 0 ? 0 : n - r + 1;
+}
+
+template <typename T>
+void ppotrf_bottom_right_workspace_size(const DdlaHandle_t&, char, int n, T*, const int*, std::size_t* backend_bytes,
+                                        std::size_t* host_bytes)
+{
+    *backend_bytes = n > 0 ? detail::padded_bytes<int>(1) : 0;  // the device info word
+    *host_bytes = 0;
+}
+
+template <typename T>
+void ppotrf_bottom_right_run(const DdlaHandle_t& h, char uplo, int n, T* A, const int* descA, int& info,
+                             void* backend_work, std::size_t backend_bytes, void*, std::size_t)
+{
+    bottom_right_core<T>(h, uplo, n, A, descA[DDLA_LLD_], info, backend_work, backend_bytes);
+}
+
+}  // namespace cholesky_impl
+
+template <typename T>
+void potrf_bottom_right(char uplo, int n, T* A, int lda, int& info, const DdlaHandle_t& handle)
+{
+    potrf_bottom_right_check(handle, uplo, n, A, lda);
+    info = 0;
+    if (n == 0) return;
+    detail::DeviceScratch work(handle, detail::padded_bytes<int>(1));
+    cholesky_impl::bottom_right_core<T>(handle, uplo, n, A, lda, info, work.data(), detail::padded_bytes<int>(1));
+}
+
+template <typename T>
+void ppotrf_bottom_right(const DdlaHandle_t& handle, char uplo, int n, T* A, const int* descA, int& info)
+{
+    ppotrf_bottom_right_check(handle, uplo, n, A, descA);
+    info = 0;
+    if (n == 0) return;
+    std::size_t bb = 0, hb = 0;
+    cholesky_impl::ppotrf_bottom_right_workspace_size<T>(handle, uplo, n, A, descA, &bb, &hb);
+    detail::DeviceScratch work(handle, bb);
+    cholesky_impl::ppotrf_bottom_right_run<T>(handle, uplo, n, A, descA, info, work.data(), bb, nullptr, 0);
+}
 
 template <typename T>
 void ppotrf(const DdlaHandle_t& handle, char uplo, int n, T* A, int ia, int ja, const int* descA, int& info)
@@ -211,18 +297,19 @@ void potrf(const DdlaHandle_t& h, char uplo, int n, T* A, int lda, int* info)
     detail::kernel_check(ddlak_potrf(tcode<T>(), u, n, A, lda, info, h->stream), "potrf kernels");
 }
 
+namespace {
+// DiagLogTerm / DiagLogJoin over the diagonal, then finish_diagonal_log
+// (src/diag_logdet_impl.h:42-113); `who` names the routine in the domain_error.
 template <typename T>
-void diag_logdet(const DdlaHandle_t& h, int n, const T* a, int lda, std::complex<real_type_t<T>>& result)
+void logdet_core(const DdlaHandle_t& h, int n, const T* a, long long lda, std::complex<real_type_t<T>>& result,
+                 const char* who)
 {
     using R = real_type_t<T>;
-    detail::require_gpu(h, "diag_logdet");
-    if (n < 0 || lda < std::max(1, n) || (n > 0 && !a))
-        throw std::invalid_argument("diag_logdet: invalid order, leading dimension or pointer");
     if (n > 0) {
         // the reference's check_diag_span (src/diag_logdet_impl.h:33-40)
         const auto last = std::uint64_t(n - 1) * std::uint64_t(lda) + std::uint64_t(n) - 1;
         if (last > std::uint64_t(std::numeric_limits<std::ptrdiff_t>::max()) / sizeof(T))
-            throw std::overflow_error("diag_logdet: matrix address span is not representable");
+            throw std::overflow_error(std::string(who) + ": matrix address span is not representable");
     }
     double magnitude = 0, phase = 0;
     int flags = 0;
@@ -242,7 +329,7 @@ void diag_logdet(const DdlaHandle_t& h, int n, const T* a, int lda, std::complex
         phase = st.phase;
         flags = st.flags;
     }
-    if (flags & 1) throw std::domain_error("diag_logdet: nonfinite diagonal");
+    if (flags & 1) throw std::domain_error(std::string(who) + ": nonfinite diagonal");
     // finish_diagonal_log (src/diag_logdet_impl.h:104-113)
     if (flags & 2) {
         result = {-std::numeric_limits<R>::infinity(), R(0)};
@@ -253,6 +340,30 @@ void diag_logdet(const DdlaHandle_t& h, int n, const T* a, int lda, std::complex
     if (phase <= -pi) phase = pi;
     result = {static_cast<R>(magnitude), static_cast<R>(phase)};
 }
+}  // namespace
+
+template <typename T>
+void diag_logdet(const DdlaHandle_t& h, int n, const T* a, int lda, std::complex<real_type_t<T>>& result)
+{
+    detail::require_gpu(h, "diag_logdet");
+    if (n < 0 || lda < std::max(1, n) || (n > 0 && !a))
+        throw std::invalid_argument("diag_logdet: invalid order, leading dimension or pointer");
+    logdet_core<T>(h, n, a, lda, result, "diag_logdet");
+}
+
+// The descriptor form (src/PBLAS/pdiag_logdet.cpp:11-48) on a 1x1 grid: the local
+// block is the whole matrix and the all-reduce of the four partial sums is the
+// identity, so the result is diag_logdet's with LLD_ as the leading dimension.
+template <typename T>
+void pdiag_logdet(const DdlaHandle_t& h, int n, const T* a, const int* desc, std::complex<real_type_t<T>>& result)
+{
+    detail::require_gpu(h, "pdiag_logdet");
+    detail::check_desc(desc, h);
+    if (n < 0 || n > desc[DDLA_M_] || n > desc[DDLA_N_])
+        throw std::invalid_argument("pdiag_logdet: order exceeds descriptor");
+    if (n > 0 && !a) throw std::invalid_argument("pdiag_logdet: null local matrix");
+    logdet_core<T>(h, n, a, desc[DDLA_LLD_], result, "pdiag_logdet");
+}
 
 #define DDLA_INSTANTIATE(T)                                                                                          \
     template void ppotrf<T>(const DdlaHandle_t&, char, int, T*, int, int, const int*, int&);                         \
@@ -261,6 +372,7 @@ void diag_logdet(const DdlaHandle_t& h, int n, const T* a, int lda, std::complex
                            const int*, int&);                                                                        \
     template void potrf<T>(const DdlaHandle_t&, char, int, T*, int, int*);                                          \
     template void diag_logdet<T>(const DdlaHandle_t&, int, const T*, int, std::complex<real_type_t<T>>&);           \
+    template void pdiag_logdet<T>(const DdlaHandle_t&, int, const T*, const int*, std::complex<real_type_t<T>>&);   \
     template void cholesky_impl::ppotrf_workspace_size<T>(const DdlaHandle_t&, char, int, const T*, const int*,      \
                                                           std::size_t*, std::size_t*);                               \
     template void cholesky_impl::ppotrf_run<T>(const DdlaHandle_t&, char, int, T*, int, int, const int*, int&,       \
@@ -268,7 +380,13 @@ void diag_logdet(const DdlaHandle_t& h, int n, const T* a, int lda, std::complex
     template void cholesky_impl::ppotrs_workspace_size<T>(const DdlaHandle_t&, char, int, int, const int*,           \
                                                           const int*, std::size_t*, std::size_t*);                   \
     template void cholesky_impl::ppotrs_run<T>(const DdlaHandle_t&, char, char, char, int, int, const T*,           \
-                                               const int*, T*, const int*, void*, std::size_t, void*, std::size_t);
+                                               const int*, T*, const int*, void*, std::size_t, void*, std::size_t); \
+    template void potrf_bottom_right<T>(char, int, T*, int, int&, const DdlaHandle_t&);                             \
+    template void ppotrf_bottom_right<T>(const DdlaHandle_t&, char, int, T*, const int*, int&);                     \
+    template void cholesky_impl::ppotrf_bottom_right_workspace_size<T>(const DdlaHandle_t&, char, int, T*,           \
+                                                                       const int*, std::size_t*, std::size_t*);     \
+    template void cholesky_impl::ppotrf_bottom_right_run<T>(const DdlaHandle_t&, char, int, T*, const int*, int&,    \
+                                                            void*, std::size_t, void*, std::size_t);
 
 DDLA_INSTANTIATE(float)
 DDLA_INSTANTIATE(double)

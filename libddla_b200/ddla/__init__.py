@@ -17,7 +17,8 @@ from .backend import Backend, Communication, Handle  # noqa: F401
 from .layout import ProcessorLayout  # noqa: F401
 from .matrix import DistributedMatrix  # noqa: F401
 from . import autograd, batched  # noqa: F401
-from .ops import diag_logdet, gather, potrf, pposv, pposv_mixed, ppotrf, ppotrs, scatter  # noqa: F401
+from .ops import (diag_logdet, gather, pdiag_logdet, potrf, potrf_bottom_right, pposv, pposv_mixed, ppotrf,  # noqa: F401
+                  ppotrf_bottom_right, ppotrs, scatter)
 
 
 def finalize():

@@ -1,5 +1,6 @@
 """Cholesky-path routines -- mirror of ppotrf / ppotrs / pposv in the reference's
-python/ddla/ops.py:113-143, plus potrf, diag_logdet and pposv_mixed."""
+python/ddla/ops.py:113-143, plus potrf, potrf_bottom_right / ppotrf_bottom_right,
+diag_logdet / pdiag_logdet and pposv_mixed."""
 from __future__ import annotations
 
 import ctypes
@@ -53,6 +54,37 @@ def potrf(handle, type_char: str, uplo: str, n: int, A_ptr: int, lda: int, dinfo
     """LAPACK-style potrf with a DEVICE info pointer (asynchronous on the handle's stream)."""
     f = getattr(C.lib, f"ddla_{type_char}_potrf")
     C.check_status(f(handle.ptr, _ch(uplo), int(n), A_ptr, int(lda), dinfo_ptr), f"ddla_{type_char}_potrf")
+
+
+def potrf_bottom_right(handle, type_char: str, uplo: str, n: int, A_ptr: int, lda: int) -> int:
+    """Cholesky from the bottom-right corner in place (A = U U^H for 'U', L^H L for 'L');
+    returns info (0, or the index of the failed pivot).  The binding of
+    ddla_?_potrf_bottom_right (the reference's fortran/ddla_c_api.cpp:1191-1225)."""
+    info = ctypes.c_int(0)
+    f = getattr(C.lib, f"ddla_{type_char}_potrf_bottom_right")
+    C.check_status(f(handle.ptr, _ch(uplo), int(n), A_ptr, int(lda), ctypes.byref(info)),
+                   f"ddla_{type_char}_potrf_bottom_right")
+    return info.value
+
+
+def ppotrf_bottom_right(A: DistributedMatrix, uplo: str = "U") -> Tuple[DistributedMatrix, int]:
+    """Bottom-right Cholesky of a descriptor-described matrix in place; returns (A, info)."""
+    info = ctypes.c_int(0)
+    f = getattr(C.lib, f"ddla_{A.type_char}_ppotrf_bottom_right")
+    C.check_status(f(A.handle.ptr, _ch(uplo), A.n, A.data_ptr, A.desc.ctypes.data, ctypes.byref(info)),
+                   f"ddla_{A.type_char}_ppotrf_bottom_right")
+    return A, info.value
+
+
+def pdiag_logdet(A: DistributedMatrix, n: int = -1) -> complex:
+    """diag_logdet through A's descriptor (ddla_?_pdiag_logdet; the reference's
+    src/PBLAS/pdiag_logdet.cpp on a 1x1 grid)."""
+    n = A.n if n < 0 else n
+    out = np.zeros(2, dtype=np.float32 if A.type_char in "sc" else np.float64)
+    f = getattr(C.lib, f"ddla_{A.type_char}_pdiag_logdet")
+    C.check_status(f(A.handle.ptr, int(n), A.data_ptr, A.desc.ctypes.data, out.ctypes.data),
+                   f"ddla_{A.type_char}_pdiag_logdet")
+    return complex(float(out[0]), float(out[1]))
 
 
 def diag_logdet(A: DistributedMatrix, n: int = -1) -> complex:

@@ -11,6 +11,12 @@
  *              with first/second from src/Cholesky/ppotrs.cpp:44-48, reached via
  *              src/PBLAS/ptrtrs.cpp:150-155 and src/BLAS/trsm.cpp:137-144
  *   pposv   -> ppotrf, then ppotrs when info == 0  src/Cholesky/pposv.cpp:22-40
+ *   potrf_bottom_right -> the blocked loop of src/Cholesky/potrf_bottom_right.cpp:208-256
+ *              (128-blocks from the bottom-right corner: reverse-pack the block
+ *              onto the opposite triangle, potrf_bottom_right_transform.cpp:18-47,
+ *              ?potrf of that triangle, map back, potrf_bottom_right.cpp:77-107;
+ *              then ?trsm of the panel and ?syrk/?herk of the leading block,
+ *              potrf_bottom_right.cpp:27-56, 233-252)
  *   diag_logdet -> DiagLogTerm / DiagLogJoin / finish_diagonal_log,
  *              src/diag_logdet_impl.h:42-113, summed in index order as the
  *              sequential CPU loop of src/diag_logdet.cpp:12-38 does.
@@ -25,6 +31,7 @@
 #include <float.h>
 #include <math.h>
 #include <stddef.h>
+#include <stdlib.h>
 
 #define IDX(i, j, ld) ((size_t)(i) + (size_t)(j) * (size_t)(ld))
 
@@ -180,6 +187,57 @@
     {                                                                                                       \
         int info = oracle_##P##_potrf(uplo, n, A, lda);                                                     \
         if (info == 0) oracle_##P##_ppotrs(side, uplo, n, nrhs, A, lda, B, ldb);                            \
+        return info;                                                                                        \
+    }                                                                                                       \
+                                                                                                            \
+    /* A = U U^H ('U') or L^H L ('L') from the bottom-right corner.  Returns info: 0, or           \
+       block_start + block_n - solver_info + 1 for the first block whose ?potrf fails (that block is \
+       left as it was, the loop stops), potrf_bottom_right.cpp:89-99, 224-226. */                     \
+    int oracle_##P##_potrf_bottom_right(char uplo, int n, T* A, int lda)                                    \
+    {                                                                                                       \
+        const int NB = 128;                                                                                 \
+        const int upper = (uplo == 'U');                                                                    \
+        int b0, r, c, i, j, k, info = 0;                                                                    \
+        T* work;                                                                                            \
+        if (n <= 0) return 0;                                                                               \
+        work = (T*)malloc(sizeof(T) * (size_t)NB * NB);                                                     \
+        if (!work) return -1;                                                                               \
+        for (b0 = ((n - 1) / NB) * NB; b0 >= 0; b0 -= NB) {                                                 \
+            const int bn = (n - b0) < NB ? (n - b0) : NB;                                                   \
+            T* D = A + IDX(b0, b0, lda);                                                                    \
+            int si;                                                                                         \
+            for (c = 0; c < bn; ++c) /* the selected triangle, reversed, onto the opposite one of work */ \
+                for (r = 0; r < bn; ++r)                                                                    \
+                    if (upper ? r >= c : r <= c) work[IDX(r, c, bn)] = D[IDX(bn - 1 - r, bn - 1 - c, lda)]; \
+            si = oracle_##P##_potrf(upper ? 'L' : 'U', bn, work, bn);                                       \
+            if (si != 0) { info = b0 + bn - si + 1; break; }                                                \
+            for (c = 0; c < bn; ++c)                                                                        \
+                for (r = 0; r < bn; ++r)                                                                    \
+                    if (upper ? r <= c : r >= c) D[IDX(r, c, lda)] = work[IDX(bn - 1 - r, bn - 1 - c, bn)]; \
+            if (b0 == 0) continue;                                                                          \
+            if (upper) {                                                                                    \
+                T* Pn = A + IDX(0, b0, lda); /* b0 x bn: Pn := Pn inv(D^H), then A00 -= Pn Pn^H (upper) */  \
+                oracle_##P##_trsm('R', 'U', 'C', b0, bn, D, lda, Pn, lda);                                  \
+                for (j = 0; j < b0; ++j)                                                                    \
+                    for (i = 0; i <= j; ++i) {                                                              \
+                        T s = 0;                                                                            \
+                        for (k = 0; k < bn; ++k) s += Pn[IDX(i, k, lda)] * CONJ(Pn[IDX(j, k, lda)]);        \
+                        A[IDX(i, j, lda)] -= s;                                                             \
+                        if (i == j) A[IDX(i, j, lda)] = REAL(A[IDX(i, j, lda)]);                            \
+                    }                                                                                       \
+            } else {                                                                                        \
+                T* Pn = A + IDX(b0, 0, lda); /* bn x b0: Pn := inv(D^H) Pn, then A00 -= Pn^H Pn (lower) */  \
+                oracle_##P##_trsm('L', 'L', 'C', bn, b0, D, lda, Pn, lda);                                  \
+                for (j = 0; j < b0; ++j)                                                                    \
+                    for (i = j; i < b0; ++i) {                                                              \
+                        T s = 0;                                                                            \
+                        for (k = 0; k < bn; ++k) s += CONJ(Pn[IDX(k, i, lda)]) * Pn[IDX(k, j, lda)];        \
+                        A[IDX(i, j, lda)] -= s;                                                             \
+                        if (i == j) A[IDX(i, j, lda)] = REAL(A[IDX(i, j, lda)]);                            \
+                    }                                                                                       \
+            }                                                                                               \
+        }                                                                                                   \
+        free(work);                                                                                         \
         return info;                                                                                        \
     }                                                                                                       \
                                                                                                             \

@@ -35,6 +35,8 @@ def _lib():
             getattr(L, f"oracle_{p}_ppotrs").restype = None
             getattr(L, f"oracle_{p}_pposv").argtypes = [c, c, i, i, vp, i, vp, i]
             getattr(L, f"oracle_{p}_pposv").restype = i
+            getattr(L, f"oracle_{p}_potrf_bottom_right").argtypes = [c, i, vp, i]
+            getattr(L, f"oracle_{p}_potrf_bottom_right").restype = i
             getattr(L, f"oracle_{p}_diag_logdet").argtypes = [i, vp, i, vp]
             getattr(L, f"oracle_{p}_diag_logdet").restype = i
         _LIB = L
@@ -50,6 +52,15 @@ def potrf(a: np.ndarray, uplo: str = "L", n: int | None = None):
     A = _f(a)
     n = A.shape[1] if n is None else n
     info = getattr(_lib(), f"oracle_{_TC[A.dtype]}_potrf")(uplo.encode(), n, A.ctypes.data, max(1, A.shape[0]))
+    return A, int(info)
+
+
+def potrf_bottom_right(a: np.ndarray, uplo: str = "U", n: int | None = None):
+    """Return (factor array, info) of the bottom-right factorization: A = U U^H ('U') or L^H L ('L')."""
+    A = _f(a)
+    n = A.shape[1] if n is None else n
+    info = getattr(_lib(), f"oracle_{_TC[A.dtype]}_potrf_bottom_right")(uplo.encode(), n, A.ctypes.data,
+                                                                         max(1, A.shape[0]))
     return A, int(info)
 
 
