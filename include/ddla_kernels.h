@@ -120,6 +120,14 @@ int ddlak_bis_solve(int n, int nrhs, const void* L32, long long ldl, const void*
                     void* work, unsigned long long work_bytes, void* stream);
 int ddlak_bis_solve_f32(int n, int nrhs, const void* L32, long long ldl, const void* Dinv32, void* B, long long ldb,
                         void* work, unsigned long long work_bytes, void* stream);
+/* Host-side view of that solve's unit queue (no device work): the number of
+ * forward units and of all units for order n, and unit u decoded to its kind
+ * (0 forward diagonal slice, 1 forward panel slice, 2 backward diagonal slice,
+ * 3 backward panel slice, 4 forward bulk panel, 5 backward bulk panel), phase
+ * (diagonal block), index (64-row part, row tile or column tile) and 256-wide
+ * slice of the inner dimension.  For tests of the queue's ordering rules. */
+int ddlak_bis_queue_size(int n, long long* forward_units, long long* total_units);
+int ddlak_bis_queue_unit(int n, long long u, int* kind, int* phase, int* index, int* slice);
 
 /* R = B - A X, A symmetric FP64 stored in its lower triangle, each lower tile read once
  * (atomics fold the partial products into R: its last bits depend on their order). */

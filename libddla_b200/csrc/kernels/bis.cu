@@ -758,6 +758,34 @@ extern "C" int ddlak_bis_inverse_narrow(int n, const void* Dinv, void* Dinv32, v
     return (int)cudaGetLastError();
 }
 
+// The solve's queue as the kernel walks it, for checking on the host: the unit
+// counts of both directions and the decode of one unit.
+extern "C" int ddlak_bis_queue_size(int n, long long* forward_units, long long* total_units)
+{
+    using namespace ddlak;
+    if (n <= 0 || !forward_units || !total_units) return (int)cudaErrorInvalidValue;
+    const ChainLayout l = chain_layout(n, sizeof(float));
+    *forward_units = l.nf;
+    *total_units = l.nf + l.nb;
+    return 0;
+}
+
+extern "C" int ddlak_bis_queue_unit(int n, long long u, int* kind, int* phase, int* index, int* slice)
+{
+    using namespace ddlak;
+    if (n <= 0 || !kind || !phase || !index || !slice) return (int)cudaErrorInvalidValue;
+    const ChainLayout l = chain_layout(n, sizeof(float));
+    if (u < 0 || u >= l.nf + l.nb) return (int)cudaErrorInvalidValue;
+    Chain c{};
+    c.n = n;
+    c.S = l.S;
+    c.Tt = l.Tt;
+    c.nf = l.nf;
+    c.total = l.nf + l.nb;
+    decode_unit(c, u, *kind, *phase, *index, *slice);
+    return 0;
+}
+
 extern "C" unsigned long long ddlak_bis_solve_workspace(int n, int nrhs)
 {
     using namespace ddlak;
