@@ -76,6 +76,25 @@ template <typename T>
 void pdiag_logdet(const DdlaHandle_t& handle, int n, const T* A, const int* descA,
                   std::complex<real_type_t<T>>& result);
 
+// A batch of GEMMs of differing sizes (reference ddla.h:1836-1849,
+// src/BLAS/gemm_vbatched.cpp:349-399): for b < batch_count,
+//   C_b = alpha op(A_b) op(B_b) + beta C_b,  op(A_b) d_m[b] x d_k[b],
+// with every array device resident.  T is float, double, std::complex<float>
+// or std::complex<double>; trans* are 'N', 'T' or 'C' in either case.  A GPU
+// handle is required.  std::invalid_argument for: a null or non-GPU handle, a
+// negative batch count, a null pointer array, a bad transpose mode, a null
+// dimension array, and "gemmVbatched: invalid dimensions at batch <b>" for the
+// first entry found with a negative size or a leading dimension below the
+// rows of its matrix (the sizes are validated on the device and read back
+// once).  An empty batch does nothing.  Per entry: m or n of 0 does nothing;
+// k == 0 or alpha == 0 scales C by beta without reading A or B; a null A, B
+// or C pointer skips the entry; beta == 0 never reads C.  Enqueued on the
+// handle's stream.
+template <typename T>
+void gemmVbatched(const DdlaHandle_t& handle, char transA, char transB, int* d_m, int* d_n, int* d_k, T alpha,
+                  const T* const* d_A_array, int* d_lda, const T* const* d_B_array, int* d_ldb, T beta,
+                  T** d_C_array, int* d_ldc, int batch_count);
+
 // ppotrs<double> that allocates nothing (no reference counterpart): for callers
 // that cannot allocate device memory while running.  The solve's flags live in
 // a fixed device array inside the library (n <= 65536, nrhs <= 256; larger

@@ -125,6 +125,22 @@ int ddla_s_pdiag_logdet(void* handle, int n, const void* A, const int* descA, vo
 int ddla_d_pdiag_logdet(void* handle, int n, const void* A, const int* descA, void* result);
 int ddla_c_pdiag_logdet(void* handle, int n, const void* A, const int* descA, void* result);
 int ddla_z_pdiag_logdet(void* handle, int n, const void* A, const int* descA, void* result);
+/* gemmVbatched (reference include/ddla/ddla.h:1836-1849, a C++ template with
+ * no C export there): the batched GEMM over device-resident size, leading-
+ * dimension and pointer arrays; alpha and beta point to one host scalar of the
+ * routine's type.  Errors as the template's (ST_EXCEPTION with its message). */
+int ddla_s_gemm_vbatched(void* handle, char transA, char transB, int* d_m, int* d_n, int* d_k, const void* alpha,
+                         const void* const* d_A, int* d_lda, const void* const* d_B, int* d_ldb, const void* beta,
+                         void** d_C, int* d_ldc, int batch_count);
+int ddla_d_gemm_vbatched(void* handle, char transA, char transB, int* d_m, int* d_n, int* d_k, const void* alpha,
+                         const void* const* d_A, int* d_lda, const void* const* d_B, int* d_ldb, const void* beta,
+                         void** d_C, int* d_ldc, int batch_count);
+int ddla_c_gemm_vbatched(void* handle, char transA, char transB, int* d_m, int* d_n, int* d_k, const void* alpha,
+                         const void* const* d_A, int* d_lda, const void* const* d_B, int* d_ldb, const void* beta,
+                         void** d_C, int* d_ldc, int batch_count);
+int ddla_z_gemm_vbatched(void* handle, char transA, char transB, int* d_m, int* d_n, int* d_k, const void* alpha,
+                         const void* const* d_A, int* d_lda, const void* const* d_B, int* d_ldb, const void* beta,
+                         void** d_C, int* d_ldc, int batch_count);
 
 /* The reference's internal check / size / run split of ppotrf and ppotrs
  * (src/Cholesky/cholesky_workspace.h:133-154, 207-222) exported so a caller can

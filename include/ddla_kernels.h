@@ -35,6 +35,28 @@ int ddlak_potrf(char type, char uplo, int n, void* A, long long lda, int* dinfo,
  * permuted and restored, never altered. */
 int ddlak_reverse_swap(char type, int n, void* A, long long lda, void* stream);
 
+/* Validation pass of the variable-size batched GEMM (the reference's
+ * validate_and_max_dimensions, src/BLAS/gemm_vbatched.cpp:72-106): zeroes the
+ * four ints at d_summary, then writes summary[0..2] = largest m, n, k and
+ * summary[3] = 1 + the index of an entry with a negative size or a leading
+ * dimension below max(1, rows of its matrix) (0: all valid).  transA/transB
+ * 'N', 'T', 'C' in either case. */
+int ddlak_gemm_vbatched_check(char transA, char transB, const int* d_m, const int* d_n, const int* d_k,
+                              const int* d_lda, const int* d_ldb, const int* d_ldc, int batch, int* d_summary,
+                              void* stream);
+
+/* C_b = alpha op(A_b) op(B_b) + beta C_b for b < batch (the reference's
+ * gemm_vbatched core, src/BLAS/gemm_vbatched.cpp:162-219 and
+ * src/vbatched/gemm_template_kernel_vbatched.hpp): type 's' 'd' 'c' 'z';
+ * alpha/beta point to one host scalar of that type; max_m/max_n bound every
+ * entry's m and n (from ddlak_gemm_vbatched_check).  Entries with m or n of
+ * 0 are untouched; k == 0 or alpha == 0 gives C = beta C (C = 0 for beta == 0,
+ * C unchanged for beta == 1) without reading A or B; a null A, B or C skips
+ * the entry; beta == 0 never reads C. */
+int ddlak_gemm_vbatched(char type, char transA, char transB, int max_m, int max_n, const int* d_m, const int* d_n,
+                        const int* d_k, const void* alpha, const void* d_A, const int* d_lda, const void* d_B,
+                        const int* d_ldb, const void* beta, void* d_C, const int* d_ldc, int batch, void* stream);
+
 /* Bytes of device scratch ddlak_potrs needs for (n, nrhs). */
 unsigned long long ddlak_potrs_workspace(int n, int nrhs);
 

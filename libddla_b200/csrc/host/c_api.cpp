@@ -136,6 +136,23 @@ int pdiag_logdet_impl(void* handle, int n, const void* A, const int* descA, void
 }
 
 template <class T>
+int gemm_vbatched_impl(void* handle, char ta, char tb, int* d_m, int* d_n, int* d_k, const void* alpha,
+                       const void* const* d_A, int* d_lda, const void* const* d_B, int* d_ldb, const void* beta,
+                       void** d_C, int* d_ldc, int batch_count)
+{
+    return run(handle, [&](ddla::DdlaHandle_t h) -> int {
+        if (alpha == nullptr || beta == nullptr) return ST_INVALID_VALUE;
+        T al, be;
+        std::memcpy(&al, alpha, sizeof(T));
+        std::memcpy(&be, beta, sizeof(T));
+        ddla::gemmVbatched<T>(h, ta, tb, d_m, d_n, d_k, al, reinterpret_cast<const T* const*>(d_A), d_lda,
+                              reinterpret_cast<const T* const*>(d_B), d_ldb, be, reinterpret_cast<T**>(d_C), d_ldc,
+                              batch_count);
+        return ST_SUCCESS;
+    });
+}
+
+template <class T>
 int ppotrf_ws_impl(void* handle, char uplo, int n, const int* descA, long long* bytes)
 {
     return run(handle, [&](ddla::DdlaHandle_t h) -> int {
@@ -398,6 +415,13 @@ int ddla_c_bcast_dims(int, int* m, int* n, int* type_char, int root)
     int ddla_##P##_pdiag_logdet(void* handle, int n, const void* A, const int* descA, void* result)                \
     {                                                                                                                \
         return pdiag_logdet_impl<T>(handle, n, A, descA, result);                                                    \
+    }                                                                                                                \
+    int ddla_##P##_gemm_vbatched(void* handle, char ta, char tb, int* d_m, int* d_n, int* d_k, const void* alpha,  \
+                                 const void* const* d_A, int* d_lda, const void* const* d_B, int* d_ldb,             \
+                                 const void* beta, void** d_C, int* d_ldc, int batch_count)                          \
+    {                                                                                                                \
+        return gemm_vbatched_impl<T>(handle, ta, tb, d_m, d_n, d_k, alpha, d_A, d_lda, d_B, d_ldb, beta, d_C, d_ldc, \
+                                     batch_count);                                                                   \
     }                                                                                                                \
     int ddla_##P##_ppotrf_workspace_size(void* handle, char uplo, int n, const int* descA, long long* bytes)       \
     {                                                                                                                \

@@ -181,3 +181,48 @@ def shard_lpt(orders, world: int):
         shards[r].append(i)
         heapq.heappush(heap, (load + float(orders[i]) ** 3, r))
     return [sorted(s) for s in shards]
+
+
+# ---- variable-size batched GEMM --------------------------------------------
+_GV_SFX = {"torch.float32": "s", "torch.float64": "d", "torch.complex64": "c", "torch.complex128": "z"}
+
+
+def gemm_vbatched(handle, transA: str, transB: str, m, n, k, alpha, A_list, lda, B_list, ldb, beta, C_list, ldc,
+                  d_m=None, d_n=None, d_k=None) -> None:
+    """C_i = alpha op(A_i) op(B_i) + beta C_i for every i (ddla_?_gemm_vbatched, the
+    reference's gemmVbatched).  A_list / B_list / C_list are CUDA tensors (or None
+    for a null entry) holding column-major matrices at their data_ptr; m, n, k,
+    lda, ldb, ldc are per-entry integer sequences.  d_m / d_n / d_k override the
+    device size arrays (e.g. to pass a null one).  Completes before returning."""
+    torch = _torch()
+    tensors = [t for t in list(A_list) + list(B_list) + list(C_list) if t is not None]
+    if not tensors:
+        raise ValueError("gemm_vbatched: at least one matrix is needed to fix the type")
+    sfx = _GV_SFX[str(tensors[0].dtype)]
+    dev = tensors[0].device
+    batch = len(C_list)
+
+    def iarr(v):
+        return torch.tensor(np.asarray(v, dtype=np.int32), device=dev)
+
+    def parr(ts):
+        return torch.tensor(np.array([0 if t is None else t.data_ptr() for t in ts], dtype=np.int64), device=dev)
+
+    dm = iarr(m) if d_m is None else d_m
+    dn = iarr(n) if d_n is None else d_n
+    dk = iarr(k) if d_k is None else d_k
+    dlda, dldb, dldc = iarr(lda), iarr(ldb), iarr(ldc)
+    pa, pb, pc = parr(A_list), parr(B_list), parr(C_list)
+    sdt = {"s": np.float32, "d": np.float64, "c": np.complex64, "z": np.complex128}[sfx]
+    al = np.array([alpha], dtype=sdt)
+    be = np.array([beta], dtype=sdt)
+    torch.cuda.synchronize(dev)  # inputs written on torch's stream; the call runs on the handle's
+
+    def ptr(t):
+        return None if t is None or (hasattr(t, "numel") and t.numel() == 0) else t.data_ptr()
+
+    fn = getattr(C, f"ddla_{sfx}_gemm_vbatched")
+    C.check_status(fn(handle.ptr, transA.encode(), transB.encode(), ptr(dm), ptr(dn), ptr(dk), al.ctypes.data,
+                      ptr(pa), ptr(dlda), ptr(pb), ptr(dldb), be.ctypes.data, ptr(pc), ptr(dldc), batch),
+                   "gemm_vbatched")
+    C.check_status(C.ddla_c_synchronize(handle.ptr), "gemm_vbatched: synchronize")

@@ -95,3 +95,45 @@ def diag_logdet(a: np.ndarray, n: int | None = None, lda: int | None = None):
     if st != 0:
         raise ValueError("diag_logdet: nonfinite diagonal")
     return complex(out[0], out[1])
+
+
+def gemm_vbatched(ta: str, tb: str, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
+    """The variable-size batched GEMM, entry by entry, on host arrays.
+
+    Restates the reference's gemmVbatched (src/BLAS/gemm_vbatched.cpp:349-399) as
+    its kernel applies it per entry (src/vbatched/gemm_template_kernel_vbatched.hpp:
+    61-85 for the early exits and gemm_template_device.hpp:226-227 for the store),
+    with the product of its test's reference_gemm (tests/test_gemm_vbatched.cpp:
+    56-90): op(X)(r, c) is X[r + c ld] for 'N', X[c + r ld] for 'T', its conjugate
+    for 'C'.  Rules: m or n <= 0 leaves C; k == 0 or alpha == 0 makes C = beta C
+    (0 for beta == 0, untouched for beta == 1 or a null C) without reading A or B;
+    a null (None) A, B or C leaves C; beta == 0 never reads C.  A, B, C are lists
+    of 1-D column-major arrays (or None); returns new arrays for C.
+    """
+    def view(x, rows, cols, ld):
+        return x[:ld * cols].reshape(cols, ld).T[:rows]
+
+    def op(x, t, rows, cols, ld):
+        if t in "Nn":
+            return view(x, rows, cols, ld)
+        s = view(x, cols, rows, ld).T
+        return np.conj(s) if t in "Cc" else s
+
+    out = []
+    for b in range(len(C)):
+        c = None if C[b] is None else C[b].copy()
+        out.append(c)
+        mb, nb, kb = int(m[b]), int(n[b]), int(k[b])
+        if mb <= 0 or nb <= 0:
+            continue
+        cv = None if c is None else view(c, mb, nb, int(ldc[b]))
+        if kb == 0 or alpha == 0:
+            if beta == 1 or cv is None:
+                continue
+            cv[...] = 0 if beta == 0 else beta * cv
+            continue
+        if A[b] is None or B[b] is None or cv is None:
+            continue
+        prod = alpha * (op(A[b], ta, mb, kb, int(lda[b])) @ op(B[b], tb, kb, nb, int(ldb[b])))
+        cv[...] = prod if beta == 0 else prod + beta * cv
+    return out
