@@ -1,22 +1,26 @@
 // In-shared-memory Cholesky of one diagonal block (lower triangle of
-// s[i + j*ld], i, j < nbk <= 128), shared by the plain and mixed factorizations.
+// s[i + j*ld], i, j < nbk <= 128; nbk <= 64 for complex double), shared by the
+// plain and mixed factorizations.
 //
-// Right-looking, one column per step, with the block held in REGISTERS: the
-// lower triangle is cut into BxB tiles and each thread owns one tile (136
-// threads for a 128 x 128 block with B = 8).  Step j reads column j (current,
-// unscaled values) and its pivot d = a_jj from a double-buffered shared
-// vector, applies a_ik -= a_ij conj(a_kj) / d to the owned tile, the owners of
-// column j+1 publish it, and the CTA synchronises once.  The square roots are
-// deferred: the pivots are kept and every column is scaled by 1/sqrt(d_j) after
-// the last step, so a step's critical path is one division and one
-// multiply-add per element.  The column loop is unrolled by B so that the
-// column's position inside a tile is a compile-time constant: the update has
-// no per-element conditions (an upper-triangle element of a diagonal tile is
-// updated too, never read for a lower one and never stored).
+// Blocked by 32-column panels, so the CTA synchronises three times per panel
+// instead of once per column.  Panel c0..c0+31:
+//   (A) warp 0 factors the 32 x 32 diagonal block in registers (lane i holds
+//       row i).  Step j publishes column j in a double-buffered shared vector
+//       (one __syncwarp), every lane applies a_ik -= a_ij conj(a_kj) / d_j to
+//       its row, and the owner of the next pivot computes 1/d_(j+1) inside the
+//       step, so a step's critical path is one multiply, one multiply-add and
+//       the shared round trip.  The square roots are deferred: column j is
+//       scaled by 1/sqrt(d_j) once the panel is done.
+//   (B) one thread per row below the panel solves x L11^H = a (forward
+//       substitution with the final L11 and its reciprocal pivots from shared
+//       memory).
+//   (C) the trailing lower triangle is updated by the panel: 256 threads in a
+//       16 x 16 grid, thread (tx, ty) owning rows tx + 16p and columns
+//       ty + 16q (q <= p), so the shared reads are conflict-free or broadcast.
 // Returns 0, or 1 + the index of the first column whose pivot is not positive
-// (or NaN).  As in LAPACK ?potf2, the columns before it are final and the
-// failed pivot keeps its value.
-// Must be called by all threads of the CTA (blockDim.x >= number of tiles).
+// (or NaN).  As in LAPACK ?potf2, the columns before it are final (in every
+// row of the block) and the failed pivot keeps its value.
+// Must be called by all 256 threads of the CTA.
 #pragma once
 #include "common.cuh"
 
@@ -34,128 +38,162 @@ __device__ __forceinline__ T shfl(T v, int src)
     }
 }
 
-// tile edge: 8 for 4- and 8-byte types, 4 for complex double (register budget;
-// complex double blocks are 64 wide, so 136 tiles either way)
-template <class T> constexpr int diag_tile() { return sizeof(T) >= 16 ? 4 : 8; }
+namespace diagf {
+
+constexpr int PW = 32;    // panel width
+constexpr int MAXN = 128;  // largest block
+constexpr int UP = (MAXN - PW) / 16;  // row groups of the trailing update (6)
+
+// (A) warp 0: the w x w diagonal block at (c0, c0).  On exit the block's
+// columns before the first failed one hold L, s_rs[c0 + j] = 1 / l_jj for
+// them, and a failure is recorded as *s_fail = c0 + j + 1.
+template <class T>
+__device__ __forceinline__ void panel_diag(T* s, int ld, int c0, int w, int lane, T (*colbuf)[PW],
+                                           real_t<T>* s_inv, real_t<T>* s_rs, int* s_fail)
+{
+    using R = real_t<T>;
+    const int i = lane;
+    T a[PW];
+#pragma unroll
+    for (int k = 0; k < PW; ++k) a[k] = (i < w && k <= i) ? s[(c0 + i) + (c0 + k) * ld] : zero<T>();
+    // column 0 and its pivot's reciprocal
+    colbuf[0][i] = a[0];
+    if (i == 0) s_inv[0] = R(1) / re(a[0]);
+    __syncwarp();
+    int fail = 0;
+    R dpiv = R(0);
+#pragma unroll
+    for (int j = 0; j < PW; ++j) {
+        if (j < w && !fail) {
+            const T* cv = colbuf[j & 1];
+            const R d = re(cv[j]);
+            if (!(d > R(0))) {
+                fail = j + 1;
+            } else {
+                if (i == j) dpiv = d;
+                const R invd = s_inv[j & 1];
+                const T tj = scal(a[j], invd);  // a_ij / d_j (upper-triangle garbage for i < j, never stored)
+                if (j + 1 < PW) {
+                    // the next column first, so its publication overlaps the rest of the step
+                    a[j + 1] = fms(a[j + 1], tj, cj(cv[j + 1]));
+                    colbuf[(j + 1) & 1][i] = a[j + 1];
+                    if (i == j + 1) s_inv[(j + 1) & 1] = R(1) / re(a[j + 1]);
+#pragma unroll
+                    for (int k = j + 2; k < PW; ++k) a[k] = fms(a[k], tj, cj(cv[k]));
+                }
+            }
+            __syncwarp();
+        }
+    }
+    // deferred scaling: l_kk = sqrt(d_k), l_ik = a_ik / sqrt(d_k)
+    const int done = fail ? fail - 1 : w;
+    R rs = R(0), sk = R(0);
+    if (i < done) {
+        sk = sqrt(dpiv);
+        rs = R(1) / sk;
+        s_rs[c0 + i] = rs;
+    }
+#pragma unroll
+    for (int k = 0; k < PW; ++k) {
+        const R rk = shfl(rs, k);
+        if (k < done) {
+            if (i == k) a[k] = from_real<T>(sk);
+            else if (i > k) a[k] = scal(a[k], rk);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < PW; ++k)
+        if (i < w && k <= i) s[(c0 + i) + (c0 + k) * ld] = a[k];
+    if (fail && lane == 0) *s_fail = c0 + fail;
+}
+
+// (B) row r below the panel: x L11^H = a over the panel's first jd columns.
+template <class T>
+__device__ __forceinline__ void panel_row(T* s, int ld, int c0, int r, int jd, const real_t<T>* s_rs)
+{
+    T x[PW];
+#pragma unroll
+    for (int k = 0; k < PW; ++k) x[k] = k < jd ? s[r + (c0 + k) * ld] : zero<T>();
+#pragma unroll
+    for (int j = 0; j < PW; ++j) {
+        if (j < jd) {
+            x[j] = scal(x[j], s_rs[c0 + j]);
+#pragma unroll
+            for (int k = j + 1; k < PW; ++k) x[k] = fms(x[k], x[j], cj(s[(c0 + k) + (c0 + j) * ld]));
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < PW; ++k)
+        if (k < jd) s[r + (c0 + k) * ld] = x[k];
+}
+
+// (C) s[i, k] -= sum_j L[i, c0 + j] conj(L[k, c0 + j]) for c1 <= k <= i < nbk.
+template <class T>
+__device__ __forceinline__ void trailing(T* s, int ld, int c0, int c1, int nbk, int t)
+{
+    const int tx = t & 15, ty = t >> 4;
+    const int m2 = nbk - c1;
+    T acc[UP][UP];
+#pragma unroll
+    for (int p = 0; p < UP; ++p)
+#pragma unroll
+        for (int q = 0; q <= p; ++q) acc[p][q] = zero<T>();
+#pragma unroll 4
+    for (int j = 0; j < PW; ++j) {
+        const T* col = s + (c0 + j) * ld + c1;
+        T li[UP], lk[UP];
+#pragma unroll
+        for (int p = 0; p < UP; ++p) {
+            li[p] = (16 * p < m2 && tx + 16 * p < m2) ? col[tx + 16 * p] : zero<T>();
+            lk[p] = (16 * p < m2 && ty + 16 * p < m2) ? cj(col[ty + 16 * p]) : zero<T>();
+        }
+#pragma unroll
+        for (int p = 0; p < UP; ++p)
+            if (16 * p < m2)
+#pragma unroll
+                for (int q = 0; q <= p; ++q) acc[p][q] = fma_(acc[p][q], li[p], lk[q]);
+    }
+#pragma unroll
+    for (int p = 0; p < UP; ++p)
+#pragma unroll
+        for (int q = 0; q <= p; ++q) {
+            const int i = tx + 16 * p, k = ty + 16 * q;
+            if (i < m2 && k <= i) {
+                T* e = s + (c1 + i) + (long long)(c1 + k) * ld;
+                *e = sub(*e, acc[p][q]);
+            }
+        }
+}
+
+}  // namespace diagf
 
 template <class T>
 __device__ int factor_block_smem(T* s, int ld, int nbk)
 {
     using R = real_t<T>;
-    constexpr int B = diag_tile<T>();
-    constexpr int MAXN = 128;
-    static_assert(B % 2 == 0, "the column buffer parity must follow the column index within a tile");
-    __shared__ T col[2][MAXN];
-    __shared__ R piv[MAXN];
+    using namespace diagf;
+    __shared__ T colbuf[2][PW];
+    __shared__ R s_inv[2];
+    __shared__ R s_rs[MAXN];
     __shared__ int s_fail;
-    const int nt = (nbk + B - 1) / B;  // tiles per dimension
-    const int ntiles = nt * (nt + 1) / 2;
-    const int t = threadIdx.x;
-    const bool owner = t < ntiles;
-    int bi = 0, bk = 0;
-    if (owner) {
-        int i = (int)((sqrtf(8.f * t + 1.f) - 1.f) * 0.5f);
-        while ((i + 1) * (i + 2) / 2 <= t) ++i;
-        while (i * (i + 1) / 2 > t) --i;
-        bi = i;
-        bk = t - i * (i + 1) / 2;
-    }
-    const int r0 = bi * B, c0 = bk * B;
-    T a[B][B];
-#pragma unroll
-    for (int p = 0; p < B; ++p)
-#pragma unroll
-        for (int q = 0; q < B; ++q) {
-            const int i = r0 + p, k = c0 + q;
-            a[p][q] = (owner && i < nbk && k < nbk && i >= k) ? s[i + k * ld] : zero<T>();
-        }
-    // entries past nbk stay zero, so the update needs no range checks
-    for (int i = t; i < 2 * MAXN; i += blockDim.x) col[i / MAXN][i % MAXN] = zero<T>();
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     if (t == 0) s_fail = 0;
     __syncthreads();
-    if (owner && bk == 0)
-#pragma unroll
-        for (int p = 0; p < B; ++p)
-            if (r0 + p < nbk) col[0][r0 + p] = a[p][0];
-    __syncthreads();
-
-    int fail = 0;
-    for (int jt = 0; jt < nt && !fail; ++jt) {
-#pragma unroll
-        for (int jq = 0; jq < B; ++jq) {
-            const int j = jt * B + jq;
-            if (j < nbk && !fail) {
-                const T* cv = col[jq & 1];
-                const R d = re(cv[j]);
-                if (!(d > R(0))) {
-                    fail = j + 1;
-                } else {
-                    const R invd = R(1) / d;
-                    if (t == 0) piv[j] = d;
-                    if (owner && bk >= jt) {
-                        T lk[B];
-#pragma unroll
-                        for (int q = 0; q < B; ++q) lk[q] = scal(cj(cv[c0 + q]), invd);
-                        if (bk > jt) {
-#pragma unroll
-                            for (int p = 0; p < B; ++p) {
-                                const T li = cv[r0 + p];
-#pragma unroll
-                                for (int q = 0; q < B; ++q) a[p][q] = fms(a[p][q], li, lk[q]);
-                            }
-                        } else {
-#pragma unroll
-                            for (int p = 0; p < B; ++p) {
-                                const T li = cv[r0 + p];
-#pragma unroll
-                                for (int q = jq + 1; q < B; ++q) a[p][q] = fms(a[p][q], li, lk[q]);
-                            }
-                        }
-                        // publish column j+1 (its step-j update is complete)
-                        if (jq + 1 < B) {
-                            if (bk == jt)
-#pragma unroll
-                                for (int p = 0; p < B; ++p)
-                                    if (r0 + p < nbk) col[(jq + 1) & 1][r0 + p] = a[p][jq + 1];
-                        } else if (bk == jt + 1) {
-#pragma unroll
-                            for (int p = 0; p < B; ++p)
-                                if (r0 + p < nbk) col[0][r0 + p] = a[p][0];
-                        }
-                    }
-                }
-                __syncthreads();
-            }
+    for (int c0 = 0; c0 < nbk; c0 += PW) {
+        const int w = nbk - c0 < PW ? nbk - c0 : PW;
+        const int c1 = c0 + w;
+        if (warp == 0) panel_diag<T>(s, ld, c0, w, lane, colbuf, s_inv, s_rs, &s_fail);
+        __syncthreads();
+        const int fail = s_fail;
+        const int jd = fail ? fail - 1 - c0 : w;  // final columns of this panel
+        for (int r = c1 + t; r < nbk; r += blockDim.x) panel_row<T>(s, ld, c0, r, jd, s_rs);
+        __syncthreads();
+        if (fail) break;
+        if (c1 < nbk) {
+            trailing<T>(s, ld, c0, c1, nbk, t);
+            __syncthreads();
         }
     }
-    // deferred scaling of the final columns: l_kk = sqrt(d_k), l_ik = a_ik / sqrt(d_k)
-    const int done = fail ? fail - 1 : nbk;
-    if (owner) {
-#pragma unroll
-        for (int q = 0; q < B; ++q) {
-            const int k = c0 + q;
-            if (k < done) {
-                const R dk = piv[k];
-                const R sk = sqrt(dk);
-                const R rs = R(1) / sk;
-#pragma unroll
-                for (int p = 0; p < B; ++p) {
-                    const int i = r0 + p;
-                    if (i == k) a[p][q] = from_real<T>(sk);
-                    else if (i > k) a[p][q] = scal(a[p][q], rs);
-                }
-            }
-        }
-    }
-    if (t == 0) s_fail = fail;
-#pragma unroll
-    for (int p = 0; p < B; ++p)
-#pragma unroll
-        for (int q = 0; q < B; ++q) {
-            const int i = r0 + p, k = c0 + q;
-            if (owner && i < nbk && k < nbk && i >= k) s[i + k * ld] = a[p][q];
-        }
-    __syncthreads();
     return s_fail;
 }
 
