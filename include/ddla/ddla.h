@@ -95,6 +95,23 @@ void gemmVbatched(const DdlaHandle_t& handle, char transA, char transB, int* d_m
                   const T* const* d_A_array, int* d_lda, const T* const* d_B_array, int* d_ldb, T beta,
                   T** d_C_array, int* d_ldc, int batch_count);
 
+// Two dependent batched GEMM stages sharing reusable temporaries (reference
+// ddla.h:1851-1876, src/BLAS/gemm_vbatched.cpp:420-509): for each host-resident
+// segment of segment_sizes in turn, stage 0 gives C0_b = alpha_0 op(A0_b)
+// op(B0_b) for the segment's entries, then stage 1 gives C1_b = alpha_1 op(X_b)
+// op(Y_b) + beta_1 C1_b with (X, Y) = (C0_b, AB1_b) if C0_left, else
+// (AB1_b, C0_b); the C0 operand is read with d_lda_1 or d_ldb_1.  C0 entries of
+// different segments may alias.  beta_0 must be zero, every segment positive and
+// the segments must add up to batch_count (std::invalid_argument otherwise, as
+// for the single-stage checks, which both stages also pass).
+template <typename T>
+void gemmVbatched2s(const DdlaHandle_t& handle, char transA_0, char transB_0, int* d_m_0, int* d_n_0, int* d_k_0,
+                    T alpha_0, const T* const* d_A_array_0, int* d_lda_0, const T* const* d_B_array_0, int* d_ldb_0,
+                    T beta_0, T** d_C_array_0, int* d_ldc_0, char transA_1, char transB_1, int* d_m_1, int* d_n_1,
+                    int* d_k_1, T alpha_1, const T* const* d_AB_array_1, int* d_lda_1, int* d_ldb_1, T beta_1,
+                    T** d_C_array_1, int* d_ldc_1, bool C0_left, int batch_count, const int* segment_sizes,
+                    int segment_count);
+
 // ppotrs<double> that allocates nothing (no reference counterpart): for callers
 // that cannot allocate device memory while running.  The solve's flags live in
 // a fixed device array inside the library (n <= 65536, nrhs <= 256; larger

@@ -141,6 +141,19 @@ int ddla_c_gemm_vbatched(void* handle, char transA, char transB, int* d_m, int* 
 int ddla_z_gemm_vbatched(void* handle, char transA, char transB, int* d_m, int* d_n, int* d_k, const void* alpha,
                          const void* const* d_A, int* d_lda, const void* const* d_B, int* d_ldb, const void* beta,
                          void** d_C, int* d_ldc, int batch_count);
+/* gemmVbatched2s (reference include/ddla/ddla.h:1851-1876, C++ only there):
+ * the two-stage form; alphas and betas point to one host scalar of the
+ * routine's type, c0_left is 0 or 1, segment_sizes is host memory. */
+#define DDLA_GEMM_VBATCHED2S_ARGS                                                                                  \
+    void *handle, char transA_0, char transB_0, int *d_m_0, int *d_n_0, int *d_k_0, const void *alpha_0,          \
+        const void *const *d_A_0, int *d_lda_0, const void *const *d_B_0, int *d_ldb_0, const void *beta_0,        \
+        void **d_C_0, int *d_ldc_0, char transA_1, char transB_1, int *d_m_1, int *d_n_1, int *d_k_1,             \
+        const void *alpha_1, const void *const *d_AB_1, int *d_lda_1, int *d_ldb_1, const void *beta_1,            \
+        void **d_C_1, int *d_ldc_1, int c0_left, int batch_count, const int *segment_sizes, int segment_count
+int ddla_s_gemm_vbatched2s(DDLA_GEMM_VBATCHED2S_ARGS);
+int ddla_d_gemm_vbatched2s(DDLA_GEMM_VBATCHED2S_ARGS);
+int ddla_c_gemm_vbatched2s(DDLA_GEMM_VBATCHED2S_ARGS);
+int ddla_z_gemm_vbatched2s(DDLA_GEMM_VBATCHED2S_ARGS);
 
 /* The reference's internal check / size / run split of ppotrf and ppotrs
  * (src/Cholesky/cholesky_workspace.h:133-154, 207-222) exported so a caller can

@@ -153,6 +153,29 @@ int gemm_vbatched_impl(void* handle, char ta, char tb, int* d_m, int* d_n, int* 
 }
 
 template <class T>
+int gemm_vbatched2s_impl(void* handle, char ta0, char tb0, int* m0, int* n0, int* k0, const void* alpha0,
+                         const void* const* A0, int* lda0, const void* const* B0, int* ldb0, const void* beta0,
+                         void** C0, int* ldc0, char ta1, char tb1, int* m1, int* n1, int* k1, const void* alpha1,
+                         const void* const* AB1, int* lda1, int* ldb1, const void* beta1, void** C1, int* ldc1,
+                         int c0_left, int batch_count, const int* segment_sizes, int segment_count)
+{
+    return run(handle, [&](ddla::DdlaHandle_t h) -> int {
+        if (!alpha0 || !beta0 || !alpha1 || !beta1) return ST_INVALID_VALUE;
+        T a0, b0, a1, b1;
+        std::memcpy(&a0, alpha0, sizeof(T));
+        std::memcpy(&b0, beta0, sizeof(T));
+        std::memcpy(&a1, alpha1, sizeof(T));
+        std::memcpy(&b1, beta1, sizeof(T));
+        ddla::gemmVbatched2s<T>(h, ta0, tb0, m0, n0, k0, a0, reinterpret_cast<const T* const*>(A0), lda0,
+                                reinterpret_cast<const T* const*>(B0), ldb0, b0, reinterpret_cast<T**>(C0), ldc0, ta1,
+                                tb1, m1, n1, k1, a1, reinterpret_cast<const T* const*>(AB1), lda1, ldb1, b1,
+                                reinterpret_cast<T**>(C1), ldc1, c0_left != 0, batch_count, segment_sizes,
+                                segment_count);
+        return ST_SUCCESS;
+    });
+}
+
+template <class T>
 int ppotrf_ws_impl(void* handle, char uplo, int n, const int* descA, long long* bytes)
 {
     return run(handle, [&](ddla::DdlaHandle_t h) -> int {
@@ -422,6 +445,13 @@ int ddla_c_bcast_dims(int, int* m, int* n, int* type_char, int root)
     {                                                                                                                \
         return gemm_vbatched_impl<T>(handle, ta, tb, d_m, d_n, d_k, alpha, d_A, d_lda, d_B, d_ldb, beta, d_C, d_ldc, \
                                      batch_count);                                                                   \
+    }                                                                                                                \
+    int ddla_##P##_gemm_vbatched2s(DDLA_GEMM_VBATCHED2S_ARGS)                                                      \
+    {                                                                                                                \
+        return gemm_vbatched2s_impl<T>(handle, transA_0, transB_0, d_m_0, d_n_0, d_k_0, alpha_0, d_A_0, d_lda_0,    \
+                                       d_B_0, d_ldb_0, beta_0, d_C_0, d_ldc_0, transA_1, transB_1, d_m_1, d_n_1,    \
+                                       d_k_1, alpha_1, d_AB_1, d_lda_1, d_ldb_1, beta_1, d_C_1, d_ldc_1, c0_left,    \
+                                       batch_count, segment_sizes, segment_count);                                   \
     }                                                                                                                \
     int ddla_##P##_ppotrf_workspace_size(void* handle, char uplo, int n, const int* descA, long long* bytes)       \
     {                                                                                                                \

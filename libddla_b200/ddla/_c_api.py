@@ -168,6 +168,9 @@ for _p in "sdcz":
         f"ddla_{_p}_ppotrf_bottom_right": (_i, [_vp, _c, _i, _vp, _vp, _ip]),
         f"ddla_{_p}_gemm_vbatched": (_i, [_vp, _c, _c, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                           _i]),
+        f"ddla_{_p}_gemm_vbatched2s": (_i, [_vp, _c, _c, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                            _c, _c, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp,
+                                            _i]),
         f"ddla_{_p}_ppotrf_workspace_size": (_i, [_vp, _c, _i, _vp, _llp]),
         f"ddla_{_p}_ppotrf_run": (_i, [_vp, _c, _i, _vp, _vp, _ip, _vp, _ll]),
         f"ddla_{_p}_ppotrs_workspace_size": (_i, [_vp, _c, _i, _i, _vp, _vp, _llp]),

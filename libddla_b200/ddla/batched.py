@@ -218,11 +218,59 @@ def gemm_vbatched(handle, transA: str, transB: str, m, n, k, alpha, A_list, lda,
     be = np.array([beta], dtype=sdt)
     torch.cuda.synchronize(dev)  # inputs written on torch's stream; the call runs on the handle's
 
-    def ptr(t):
-        return None if t is None or (hasattr(t, "numel") and t.numel() == 0) else t.data_ptr()
-
     fn = getattr(C, f"ddla_{sfx}_gemm_vbatched")
-    C.check_status(fn(handle.ptr, transA.encode(), transB.encode(), ptr(dm), ptr(dn), ptr(dk), al.ctypes.data,
-                      ptr(pa), ptr(dlda), ptr(pb), ptr(dldb), be.ctypes.data, ptr(pc), ptr(dldc), batch),
+    C.check_status(fn(handle.ptr, transA.encode(), transB.encode(), _ptr(dm), _ptr(dn), _ptr(dk), al.ctypes.data,
+                      _ptr(pa), _ptr(dlda), _ptr(pb), _ptr(dldb), be.ctypes.data, _ptr(pc), _ptr(dldc), batch),
                    "gemm_vbatched")
     C.check_status(C.ddla_c_synchronize(handle.ptr), "gemm_vbatched: synchronize")
+
+
+def _ptr(t):
+    return None if t is None or (hasattr(t, "numel") and t.numel() == 0) else t.data_ptr()
+
+
+def _addr(x):
+    """Device address of an entry: a CUDA tensor, an int address, or None (null)."""
+    if x is None:
+        return 0
+    return int(x) if isinstance(x, int) else x.data_ptr()
+
+
+def gemm_vbatched2s(handle, ops0: str, m0, n0, k0, alpha0, A0, lda0, B0, ldb0, C0, ldc0,
+                    ops1: str, m1, n1, k1, alpha1, AB1, lda1, ldb1, beta1, C1, ldc1,
+                    c0_left: bool, segments, dtype, beta0=0) -> None:
+    """The two-stage batched GEMM (ddla_?_gemm_vbatched2s, the reference's
+    gemmVbatched2s): per segment, C0_i = alpha0 op(A0_i) op(B0_i), then
+    C1_i = alpha1 op(X_i) op(Y_i) + beta1 C1_i with (X, Y) = (C0_i, AB1_i) when
+    c0_left, else (AB1_i, C0_i).  ops0 / ops1 are two-letter transpose pairs
+    ("NN", "TC", ...); matrix entries are CUDA tensors, int device addresses (C0
+    entries of different segments may share storage) or None; dtype is the
+    torch dtype.  Completes before returning."""
+    torch = _torch()
+    sfx = _GV_SFX[str(dtype)]
+    batch = len(C1)
+    tensors = [x for xs in (A0, B0, C0, AB1, C1) for x in xs if x is not None and not isinstance(x, int)]
+    dev = tensors[0].device if tensors else torch.device("cuda")
+
+    def iarr(v):
+        return torch.tensor(np.asarray(v, dtype=np.int32), device=dev)
+
+    def parr(xs):
+        return torch.tensor(np.array([_addr(x) for x in xs], dtype=np.int64), device=dev)
+
+    d = [iarr(v) for v in (m0, n0, k0, lda0, ldb0, ldc0, m1, n1, k1, lda1, ldb1, ldc1)]
+    p = [parr(v) for v in (A0, B0, C0, AB1, C1)]
+    sdt = {"s": np.float32, "d": np.float64, "c": np.complex64, "z": np.complex128}[sfx]
+    sc = [np.array([v], dtype=sdt) for v in (alpha0, beta0, alpha1, beta1)]
+    seg = np.asarray(segments, dtype=np.int32)
+    if dev.type == "cuda":
+        torch.cuda.synchronize(dev)  # inputs written on torch's stream; the call runs on the handle's
+    fn = getattr(C, f"ddla_{sfx}_gemm_vbatched2s")
+    C.check_status(fn(handle.ptr, ops0[0].encode(), ops0[1].encode(), _ptr(d[0]), _ptr(d[1]), _ptr(d[2]),
+                      sc[0].ctypes.data, _ptr(p[0]), _ptr(d[3]), _ptr(p[1]), _ptr(d[4]), sc[1].ctypes.data,
+                      _ptr(p[2]), _ptr(d[5]), ops1[0].encode(), ops1[1].encode(), _ptr(d[6]), _ptr(d[7]),
+                      _ptr(d[8]), sc[2].ctypes.data, _ptr(p[3]), _ptr(d[9]), _ptr(d[10]), sc[3].ctypes.data,
+                      _ptr(p[4]), _ptr(d[11]), int(bool(c0_left)), batch,
+                      seg.ctypes.data if seg.size else None, int(seg.size)),
+                   "gemm_vbatched2s")
+    C.check_status(C.ddla_c_synchronize(handle.ptr), "gemm_vbatched2s: synchronize")

@@ -137,3 +137,34 @@ def gemm_vbatched(ta: str, tb: str, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc
         prod = alpha * (op(A[b], ta, mb, kb, int(lda[b])) @ op(B[b], tb, kb, nb, int(ldb[b])))
         cv[...] = prod if beta == 0 else prod + beta * cv
     return out
+
+
+def gemm_vbatched2s(ops0, m0, n0, k0, alpha0, A0, lda0, B0, ldb0, C0, ldc0,
+                    ops1, m1, n1, k1, alpha1, AB1, lda1, ldb1, beta1, C1, ldc1, c0_left, segments):
+    """Two dependent variable-size GEMM stages over segments of the batch.
+
+    Restates the reference's gemmVbatched2s (src/BLAS/gemm_vbatched.cpp:420-465,
+    src/vbatched/gemm_template_kernel_vbatched.hpp:440-497): segment by segment,
+    stage 0 gives C0_b = alpha0 op(A0_b) op(B0_b) (stage-zero beta is zero), then
+    stage 1 gives C1_b = alpha1 op(X_b) op(Y_b) + beta1 C1_b with (X, Y) = (C0_b,
+    AB1_b) when c0_left, else (AB1_b, C0_b), the C0 operand read with lda1 / ldb1.
+    C0 entries are (buffer, offset) pairs so that entries of different segments can
+    share temporary storage, as the reference's test does; the buffers are updated
+    in place.  Returns the new C1 list.
+    """
+    out = [None if c is None else c.copy() for c in C1]
+    start = 0
+    for seg in segments:
+        for b in range(start, start + seg):
+            buf, off = C0[b]
+            t = gemm_vbatched(ops0[0], ops0[1], [m0[b]], [n0[b]], [k0[b]], alpha0, [A0[b]], [lda0[b]], [B0[b]],
+                              [ldb0[b]], 0, [buf[off:].copy()], [ldc0[b]])[0]
+            buf[off:off + t.size] = t
+        for b in range(start, start + seg):
+            buf, off = C0[b]
+            tmp = buf[off:]
+            x, y = (tmp, AB1[b]) if c0_left else (AB1[b], tmp)
+            out[b] = gemm_vbatched(ops1[0], ops1[1], [m1[b]], [n1[b]], [k1[b]], alpha1, [x], [lda1[b]], [y],
+                                   [ldb1[b]], beta1, [out[b]], [ldc1[b]])[0]
+        start += seg
+    return out

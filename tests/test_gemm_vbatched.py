@@ -295,3 +295,200 @@ def test_argument_errors(handle):
                             "dims")
     # nothing was written by the rejected calls
     assert float(x.abs().sum()) == 0.0
+
+
+# ---- two stages (gemmVbatched2s) ----------------------------------------------------
+
+def _two_stage_inputs(p, left):
+    """The reference test's two-stage case (tests/test_gemm_vbatched.cpp:375-447)."""
+    m0, n0, k0 = [2, 3, 2, 5], [3, 2, 4, 2], [4, 2, 3, 2]
+    lda0, ldb0, ldc0 = list(m0), list(k0), list(m0)
+    A0 = [_matrix(p, lda0[b], k0[b], 71 * b + 1) for b in range(4)]
+    B0 = [_matrix(p, ldb0[b], n0[b], 71 * b + 19) for b in range(4)]
+    if left:
+        m1, n1, k1 = list(m0), [2, 3, 1, 1], list(n0)
+    else:
+        m1, n1, k1 = [3, 2, 4, 4], list(n0), list(m0)
+    lda1, ldb1, ldc1 = list(m1), list(k1), [m + 1 for m in m1]
+    AB1 = [_matrix(p, ldb1[b], n1[b], 71 * b + 37) if left else _matrix(p, lda1[b], k1[b], 71 * b + 37)
+           for b in range(4)]
+    C1 = [_matrix(p, ldc1[b], n1[b], 71 * b + 53) for b in range(4)]
+    alphas = (DT[p](_value(p, 17)), DT[p](_value(p, 21)), DT[p](_value(p, 25)))
+    offsets = [0, 6, 0, 8]  # the segments {2, 2} reuse one 18-element temporary buffer
+    return (m0, n0, k0, lda0, ldb0, ldc0, A0, B0, m1, n1, k1, lda1, ldb1, ldc1, AB1, C1, alphas, offsets)
+
+
+def _two_stage_loop(p, left, inp):
+    m0, n0, k0, lda0, ldb0, ldc0, A0, B0, m1, n1, k1, lda1, ldb1, ldc1, AB1, C1, (a0, a1, b1), _ = inp
+    hi = np.complex128 if p in "cz" else np.float64
+    cast = complex if p in "cz" else float
+    out = []
+    for b in range(4):
+        tmp = _loop_gemm("N", "N", m0[b], n0[b], k0[b], cast(a0), A0[b].astype(hi), lda0[b], B0[b].astype(hi),
+                         ldb0[b], 0.0, np.zeros(ldc0[b] * n0[b], dtype=hi), ldc0[b])
+        x, y = (tmp, AB1[b].astype(hi)) if left else (AB1[b].astype(hi), tmp)
+        out.append(_loop_gemm("N", "N", m1[b], n1[b], k1[b], cast(a1), x, lda1[b], y, ldb1[b], cast(b1),
+                              C1[b].astype(hi), ldc1[b]))
+    return out
+
+
+@pytest.mark.parametrize("p", list("sdcz"))
+@pytest.mark.parametrize("left", [True, False])
+def test_oracle_two_stage_matches_reference_test_loop(p, left):
+    inp = _two_stage_inputs(p, left)
+    m0, n0, k0, lda0, ldb0, ldc0, A0, B0, m1, n1, k1, lda1, ldb1, ldc1, AB1, C1, (a0, a1, b1), offs = inp
+    buf = np.full(18, np.nan, dtype=DT[p])
+    got = restated.gemm_vbatched2s("NN", m0, n0, k0, a0, A0, lda0, B0, ldb0, [(buf, o) for o in offs], ldc0,
+                                   "NN", m1, n1, k1, a1, AB1, lda1, ldb1, b1, C1, ldc1, left, [2, 2])
+    want = _two_stage_loop(p, left, inp)
+    for b in range(4):
+        g = got[b].reshape(n1[b], ldc1[b]).T[:m1[b]]
+        w = want[b].reshape(n1[b], ldc1[b]).T[:m1[b]]
+        assert np.max(np.abs(g - w)) <= TOL[p]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("p", list("sdcz"))
+@pytest.mark.parametrize("left", [True, False])
+def test_two_stage_shared_temporaries(handle, p, left):
+    torch = _torch()
+    from libddla_b200.ddla import batched
+    inp = _two_stage_inputs(p, left)
+    m0, n0, k0, lda0, ldb0, ldc0, A0, B0, m1, n1, k1, lda1, ldb1, ldc1, AB1, C1, (a0, a1, b1), offs = inp
+    tdt = {"s": torch.float32, "d": torch.float64, "c": torch.complex64, "z": torch.complex128}[p]
+    temp = torch.full((18,), float("nan"), dtype=tdt, device="cuda")
+    es = temp.element_size()
+    dC1 = [_dev(c) for c in C1]
+    batched.gemm_vbatched2s(handle, "NN", m0, n0, k0, a0, [_dev(a) for a in A0], lda0, [_dev(b) for b in B0], ldb0,
+                            [temp.data_ptr() + o * es for o in offs], ldc0, "NN", m1, n1, k1, a1,
+                            [_dev(x) for x in AB1], lda1, ldb1, b1, dC1, ldc1, left, [2, 2], tdt)
+    want = _two_stage_loop(p, left, inp)
+    for b in range(4):
+        got = dC1[b].cpu().numpy().reshape(n1[b], ldc1[b]).T
+        w = want[b].reshape(n1[b], ldc1[b]).T
+        assert np.max(np.abs(got[:m1[b]] - w[:m1[b]])) <= TOL[p], (p, left, b)
+        assert got[m1[b]:].tobytes() == C1[b].reshape(n1[b], ldc1[b]).T[m1[b]:].tobytes()
+
+
+def _two_stage_call(handle, beta0=0.0, segments=(2, 2), batch=4, **over):
+    from libddla_b200.ddla import batched
+    inp = _two_stage_inputs("d", True)
+    m0, n0, k0, lda0, ldb0, ldc0, A0, B0, m1, n1, k1, lda1, ldb1, ldc1, AB1, C1, (a0, a1, b1), offs = inp
+    torch = _torch()
+    temp = torch.zeros(18, dtype=torch.float64, device="cuda")
+    args = dict(ops0="NN", m0=m0, n0=n0, k0=k0, alpha0=a0, A0=[_dev(a) for a in A0], lda0=lda0,
+                B0=[_dev(b) for b in B0], ldb0=ldb0, C0=[temp.data_ptr() + o * 8 for o in offs], ldc0=ldc0,
+                ops1="NN", m1=m1, n1=n1, k1=k1, alpha1=a1, AB1=[_dev(x) for x in AB1], lda1=lda1, ldb1=ldb1,
+                beta1=b1, C1=[_dev(c) for c in C1], ldc1=ldc1, c0_left=True, segments=list(segments),
+                dtype=torch.float64, beta0=beta0)
+    args.update(over)
+    batched.gemm_vbatched2s(handle, **args)
+
+
+@pytest.mark.gpu
+def test_two_stage_argument_errors(handle):
+    from libddla_b200.ddla import _c_api as Cc
+    for segs in ([0, 4], [-1, 5]):
+        with pytest.raises(Cc.DdlaError, match="gemmVbatched2s: segment sizes must be positive"):
+            _two_stage_call(handle, segments=segs)
+    with pytest.raises(Cc.DdlaError, match="gemmVbatched2s: segment total does not match batch count"):
+        _two_stage_call(handle, segments=[1, 1])
+    with pytest.raises(Cc.DdlaError, match="gemmVbatched2s: missing segment sizes"):
+        _two_stage_call(handle, segments=[])
+    with pytest.raises(Cc.DdlaError, match="gemmVbatched2s: stage-zero beta must be zero"):
+        _two_stage_call(handle, beta0=1.0)
+    with pytest.raises(Cc.DdlaError, match="gemmVbatched: invalid transpose operation"):
+        _two_stage_call(handle, ops1="NX")
+    with pytest.raises(Cc.DdlaError, match="gemmVbatched: invalid dimensions at batch 2"):
+        _two_stage_call(handle, ldc1=[3, 4, 1, 5])
+    _two_stage_call(handle)  # the valid call still works after the rejected ones
+    # an empty batch is a no-op whatever the pointers are; a null pointer array is rejected
+    f = Cc.ddla_d_gemm_vbatched2s
+    one = ctypes.c_double(1.0)
+    zero = ctypes.c_double(0.0)
+    a1, z0 = ctypes.addressof(one), ctypes.addressof(zero)
+    nulls = [None] * 3
+    Cc.check_status(f(handle.ptr, b"N", b"N", *nulls, a1, None, None, None, None, z0, None, None, b"N", b"N", *nulls,
+                      a1, None, None, None, a1, None, None, 0, 0, None, 0), "empty")
+    assert f(None, b"N", b"N", *nulls, a1, None, None, None, None, z0, None, None, b"N", b"N", *nulls,
+             a1, None, None, None, a1, None, None, 0, 0, None, 0) == Cc.STATUS_INVALID_HANDLE
+    seg = (ctypes.c_int * 1)(1)
+    with pytest.raises(Cc.DdlaError, match="gemmVbatched2s: null matrix pointer array"):
+        Cc.check_status(f(handle.ptr, b"N", b"N", *nulls, a1, None, None, None, None, z0, None, None, b"N", b"N",
+                          *nulls, a1, None, None, None, a1, None, None, 0, 1, seg, 1), "null arrays")
+    with pytest.raises(Cc.DdlaError, match="gemmVbatched2s: negative batch count"):
+        Cc.check_status(f(handle.ptr, b"N", b"N", *nulls, a1, None, None, None, None, z0, None, None, b"N", b"N",
+                          *nulls, a1, None, None, None, a1, None, None, 0, -1, seg, 1), "negative")
+
+
+@pytest.mark.gpu
+def test_two_stage_segment_above_grid_limit(handle):
+    """One segment of 70000 1x1x1 entries (tests/test_gemm_vbatched.cpp:562-607):
+    C1 = alpha1 (A0 B0) AB1 + beta1 C1 with the temporaries on the left."""
+    torch = _torch()
+    from libddla_b200.ddla import _c_api as Cc
+    nb = 70000
+    data = torch.empty(5 * nb, dtype=torch.float64, device="cuda")
+    i = torch.arange(nb, device="cuda", dtype=torch.float64)
+    data[:nb] = i % 7 + 1
+    data[nb:2 * nb] = 2.0
+    data[2 * nb:3 * nb] = 0.0
+    data[3 * nb:4 * nb] = 3.0
+    data[4 * nb:] = 1.0
+    base = data.data_ptr()
+    idx = np.arange(nb, dtype=np.int64)
+    ptrs = [torch.from_numpy(base + (s * nb + idx) * 8).cuda() for s in range(5)]
+    ones = torch.ones(nb, dtype=torch.int32, device="cuda")
+    o = ones.data_ptr()
+    one, zero, half = ctypes.c_double(1.0), ctypes.c_double(0.0), ctypes.c_double(0.5)
+    seg = (ctypes.c_int * 1)(nb)
+    torch.cuda.synchronize()
+    Cc.check_status(Cc.ddla_d_gemm_vbatched2s(
+        handle.ptr, b"N", b"N", o, o, o, ctypes.addressof(one), ptrs[0].data_ptr(), o, ptrs[1].data_ptr(), o,
+        ctypes.addressof(zero), ptrs[2].data_ptr(), o, b"N", b"N", o, o, o, ctypes.addressof(one),
+        ptrs[3].data_ptr(), o, o, ctypes.addressof(half), ptrs[4].data_ptr(), o, 1, nb, seg, 1), "2s large")
+    Cc.check_status(Cc.ddla_c_synchronize(handle.ptr), "sync")
+    out = data[4 * nb:].cpu().numpy()
+    want = 6.0 * (np.arange(nb) % 7 + 1) + 0.5
+    assert np.max(np.abs(out - want)) <= 1e-12
+
+
+def test_two_stage_helper_marshalling(monkeypatch):
+    """The Python helper hands ddla_?_gemm_vbatched2s its arrays in the C
+    signature's order (host tensors and a stub in place of the library call)."""
+    torch = _torch()
+    from libddla_b200.ddla import _c_api as Cc
+    from libddla_b200.ddla import batched
+    seen = {}
+
+    def ints(addr, n, kind=ctypes.c_int):
+        return list((kind * n).from_address(addr)) if addr else None
+
+    def stub(h, ta0, tb0, m0, n0, k0, al0, A0, lda0, B0, ldb0, be0, C0, ldc0, ta1, tb1, m1, n1, k1, al1, AB1, lda1,
+             ldb1, be1, C1, ldc1, left, batch, seg, nseg):
+        ll = ctypes.c_longlong
+        seen.update(ops=(ta0, tb0, ta1, tb1), dims0=[ints(x, batch) for x in (m0, n0, k0, lda0, ldb0, ldc0)],
+                    dims1=[ints(x, batch) for x in (m1, n1, k1, lda1, ldb1, ldc1)],
+                    ptrs=[ints(x, batch, ll) for x in (A0, B0, C0, AB1, C1)],
+                    scal=[ctypes.c_double.from_address(x).value for x in (al0, be0, al1, be1)],
+                    left=left, batch=batch, seg=ints(seg, nseg), nseg=nseg, h=h)
+        return 0
+
+    monkeypatch.setattr(Cc, "ddla_d_gemm_vbatched2s", stub)
+    monkeypatch.setattr(Cc, "ddla_c_synchronize", lambda h: 0)
+
+    class _H:
+        ptr = 77
+
+    mats = [torch.zeros(4, dtype=torch.float64) for _ in range(6)]
+    batched.gemm_vbatched2s(_H(), "nT", [1, 2], [3, 4], [5, 6], 1.5, mats[:2], [7, 8], mats[2:4], [9, 10],
+                            [1000, 2000], [11, 12], "CN", [13, 14], [15, 16], [17, 18], 2.5, [mats[4], None],
+                            [19, 20], [21, 22], -0.5, [None, mats[5]], [23, 24], False, [1, 1], torch.float64)
+    assert seen["h"] == 77 and seen["batch"] == 2 and seen["left"] == 0
+    assert seen["ops"] == (b"n", b"T", b"C", b"N")
+    assert seen["dims0"] == [[1, 2], [3, 4], [5, 6], [7, 8], [9, 10], [11, 12]]
+    assert seen["dims1"] == [[13, 14], [15, 16], [17, 18], [19, 20], [21, 22], [23, 24]]
+    d = [m.data_ptr() for m in mats]
+    assert seen["ptrs"] == [[d[0], d[1]], [d[2], d[3]], [1000, 2000], [d[4], 0], [0, d[5]]]
+    assert seen["scal"] == [1.5, 0.0, 2.5, -0.5]
+    assert seen["seg"] == [1, 1] and seen["nseg"] == 2
