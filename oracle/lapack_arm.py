@@ -1,4 +1,4 @@
-"""The reference's 1x1 CPU arm through real LAPACK (TEST / BASELINE INFRASTRUCTURE ONLY).
+"""The reference's 1x1 CPU arm through real LAPACK (TEST AND CPU-BASELINE INFRASTRUCTURE ONLY).
 
 On a CPU handle with a 1x1 grid the reference's pposv is exactly
     ?potrf_(uplo, n, A, LLD, info)                    src/Cholesky/potrf.cpp:41-59
