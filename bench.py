@@ -179,7 +179,7 @@ def run_reference(args, rank: int):
     info = None
     sample = ""
     for i in range(args.warmup + args.steps):
-        tf, sample, info = cpu_sample(budget_s=8.0, nrhs=args.nrhs, kappa=args.kappa)
+        tf, sample, info = cpu_sample(budget_s=args.cpu_budget, nrhs=args.nrhs, kappa=args.kappa)
         if i >= args.warmup:
             tf_steps.append(tf)
     v = statistics.median(tf_steps)
@@ -640,6 +640,8 @@ def main(argv=None):
     ap.add_argument("--nrhs", type=int, default=8)
     ap.add_argument("--kappa", type=float, default=1e6)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=8.0,
+                    help="seconds of CPU work per step of the reference arm's bounded sample")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-gp", action="store_true")
