@@ -230,6 +230,82 @@ def read_kernels(C):
 # ---------------------------------------------------------------------------
 # secondary legs: batched uneven SPD (factor+solve+logdet) and the GP likelihood
 # ---------------------------------------------------------------------------
+def gemm_vbatched_leg(args, torch, device, h, stream, C):
+    """Variable-size batched GEMM (gemmVbatched): 2000 entries, m, n, k uniform in [32, 256],
+    C_i = A_i B_i + 0.5 C_i, column-major with tight leading dimensions, for s/d/c/z.  Timed
+    through the kernel layer (ddlak_gemm_vbatched, kernel only) and through the public C ABI
+    (ddla_?_gemm_vbatched: the device validation pass and its read-back included); 8 entries
+    are checked against a torch FP64 product."""
+    lib = C.lib
+    f = lib.ddlak_gemm_vbatched
+    f.restype = ctypes.c_int
+    f.argtypes = ([ctypes.c_char, ctypes.c_char, ctypes.c_char, ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 11
+                  + [ctypes.c_int, ctypes.c_void_p])
+    out = {}
+    nb, reps = 2000, 20
+    rng = np.random.default_rng(0xDD1A0006)
+    m, n, k = (rng.integers(32, 257, nb).astype(np.int32) for _ in range(3))
+    mk, kn, mn = (a.astype(np.int64) * b for a, b in ((m, k), (k, n), (m, n)))
+    offA, offB, offC = (np.concatenate([[0], np.cumsum(x)[:-1]]) for x in (mk, kn, mn))
+    dm, dn, dk = (torch.from_numpy(x).to(device) for x in (m, n, k))
+    for code, tdt, sdt in (("s", torch.float32, np.float32), ("d", torch.float64, np.float64),
+                           ("c", torch.complex64, np.complex64), ("z", torch.complex128, np.complex128)):
+        g = torch.Generator(device=device).manual_seed(0xDD1A0006)
+        A = torch.randn(int(mk.sum()), dtype=tdt, device=device, generator=g)
+        B = torch.randn(int(kn.sum()), dtype=tdt, device=device, generator=g)
+        C0 = torch.randn(int(mn.sum()), dtype=tdt, device=device, generator=g)
+        Cw = C0.clone()
+        es = A.element_size()
+        pa, pb, pc = (torch.from_numpy(t.data_ptr() + off * es).to(device) for t, off in ((A, offA), (B, offB),
+                                                                                             (Cw, offC)))
+        al, be = np.array([1.0], dtype=sdt), np.array([0.5], dtype=sdt)
+        torch.cuda.synchronize()
+
+        def kernel_call():
+            rc = f(code.encode(), b"N", b"N", int(m.max()), int(n.max()), dm.data_ptr(), dn.data_ptr(), dk.data_ptr(),
+                   al.ctypes.data, pa.data_ptr(), dm.data_ptr(), pb.data_ptr(), dk.data_ptr(), be.ctypes.data,
+                   pc.data_ptr(), dm.data_ptr(), nb, stream.cuda_stream)
+            assert rc == 0, rc
+
+        def api_call():
+            fn = getattr(C, f"ddla_{code}_gemm_vbatched")
+            C.check_status(fn(h.ptr, b"N", b"N", dm.data_ptr(), dn.data_ptr(), dk.data_ptr(), al.ctypes.data,
+                              pa.data_ptr(), dm.data_ptr(), pb.data_ptr(), dk.data_ptr(), be.ctypes.data,
+                              pc.data_ptr(), dm.data_ptr(), nb), "gemm_vbatched")
+
+        # parity: one call on a fresh C, 8 entries against torch in FP64
+        kernel_call()
+        torch.cuda.synchronize()
+        hi = torch.complex128 if code in "cz" else torch.float64
+        err = 0.0
+        for i in rng.choice(nb, 8, replace=False):
+            a = A[offA[i]:offA[i] + mk[i]].view(int(k[i]), int(m[i])).t().to(hi)
+            b = B[offB[i]:offB[i] + kn[i]].view(int(n[i]), int(k[i])).t().to(hi)
+            c0 = C0[offC[i]:offC[i] + mn[i]].view(int(n[i]), int(m[i])).t().to(hi)
+            want = a @ b + 0.5 * c0
+            got = Cw[offC[i]:offC[i] + mn[i]].view(int(n[i]), int(m[i])).t().to(hi)
+            err = max(err, float((got - want).abs().max() / want.abs().max()))
+        assert err < (1e-4 if code in "sc" else 1e-12), (code, err)
+        flops = float((2.0 * m.astype(np.float64) * n * k).sum()) * (4 if code in "cz" else 1)
+        res = {"max_rel_err_vs_torch_fp64": err}
+        for name, fn in (("kernel", kernel_call), ("api", api_call)):
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                fn()
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            res[name] = {"ms": ms, "tflops": flops / ms / 1e9}
+        out[code] = res
+    return {"metric": "batched GEMM TFLOP/s", "unit": "TFLOP/s",
+            "config": {"workload": "2000 entries, m, n, k ~ U[32, 256], NN, alpha 1, beta 0.5, tight ld",
+                       "launch": "one validation pass + one tiled launch per call"}, **out}
+
+
 def batched_leg(args, torch, device, h, stream, C):
     """4096 matrices, n_i uniform in [16, 512], A_i = G_i G_i^T / n_i + 0.1 I, b_i ~ N(0, 1):
     one persistent launch replayed from a CUDA graph (VbatchedPlan) vs a per-matrix loop
@@ -489,9 +565,14 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     tf = lambda total_ms: world * flops_pposv(n, nrhs) * args.steps / (total_ms * 1e-3) / 1e12
 
     only = args.only
-    if only in ("batched", "gp"):
+    if only in ("batched", "gp", "gemm-vbatched"):
         # one secondary leg alone (a profiling driver): its object is the line
-        leg = batched_leg(args, torch, device, h, stream, C) if only == "batched" else gp_leg(args, torch, device)
+        if only == "batched":
+            leg = batched_leg(args, torch, device, h, stream, C)
+        elif only == "gp":
+            leg = gp_leg(args, torch, device)
+        else:
+            leg = gemm_vbatched_leg(args, torch, device, h, stream, C)
         if rank == 0:
             print(json.dumps({"only": only, only: leg}), flush=True)
         h.destroy()
@@ -648,7 +729,8 @@ def main(argv=None):
     ap.add_argument("--no-gp-large", action="store_true")
     ap.add_argument("--batched-count", type=int, default=4096)
     ap.add_argument("--gp-batch", type=int, default=256)
-    ap.add_argument("--only", choices=["mixed-B", "mixed-T", "plain", "batched", "gp"], default=None,
+    ap.add_argument("--only", choices=["mixed-B", "mixed-T", "plain", "batched", "gp", "gemm-vbatched"],
+                    default=None,
                     help="run one leg alone (profiling driver); prints that leg's figures only")
     args = ap.parse_args(argv)
     world = int(os.environ.get("WORLD_SIZE", "1"))
