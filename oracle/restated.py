@@ -168,3 +168,45 @@ def gemm_vbatched2s(ops0, m0, n0, k0, alpha0, A0, lda0, B0, ldb0, C0, ldc0,
                                    [ldb1[b]], beta1, [out[b]], [ldc1[b]])[0]
         start += seg
     return out
+
+
+def herm_complete(a: np.ndarray, uplo: str, n: int) -> None:
+    """In place: the leading n x n becomes Hermitian from its uplo triangle, with a
+    real diagonal (the reference's herm_complete, used by phegst.cpp:140-176)."""
+    if n == 0:
+        return
+    v = a[:n, :n]
+    low = uplo.upper() == "L"
+    sel = np.tril(v, -1) if low else np.triu(v, 1)
+    d = np.real(np.diag(v)).astype(v.dtype)
+    v[...] = sel + np.conj(sel.T) + np.diag(d)
+
+
+def phegst(a: np.ndarray, factor: np.ndarray, uplo: str = "L", n: int | None = None) -> np.ndarray:
+    """Type-1 reduction of a Hermitian-definite pair on host arrays (returns a copy).
+
+    Restates the reference's phegst at a 1x1 grid (src/Eigensolver/phegst.cpp:
+    140-176, include/ddla/ddla.h:2540-2562): with B = L L^H (uplo 'L') or U^H U
+    ('U') held in factor's selected triangle, A is completed to a Hermitian
+    matrix from its selected triangle (real diagonal), then A <- op(L)^-1 A and
+    A <- A op(L)^-H (op(L) = L, or U^H), and the result is completed again from
+    its selected triangle.  Only the selected triangles of A and factor are read;
+    rows and columns past n are left as they were.
+    """
+    from scipy.linalg import solve_triangular
+
+    a = np.array(a, copy=True, order="F")
+    n = a.shape[1] if n is None else n
+    if n == 0:
+        return a
+    low = uplo.upper() == "L"
+    f = factor[:n, :n]
+    L = np.tril(f) if low else np.conj(np.triu(f)).T  # the lower factor, other triangle never read
+    hi = np.complex128 if np.iscomplexobj(a) else np.float64
+    w = np.array(a[:n, :n], dtype=hi)
+    herm_complete(w, uplo, n)
+    w = solve_triangular(L.astype(hi), w, lower=True)
+    w = np.conj(solve_triangular(L.astype(hi), np.conj(w).T, lower=True)).T
+    herm_complete(w, uplo, n)
+    a[:n, :n] = w.astype(a.dtype)
+    return a
