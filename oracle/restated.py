@@ -1,8 +1,13 @@
-"""ctypes wrapper of oracle/ddla_oracle.c (TEST INFRASTRUCTURE ONLY).
+"""The oracle's Python face (TEST INFRASTRUCTURE ONLY: imported by tests/, the
+smoke check and bench.py's CPU baseline, never by the product).
 
-Every function takes NumPy arrays and works on Fortran-ordered copies; the
-C code it calls restates the reference's CPU arm (see ddla_oracle.c for the
-reference file:line each routine follows).
+potrf, potrf_bottom_right, ppotrs, pposv and diag_logdet are ctypes wrappers of
+oracle/ddla_oracle.c, whose C code restates the reference's CPU arm (see
+ddla_oracle.c for the reference file:line each routine follows).  The batched
+GEMM (gemm_vbatched, gemm_vbatched2s) and the Hermitian-definite reduction
+(herm_complete, phegst) are restated here in NumPy/SciPy, each citing the
+reference lines it follows.  Every function takes NumPy arrays and works on
+copies.
 """
 from __future__ import annotations
 
