@@ -183,6 +183,46 @@ def shard_lpt(orders, world: int):
     return [sorted(s) for s in shards]
 
 
+def sharded_run(orders, compute, group=None, device=None):
+    """One process per GPU over a batch: this rank's LPT shard (shard_lpt) is
+    handed to compute(indices) -> (len(indices), k) tensor of per-matrix results
+    (e.g. logdet and info from posv_vbatched on the shard), and one all-gather of
+    (index, values) rows gives every rank the (len(orders), k) float64 result in
+    the batch's order.  It is the only exchange step of the sharded batch.
+    Without an initialised torch.distributed group it runs the whole batch
+    locally.  device: where the exchange buffers live (the backend's device,
+    e.g. cuda:r for NCCL); default: compute's result device."""
+    import torch
+
+    dist = torch.distributed
+    world = dist.get_world_size(group) if dist.is_available() and dist.is_initialized() else 1
+    rank = dist.get_rank(group) if world > 1 else 0
+    shards = shard_lpt(orders, world)
+    mine = shards[rank]
+    vals = torch.as_tensor(compute(list(mine)), dtype=torch.float64)
+    if vals.dim() == 1:
+        vals = vals.unsqueeze(1)
+    if vals.shape[0] != len(mine):
+        raise ValueError("sharded_run: compute must return one row per index")
+    dev = torch.device(device) if device is not None else vals.device
+    k = vals.shape[1]
+    out = torch.full((len(orders), k), float("nan"), dtype=torch.float64, device=dev)
+    if world == 1:
+        out[torch.as_tensor(list(mine), dtype=torch.long, device=dev)] = vals.to(dev)
+        return out
+    m = max(len(sh) for sh in shards)
+    buf = torch.full((m, 1 + k), -1.0, dtype=torch.float64, device=dev)
+    if mine:
+        buf[:len(mine), 0] = torch.as_tensor(list(mine), dtype=torch.float64, device=dev)
+        buf[:len(mine), 1:] = vals.to(dev)
+    gathered = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(gathered, buf, group=group)
+    for g in gathered:
+        rows = g[:, 0] >= 0
+        out[g[rows, 0].long()] = g[rows, 1:]
+    return out
+
+
 # ---- variable-size batched GEMM --------------------------------------------
 _GV_SFX = {"torch.float32": "s", "torch.float64": "d", "torch.complex64": "c", "torch.complex128": "z"}
 
