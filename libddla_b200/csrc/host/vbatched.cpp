@@ -12,6 +12,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <numeric>
 #include <stdexcept>
@@ -257,10 +258,11 @@ VbatchedPlan* VbatchedPlan::create(const DdlaHandle_t& h, char uplo, const int* 
                                    T* const* d_B, double* d_logdet, int* d_info, int batch, int max_n)
 {
     check_args(h, "VbatchedPlan", uplo, d_n, d_A, d_lda, d_logdet, d_info, batch, max_n);
-    auto* plan = new VbatchedPlan();
+    // owned until returned: any throw below releases the plan and what it holds
+    std::unique_ptr<VbatchedPlan> plan(new VbatchedPlan());
     plan->impl_ = new Impl(make_impl<T>(h, d_n, d_A, d_lda, d_B, d_logdet, d_info, batch, max_n));
     Impl& p = *plan->impl_;
-    try {
+    {
         if (batch > 0) {
             prepare(p, plan->flops_, false);
             detail::cuda_check(cudaStreamSynchronize(h->stream), "stream synchronisation");
@@ -280,11 +282,8 @@ VbatchedPlan* VbatchedPlan::create(const DdlaHandle_t& h, char uplo, const int* 
             detail::cuda_check(cudaGraphInstantiate(&p.exec, p.graph, 0), "VbatchedPlan: graph instantiation");
         }
         plan->grid_ = p.grid;
-    } catch (...) {
-        delete plan;
-        throw;
     }
-    return plan;
+    return plan.release();
 }
 
 void VbatchedPlan::run()
@@ -366,14 +365,23 @@ VbatchedTuning autotune_typed(const DdlaHandle_t& h, int nmax)
     // enough matrices for a few waves of the largest grid
     const int count = 3 * maxgrid;
     const size_t mat_elems = (size_t)count * nmax * nmax;
-    T* d_mats = nullptr;
-    T* d_b = nullptr;
-    char* small = nullptr;
-    detail::cuda_check(cudaMalloc(&d_mats, sizeof(T) * mat_elems), "tune allocation");
-    detail::cuda_check(cudaMalloc(&d_b, sizeof(T) * (size_t)count * nmax), "tune allocation");
+    // the three buffers are freed on every exit, a throw included
+    struct DeviceBuffers {
+        void* p[3] = {nullptr, nullptr, nullptr};
+        ~DeviceBuffers()
+        {
+            for (void* q : p)
+                if (q) cudaFree(q);
+        }
+    } bufs;
     const size_t sb = sizeof(T*) * 2 * count + sizeof(int) * 2 * count + sizeof(double) * count + sizeof(int) * count +
                       count + 64;
-    detail::cuda_check(cudaMalloc(&small, sb + 256), "tune allocation");
+    detail::cuda_check(cudaMalloc(&bufs.p[0], sizeof(T) * mat_elems), "tune allocation");
+    detail::cuda_check(cudaMalloc(&bufs.p[1], sizeof(T) * (size_t)count * nmax), "tune allocation");
+    detail::cuda_check(cudaMalloc(&bufs.p[2], sb + 256), "tune allocation");
+    T* d_mats = static_cast<T*>(bufs.p[0]);
+    T* d_b = static_cast<T*>(bufs.p[1]);
+    char* small = static_cast<char*>(bufs.p[2]);
     char* c = small;
     T** d_ptrs = reinterpret_cast<T**>(c);
     c += sizeof(T*) * 2 * count;
@@ -389,7 +397,7 @@ VbatchedTuning autotune_typed(const DdlaHandle_t& h, int nmax)
     c += 16;
     unsigned char* d_wsel = reinterpret_cast<unsigned char*>(c);
     detail::cuda_check(cudaMemset(d_counters, 0, 16), "tune counters");
-    try {
+    {
         // grid: time a mid-size order at one CTA per SM and at full residency
         if (maxgrid > sms) {
             const int mid = std::min(nmax, 256);
@@ -407,15 +415,7 @@ VbatchedTuning autotune_typed(const DdlaHandle_t& h, int nmax)
                                            d_logdet, d_info, d_wsel, d_counters, 3);
             tt.variant[b] = t1 < t0 ? 1 : 0;
         }
-    } catch (...) {
-        cudaFree(d_mats);
-        cudaFree(d_b);
-        cudaFree(small);
-        throw;
     }
-    cudaFree(d_mats);
-    cudaFree(d_b);
-    cudaFree(small);
     tt.tuned = true;
     return tt;
 }
