@@ -125,7 +125,13 @@ static ddlaStatus_t set_impl(DdlaHandle_t handle, const MPI_Comm& comm, int npro
         if (e2 != cudaSuccess) return from_cuda(e2);
         handle->owns_stream = true;
         const cudaError_t e3 = cudaMallocHost(reinterpret_cast<void**>(&handle->host_word), 64);
-        if (e3 != cudaSuccess) return from_cuda(e3);
+        if (e3 != cudaSuccess) {  // leave the handle as it was, so a retry starts clean
+            cudaStreamDestroy(handle->stream);
+            handle->stream = nullptr;
+            handle->owns_stream = false;
+            handle->host_word = nullptr;
+            return from_cuda(e3);
+        }
         // Workspace comes from the device's stream-ordered pool (cudaMallocAsync).
         // Keep freed blocks in the pool instead of unmapping them at every
         // synchronisation: the multi-GB workspaces of consecutive calls then reuse
@@ -157,7 +163,7 @@ ddlaStatus_t ddlaDestroy(DdlaHandle_t& handle)
 {
     if (handle == nullptr) return ddlaStatus_t::DDLA_STATUS_SUCCESS;
     DdlaStream* s = handle;
-    if (s->initialized) {
+    if (s->initialized || s->stream || s->host_word) {
         cudaSetDevice(s->device);
         if (s->stream) cudaStreamSynchronize(s->stream);
         if (s->owns_stream && s->stream) cudaStreamDestroy(s->stream);

@@ -330,9 +330,17 @@ float time_batch(const DdlaHandle_t& h, int nmax, int order, int count, int vari
                        "tune");
     detail::cuda_check(cudaMemcpyAsync(d_wsel, ws.data(), count, cudaMemcpyHostToDevice, st), "tune");
     detail::cuda_check(cudaStreamSynchronize(st), "stream synchronisation");
-    cudaEvent_t e0, e1;
-    detail::cuda_check(cudaEventCreate(&e0), "tune event");
-    detail::cuda_check(cudaEventCreate(&e1), "tune event");
+    struct Events {  // destroyed on every exit, a throw included
+        cudaEvent_t e[2] = {nullptr, nullptr};
+        ~Events()
+        {
+            for (cudaEvent_t x : e)
+                if (x) cudaEventDestroy(x);
+        }
+    } ev;
+    detail::cuda_check(cudaEventCreate(&ev.e[0]), "tune event");
+    detail::cuda_check(cudaEventCreate(&ev.e[1]), "tune event");
+    cudaEvent_t e0 = ev.e[0], e1 = ev.e[1];
     std::vector<float> ms;
     for (int r = 0; r < reps + 1; ++r) {
         detail::kernel_check(ddlak_fill_spd_vbatched(tcode<T>(), count, d_n, reinterpret_cast<void* const*>(d_ptrs),
@@ -349,8 +357,6 @@ float time_batch(const DdlaHandle_t& h, int nmax, int order, int count, int vari
         detail::cuda_check(cudaEventElapsedTime(&t, e0, e1), "tune event");
         if (r > 0) ms.push_back(t);  // first run warms up
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     std::sort(ms.begin(), ms.end());
     return ms[ms.size() / 2];
 }
