@@ -230,6 +230,40 @@ def read_kernels(C):
 # ---------------------------------------------------------------------------
 # secondary legs: batched uneven SPD (factor+solve+logdet) and the GP likelihood
 # ---------------------------------------------------------------------------
+def vendor_leg(args, torch, A0, B0, backward_error):
+    """The reference's GPU arm at a 1x1 grid: one cusolverDn?potrf and two cublas?trsm
+    (src/Cholesky/ppotrf.cpp:39-54 -> potrf.cpp:106-113; ppotrs.cpp:44-61 -> trsm.cpp:154-159).
+    torch.linalg.cholesky_ex and torch.cholesky_solve call cuSOLVER's potrf and potrs on the
+    bench's matrix and right-hand sides (FP64); CUDA events on torch's stream around each
+    solve, the factor's allocation included as the reference allocates its lwork per call."""
+    n, nrhs = args.n, args.nrhs
+    B = B0.T  # the n x nrhs view of the column-major right-hand sides
+
+    def step():
+        L, info = torch.linalg.cholesky_ex(A0)
+        return info, torch.cholesky_solve(B, L)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    times, last = [], None
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        last = step()
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    info, X = last
+    assert int(info.item()) == 0, int(info.item())
+    total = sum(times)
+    return {"metric": "pposv TFLOP/s through cuSOLVER (the reference's GPU arm)", "unit": "TFLOP/s",
+            "value": flops_pposv(n, nrhs) * args.steps / (total * 1e-3) / 1e12, "ms_per_step": total / args.steps,
+            "backward_error": backward_error(X.T),
+            "config": {"workload": f"pposv d uplo=L n={n} nrhs={nrhs} kappa={args.kappa:g}",
+                       "calls": "torch.linalg.cholesky_ex + torch.cholesky_solve (cuSOLVER potrf, potrs)"}}
+
+
 def gemm_vbatched_leg(args, torch, device, h, stream, C):
     """Variable-size batched GEMM (gemmVbatched): 2000 entries, m, n, k uniform in [32, 256],
     C_i = A_i B_i + 0.5 C_i, column-major with tight leading dimensions, for s/d/c/z.  Timed
@@ -578,6 +612,13 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         h.destroy()
         return
 
+    if only == "vendor":
+        leg = vendor_leg(args, torch, A0, B0, backward_error)
+        if rank == 0:
+            print(json.dumps({"only": only, only: leg}), flush=True)
+        h.destroy()
+        return
+
     # ---- mixed precision + refinement (headline) ----
     mixed = {}
     precs = ("B", "T") if only is None else ((only[-1],) if only.startswith("mixed-") else ())
@@ -729,7 +770,7 @@ def main(argv=None):
     ap.add_argument("--no-gp-large", action="store_true")
     ap.add_argument("--batched-count", type=int, default=4096)
     ap.add_argument("--gp-batch", type=int, default=256)
-    ap.add_argument("--only", choices=["mixed-B", "mixed-T", "plain", "batched", "gp", "gemm-vbatched"],
+    ap.add_argument("--only", choices=["mixed-B", "mixed-T", "plain", "batched", "gp", "gemm-vbatched", "vendor"],
                     default=None,
                     help="run one leg alone (profiling driver); prints that leg's figures only")
     args = ap.parse_args(argv)
