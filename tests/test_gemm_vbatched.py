@@ -492,3 +492,51 @@ def test_two_stage_helper_marshalling(monkeypatch):
     assert seen["ptrs"] == [[d[0], d[1]], [d[2], d[3]], [1000, 2000], [d[4], 0], [0, d[5]]]
     assert seen["scal"] == [1.5, 0.0, 2.5, -0.5]
     assert seen["seg"] == [1, 1] and seen["nseg"] == 2
+
+
+# ---- one real and one complex operand: the oracle ------------------------------------
+
+def _mixed_value(i):
+    return ((i % 11) - 5) * 0.0625  # tests/test_gemm_vbatched_mixed.cpp:20-25
+
+
+def _mixed_loop(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
+    """Loop port of the mixed test's oracle (tests/test_gemm_vbatched_mixed.cpp:26-42):
+    'C' conjugates an element (a no-op on a real one), beta == 0 does not read C."""
+    def at(X, ld, t, i, j):
+        z = complex(X[i + j * ld] if t == "N" else X[j + i * ld])
+        return z.conjugate() if t == "C" else z
+
+    C = C.astype(np.complex128).copy()
+    for j in range(n):
+        for i in range(m):
+            s = 0j
+            if alpha != 0:
+                for l in range(k):
+                    s += at(A, lda, ta, i, l) * at(B, ldb, tb, l, j)
+            z = alpha * s
+            if beta != 0:
+                z += beta * C[i + j * ldc]
+            C[i + j * ldc] = z
+    return C
+
+
+@pytest.mark.parametrize("left", [False, True])
+@pytest.mark.parametrize("ta,tb", [(a, b) for a in "NTC" for b in "NTC"])
+def test_oracle_mixed_operands_match_reference_test_loop(left, ta, tb):
+    m, n, k = [3, 7, 0, 5, 2], [4, 2, 3, 0, 3], [5, 0, 2, 4, 1]
+    la = [max(1, m[q] if ta == "N" else k[q]) + 2 for q in range(5)]
+    lb = [max(1, k[q] if tb == "N" else n[q]) + 1 for q in range(5)]
+    lc = [max(1, m[q]) + 3 for q in range(5)]
+    cv = lambda i: complex(_mixed_value(i), _mixed_value(3 * i + 1))
+    rv = _mixed_value
+    A = [np.array([(cv if left else rv)(p + q) for p in range(la[q] * max(1, k[q] if ta == "N" else m[q]))])
+         for q in range(5)]
+    B = [np.array([(rv if left else cv)(p + q + 4) for p in range(lb[q] * max(1, n[q] if tb == "N" else k[q]))])
+         for q in range(5)]
+    C = [np.array([cv(p + q + 2) for p in range(lc[q] * max(1, n[q]))]) for q in range(5)]
+    alpha, beta = 0.7 - 0.2j, -0.3 + 0.1j
+    got = restated.gemm_vbatched(ta, tb, m, n, k, alpha, A, la, B, lb, beta, C, lc)
+    for q in range(5):
+        want = _mixed_loop(ta, tb, m[q], n[q], k[q], alpha, A[q], la[q], B[q], lb[q], beta, C[q], lc[q])
+        assert np.max(np.abs(got[q] - want)) <= 1e-13
