@@ -95,6 +95,59 @@ void gemmVbatched(const DdlaHandle_t& handle, char transA, char transB, int* d_m
                   const T* const* d_A_array, int* d_lda, const T* const* d_B_array, int* d_ldb, T beta,
                   T** d_C_array, int* d_ldc, int batch_count);
 
+// One real and one complex operand, complex alpha, beta and output (reference
+// ddla.h:1878-1939, src/BLAS/gemm_mixed.cpp:787-870): the rules of gemmVbatched,
+// with 'C' on the real operand meaning 'T', and an entry whose product or
+// scaling needs a null matrix rejected ("gemmVbatched(mixed): null matrix at
+// batch <b>") before anything is written.
+template <typename R>
+void gemmVbatched(const DdlaHandle_t& handle, char transA, char transB, int* d_m, int* d_n, int* d_k,
+                  std::complex<R> alpha, const R* const* d_A_array, int* d_lda,
+                  const std::complex<R>* const* d_B_array, int* d_ldb, std::complex<R> beta,
+                  std::complex<R>** d_C_array, int* d_ldc, int batch_count);
+template <typename R>
+void gemmVbatched(const DdlaHandle_t& handle, char transA, char transB, int* d_m, int* d_n, int* d_k,
+                  std::complex<R> alpha, const std::complex<R>* const* d_A_array, int* d_lda,
+                  const R* const* d_B_array, int* d_ldb, std::complex<R> beta, std::complex<R>** d_C_array,
+                  int* d_ldc, int batch_count);
+
+// Two stages with one real and one complex operand somewhere (reference
+// ddla.h:1893-2030, src/BLAS/gemm_mixed.cpp:878-994): (A0, B0, C0, AB1) element
+// types (R, Z, Z, R), (Z, R, Z, R), (R, Z, Z, Z), (Z, R, Z, Z), (Z, Z, Z, R),
+// (R, R, R, Z) with Z = std::complex<R>; C1 is complex.  The rules of
+// gemmVbatched2s, the mixed one-stage checks for both stages, and, when
+// alpha_1 != 0, "gemmVbatched2s(mixed): incompatible intermediate dimensions"
+// unless stage 1 reads C0 as the m0 x n0 matrix with leading dimension ldc0.
+#define DDLA_GEMM_VBATCHED2S_MIXED(TA, TB, T0, TX)                                                               \
+    template <typename R>                                                                                        \
+    void gemmVbatched2s(const DdlaHandle_t& handle, char transA_0, char transB_0, int* d_m_0, int* d_n_0,       \
+                        int* d_k_0, T0 alpha_0, const TA* const* d_A_array_0, int* d_lda_0,                      \
+                        const TB* const* d_B_array_0, int* d_ldb_0, T0 beta_0, T0** d_C_array_0, int* d_ldc_0,  \
+                        char transA_1, char transB_1, int* d_m_1, int* d_n_1, int* d_k_1,                        \
+                        std::complex<R> alpha_1, const TX* const* d_AB_array_1, int* d_lda_1, int* d_ldb_1,      \
+                        std::complex<R> beta_1, std::complex<R>** d_C_array_1, int* d_ldc_1, bool C0_left,       \
+                        int batch_count, const int* segment_sizes, int segment_count);
+DDLA_GEMM_VBATCHED2S_MIXED(R, std::complex<R>, std::complex<R>, R)
+DDLA_GEMM_VBATCHED2S_MIXED(std::complex<R>, R, std::complex<R>, R)
+DDLA_GEMM_VBATCHED2S_MIXED(R, std::complex<R>, std::complex<R>, std::complex<R>)
+DDLA_GEMM_VBATCHED2S_MIXED(std::complex<R>, R, std::complex<R>, std::complex<R>)
+DDLA_GEMM_VBATCHED2S_MIXED(std::complex<R>, std::complex<R>, std::complex<R>, R)
+DDLA_GEMM_VBATCHED2S_MIXED(R, R, R, std::complex<R>)
+#undef DDLA_GEMM_VBATCHED2S_MIXED
+
+// Type-1 reduction of a Hermitian-definite pair with a caller's factor
+// (reference ddla.h:2540-2562): with factorB holding B = L L^H ('L') or U^H U
+// ('U'), A becomes L^-1 A L^-H (U^-H A U^-1), the whole leading n x n written
+// Hermitian with a real diagonal.  Only the uplo triangles of A and factorB are
+// read; factorB and everything outside the leading n x n are left as they were.
+// descA / descB: matching square source-zero blocks covering n x n; the spans
+// must not overlap.  std::invalid_argument for bad arguments (the reference's
+// messages), std::runtime_error for a null handle.  Returns with the handle's
+// stream synchronised.
+template <typename T>
+void phegst(const DdlaHandle_t& handle, char uplo, int n, T* A, const int* descA, const T* factorB,
+            const int* descB);
+
 // Two dependent batched GEMM stages sharing reusable temporaries (reference
 // ddla.h:1851-1876, src/BLAS/gemm_vbatched.cpp:420-509): for each host-resident
 // segment of segment_sizes in turn, stage 0 gives C0_b = alpha_0 op(A0_b)

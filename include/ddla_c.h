@@ -125,6 +125,27 @@ int ddla_s_pdiag_logdet(void* handle, int n, const void* A, const int* descA, vo
 int ddla_d_pdiag_logdet(void* handle, int n, const void* A, const int* descA, void* result);
 int ddla_c_pdiag_logdet(void* handle, int n, const void* A, const int* descA, void* result);
 int ddla_z_pdiag_logdet(void* handle, int n, const void* A, const int* descA, void* result);
+/* phegst (reference include/ddla/ddla.h:2560-2562, no C export there): the
+ * type-1 Hermitian-definite reduction of A with the factor held in F */
+int ddla_s_phegst(void* handle, char uplo, int n, void* A, const int* descA, const void* F, const int* descF);
+int ddla_d_phegst(void* handle, char uplo, int n, void* A, const int* descA, const void* F, const int* descF);
+int ddla_c_phegst(void* handle, char uplo, int n, void* A, const int* descA, const void* F, const int* descF);
+int ddla_z_phegst(void* handle, char uplo, int n, void* A, const int* descA, const void* F, const int* descF);
+/* The mixed gemmVbatched overloads (reference include/ddla/ddla.h:1878-1939, C++
+ * only there): _rc takes a real A and a complex B, _cr a complex A and a real B;
+ * alpha, beta and C are complex (the c / z prefix is their type). */
+int ddla_c_gemm_vbatched_rc(void* handle, char transA, char transB, int* d_m, int* d_n, int* d_k, const void* alpha,
+                            const void* const* d_A, int* d_lda, const void* const* d_B, int* d_ldb, const void* beta,
+                            void** d_C, int* d_ldc, int batch_count);
+int ddla_c_gemm_vbatched_cr(void* handle, char transA, char transB, int* d_m, int* d_n, int* d_k, const void* alpha,
+                            const void* const* d_A, int* d_lda, const void* const* d_B, int* d_ldb, const void* beta,
+                            void** d_C, int* d_ldc, int batch_count);
+int ddla_z_gemm_vbatched_rc(void* handle, char transA, char transB, int* d_m, int* d_n, int* d_k, const void* alpha,
+                            const void* const* d_A, int* d_lda, const void* const* d_B, int* d_ldb, const void* beta,
+                            void** d_C, int* d_ldc, int batch_count);
+int ddla_z_gemm_vbatched_cr(void* handle, char transA, char transB, int* d_m, int* d_n, int* d_k, const void* alpha,
+                            const void* const* d_A, int* d_lda, const void* const* d_B, int* d_ldb, const void* beta,
+                            void** d_C, int* d_ldc, int batch_count);
 /* gemmVbatched (reference include/ddla/ddla.h:1836-1849, a C++ template with
  * no C export there): the batched GEMM over device-resident size, leading-
  * dimension and pointer arrays; alpha and beta point to one host scalar of the
@@ -154,6 +175,22 @@ int ddla_s_gemm_vbatched2s(DDLA_GEMM_VBATCHED2S_ARGS);
 int ddla_d_gemm_vbatched2s(DDLA_GEMM_VBATCHED2S_ARGS);
 int ddla_c_gemm_vbatched2s(DDLA_GEMM_VBATCHED2S_ARGS);
 int ddla_z_gemm_vbatched2s(DDLA_GEMM_VBATCHED2S_ARGS);
+/* The mixed gemmVbatched2s overloads (reference include/ddla/ddla.h:1893-2030,
+ * C++ only there), named by the element types of (A0, B0, C0, AB1): r real,
+ * z complex; C1 is complex.  alpha_0 / beta_0 point to a scalar of C0's type,
+ * alpha_1 / beta_1 to a complex one.  Arguments as ddla_?_gemm_vbatched2s. */
+int ddla_c_gemm_vbatched2s_rzzr(DDLA_GEMM_VBATCHED2S_ARGS);
+int ddla_c_gemm_vbatched2s_zrzr(DDLA_GEMM_VBATCHED2S_ARGS);
+int ddla_c_gemm_vbatched2s_rzzz(DDLA_GEMM_VBATCHED2S_ARGS);
+int ddla_c_gemm_vbatched2s_zrzz(DDLA_GEMM_VBATCHED2S_ARGS);
+int ddla_c_gemm_vbatched2s_zzzr(DDLA_GEMM_VBATCHED2S_ARGS);
+int ddla_c_gemm_vbatched2s_rrrz(DDLA_GEMM_VBATCHED2S_ARGS);
+int ddla_z_gemm_vbatched2s_rzzr(DDLA_GEMM_VBATCHED2S_ARGS);
+int ddla_z_gemm_vbatched2s_zrzr(DDLA_GEMM_VBATCHED2S_ARGS);
+int ddla_z_gemm_vbatched2s_rzzz(DDLA_GEMM_VBATCHED2S_ARGS);
+int ddla_z_gemm_vbatched2s_zrzz(DDLA_GEMM_VBATCHED2S_ARGS);
+int ddla_z_gemm_vbatched2s_zzzr(DDLA_GEMM_VBATCHED2S_ARGS);
+int ddla_z_gemm_vbatched2s_rrrz(DDLA_GEMM_VBATCHED2S_ARGS);
 
 /* The reference's internal check / size / run split of ppotrf and ppotrs
  * (src/Cholesky/cholesky_workspace.h:133-154, 207-222) exported so a caller can
@@ -185,8 +222,10 @@ int ddla_z_ppotrs_workspace_size(void* handle, char side, int n, int nrhs, const
  * the library until the process exits).  Same arguments, checks and result as
  * ddla_d_ppotrs, limited to n <= 65536 and nrhs <= 256 (larger sizes return
  * status 6 with a message, before any device work).  The first call on a device
- * looks the array up, so make it before any stream capture; calls that overlap
- * on the GPU share the array and race. */
+ * looks the array up, so make it before any stream capture; the address is
+ * kept for the life of the process, so the device's context must not be reset
+ * (cudaDeviceReset) between calls.  Calls that overlap on the GPU share the
+ * array and race. */
 int ddla_d_ppotrs_noalloc(void* handle, char side, char uplo, char trans, int n, int nrhs, const void* A,
                           const int* descA, void* B, const int* descB);
 

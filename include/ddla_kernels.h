@@ -26,6 +26,16 @@ extern "C" {
  * and then to the order of the first non-positive-definite leading minor. */
 int ddlak_potrf(char type, char uplo, int n, void* A, long long lda, int* dinfo, void* stream);
 
+/* The factorization runs in super-steps of `group` block columns (128 wide; 64
+ * for complex double): the diagonal blocks and panels of a super-step are
+ * factored on a high-priority look-ahead stream, and the rest of the trailing
+ * matrix is updated once per super-step with K = group * block width.
+ * ddlak_potrf uses DDLAK_POTRF_GROUP; ddlak_potrf_grouped takes 1 ..
+ * DDLAK_POTRF_MAX_GROUP (same results up to rounding). */
+#define DDLAK_POTRF_GROUP 2
+#define DDLAK_POTRF_MAX_GROUP 8
+int ddlak_potrf_grouped(char type, char uplo, int group, int n, void* A, long long lda, int* dinfo, void* stream);
+
 /* In place A <- J A J on the leading n x n (element (i, j) trades places with
  * (n-1-i, n-1-j); J the order-reversing permutation).  With it the bottom-right
  * factorization of src/Cholesky/potrf_bottom_right.cpp:208-256 (A = U U^H or
@@ -56,6 +66,45 @@ int ddlak_gemm_vbatched_check(char transA, char transB, const int* d_m, const in
 int ddlak_gemm_vbatched(char type, char transA, char transB, int max_m, int max_n, const int* d_m, const int* d_n,
                         const int* d_k, const void* alpha, const void* d_A, const int* d_lda, const void* d_B,
                         const int* d_ldb, const void* beta, void* d_C, const int* d_ldc, int batch, void* stream);
+
+/* The mixed form of ddlak_gemm_vbatched: type 'c' or 'z' is the output's
+ * type; complex_left = 1: A complex and B real, 0: A real and B complex ('C' on
+ * the real operand is 'T').  alpha and beta are complex host scalars. */
+int ddlak_gemm_vbatched_mixed(char type, int complex_left, char transA, char transB, int max_m, int max_n,
+                              const int* d_m, const int* d_n, const int* d_k, const void* alpha, const void* d_A,
+                              const int* d_lda, const void* d_B, const int* d_ldb, const void* beta, void* d_C,
+                              const int* d_ldc, int batch, void* stream);
+
+/* Zeroes *d_bad, then sets it to 1 + the index of an entry with m, n > 0 whose
+ * product (alpha != 0 and k != 0) needs a null A or B, or whose C is null while
+ * it must be written (a product, or beta != 1); the reference's
+ * mixed_vbatched_pointer_check (src/BLAS/gemm_mixed.cpp:224-234). */
+int ddlak_gemm_vbatched_pointers(const int* d_m, const int* d_n, const int* d_k, const void* const* d_A,
+                                 const void* const* d_B, void* const* d_C, int alpha_zero, int beta_one, int batch,
+                                 int* d_bad, void* stream);
+
+/* Zeroes *d_bad, then sets it to 1 + the index of an entry (m1, n1, k1 > 0)
+ * whose C0 operand in stage 1 of a two-stage GEMM -- rows x cols of op(X) read
+ * with leading dimension ld1, X on the left when left != 0, transposed when
+ * trans != 0 -- is not the m0 x n0 matrix with leading dimension ldc0 that
+ * stage 0 writes (the reference's mixed_vbatched_stage_check,
+ * src/BLAS/gemm_mixed.cpp:236-245). */
+int ddlak_gemm_vbatched_footprint(const int* d_m0, const int* d_n0, const int* d_ldc0, const int* d_m1,
+                                  const int* d_n1, const int* d_k1, const int* d_ld1, int left, int trans, int batch,
+                                  int* d_bad, void* stream);
+
+/* Hermitian completion of the leading n x n (the reference's herm_complete):
+ * the triangle opposite uplo becomes the conjugate transpose of the uplo one and
+ * the diagonal's imaginary part is zeroed.  type 's' 'd' 'c' 'z'. */
+int ddlak_herm_complete(char type, char uplo, int n, void* A, long long lda, void* stream);
+
+/* The forward half of ddlak_potrs: B <- L^-1 B (side 'L', B n x nrhs) or
+ * B <- B L^-H (side 'R', B nrhs x n), the factor read through its L view
+ * (uplo 'L': A's lower triangle; 'U': L = U^H).  Scratch and status word as for
+ * ddlak_potrs (ddlak_potrs_workspace(n, nrhs) bytes).  Replaces the two
+ * blas_impl::trsm_run calls of phegst (src/Eigensolver/phegst.cpp:145-152). */
+int ddlak_forward_solve(char type, char uplo, char side, int n, int nrhs, const void* A, long long lda, void* B,
+                        long long ldb, void* work, unsigned long long work_bytes, void* stream);
 
 /* Bytes of device scratch ddlak_potrs needs for (n, nrhs). */
 unsigned long long ddlak_potrs_workspace(int n, int nrhs);
@@ -91,7 +140,15 @@ int ddlak_diag_logsum(char type, int n, const void* A, long long lda, void* work
 
 /* ---- mixed precision (ddla::pposv_mixed; no reference counterpart) ------ */
 
-/* Bytes of one K-contiguous panel operand copy for an order-n factorization. */
+/* Super-steps of the mixed factorization: block columns of 128 factored on the
+ * look-ahead chain before one K = 128 * group trailing update of the rest
+ * (ddlak_potrf_mixed uses DDLAK_MIXED_GROUP; ddlak_potrf_mixed_grouped takes
+ * 1 .. DDLAK_MIXED_MAX_GROUP). */
+#define DDLAK_MIXED_GROUP 2
+#define DDLAK_MIXED_MAX_GROUP 4
+
+/* Bytes of one of the two panel-operand slots of an order-n factorization
+ * (enough for any group up to DDLAK_MIXED_MAX_GROUP). */
 unsigned long long ddlak_mixed_panel_bytes(int n);
 
 /* W = fl32(A) on the lower triangle (diagonal times diag_scale, a relative
@@ -108,6 +165,10 @@ int ddlak_convert_lower(int n, const void* A, long long lda, void* W, long long 
  * update writes whole 128 x 128 tiles); ldw must be a multiple of 4. */
 int ddlak_potrf_mixed(char precision, int n, void* W, long long ldw, void* P0, void* P1, int* dinfo, int* status,
                       void* stream);
+/* The same with an explicit super-step group (1 .. DDLAK_MIXED_MAX_GROUP): the
+ * trailing matrix is read and written once per `group` block columns. */
+int ddlak_potrf_mixed_grouped(char precision, int group, int n, void* W, long long ldw, void* P0, void* P1,
+                              int* dinfo, int* status, void* stream);
 
 /* Inverses (FP64) of the 64 x 64 diagonal blocks of an FP32 factor (lower):
  * ddlak_inv_diag_bytes(n) bytes, one column-major block per block row. */

@@ -152,6 +152,64 @@ int gemm_vbatched_impl(void* handle, char ta, char tb, int* d_m, int* d_n, int* 
     });
 }
 
+template <class R, bool ComplexLeft>
+int gemm_vbatched_mixed_impl(void* handle, char ta, char tb, int* d_m, int* d_n, int* d_k, const void* alpha,
+                             const void* const* d_A, int* d_lda, const void* const* d_B, int* d_ldb,
+                             const void* beta, void** d_C, int* d_ldc, int batch_count)
+{
+    using Z = std::complex<R>;
+    return run(handle, [&](ddla::DdlaHandle_t h) -> int {
+        if (alpha == nullptr || beta == nullptr) return ST_INVALID_VALUE;
+        Z al, be;
+        std::memcpy(&al, alpha, sizeof(Z));
+        std::memcpy(&be, beta, sizeof(Z));
+        if constexpr (ComplexLeft)
+            ddla::gemmVbatched<R>(h, ta, tb, d_m, d_n, d_k, al, reinterpret_cast<const Z* const*>(d_A), d_lda,
+                                  reinterpret_cast<const R* const*>(d_B), d_ldb, be, reinterpret_cast<Z**>(d_C), d_ldc,
+                                  batch_count);
+        else
+            ddla::gemmVbatched<R>(h, ta, tb, d_m, d_n, d_k, al, reinterpret_cast<const R* const*>(d_A), d_lda,
+                                  reinterpret_cast<const Z* const*>(d_B), d_ldb, be, reinterpret_cast<Z**>(d_C), d_ldc,
+                                  batch_count);
+        return ST_SUCCESS;
+    });
+}
+
+template <class R, class TA, class TB, class T0, class TX>
+int gemm_vbatched2s_mixed_impl(void* handle, char ta0, char tb0, int* m0, int* n0, int* k0, const void* alpha0,
+                               const void* const* A0, int* lda0, const void* const* B0, int* ldb0, const void* beta0,
+                               void** C0, int* ldc0, char ta1, char tb1, int* m1, int* n1, int* k1,
+                               const void* alpha1, const void* const* AB1, int* lda1, int* ldb1, const void* beta1,
+                               void** C1, int* ldc1, int c0_left, int batch_count, const int* segment_sizes,
+                               int segment_count)
+{
+    using Z = std::complex<R>;
+    return run(handle, [&](ddla::DdlaHandle_t h) -> int {
+        if (!alpha0 || !beta0 || !alpha1 || !beta1) return ST_INVALID_VALUE;
+        T0 a0, b0;
+        Z a1, b1;
+        std::memcpy(&a0, alpha0, sizeof(T0));
+        std::memcpy(&b0, beta0, sizeof(T0));
+        std::memcpy(&a1, alpha1, sizeof(Z));
+        std::memcpy(&b1, beta1, sizeof(Z));
+        ddla::gemmVbatched2s<R>(h, ta0, tb0, m0, n0, k0, a0, reinterpret_cast<const TA* const*>(A0), lda0,
+                                reinterpret_cast<const TB* const*>(B0), ldb0, b0, reinterpret_cast<T0**>(C0), ldc0,
+                                ta1, tb1, m1, n1, k1, a1, reinterpret_cast<const TX* const*>(AB1), lda1, ldb1, b1,
+                                reinterpret_cast<Z**>(C1), ldc1, c0_left != 0, batch_count, segment_sizes,
+                                segment_count);
+        return ST_SUCCESS;
+    });
+}
+
+template <class T>
+int phegst_impl(void* handle, char uplo, int n, void* A, const int* descA, const void* F, const int* descF)
+{
+    return run(handle, [&](ddla::DdlaHandle_t h) -> int {
+        ddla::phegst<T>(h, uplo, n, static_cast<T*>(A), descA, static_cast<const T*>(F), descF);
+        return ST_SUCCESS;
+    });
+}
+
 template <class T>
 int gemm_vbatched2s_impl(void* handle, char ta0, char tb0, int* m0, int* n0, int* k0, const void* alpha0,
                          const void* const* A0, int* lda0, const void* const* B0, int* ldb0, const void* beta0,
@@ -446,6 +504,11 @@ int ddla_c_bcast_dims(int, int* m, int* n, int* type_char, int root)
         return gemm_vbatched_impl<T>(handle, ta, tb, d_m, d_n, d_k, alpha, d_A, d_lda, d_B, d_ldb, beta, d_C, d_ldc, \
                                      batch_count);                                                                   \
     }                                                                                                                \
+    int ddla_##P##_phegst(void* handle, char uplo, int n, void* A, const int* descA, const void* F,                \
+                          const int* descF)                                                                          \
+    {                                                                                                                \
+        return phegst_impl<T>(handle, uplo, n, A, descA, F, descF);                                                  \
+    }                                                                                                                \
     int ddla_##P##_gemm_vbatched2s(DDLA_GEMM_VBATCHED2S_ARGS)                                                      \
     {                                                                                                                \
         return gemm_vbatched2s_impl<T>(handle, transA_0, transB_0, d_m_0, d_n_0, d_k_0, alpha_0, d_A_0, d_lda_0,    \
@@ -473,6 +536,45 @@ DDLA_C_TYPED(d, double)
 DDLA_C_TYPED(c, std::complex<float>)
 DDLA_C_TYPED(z, std::complex<double>)
 #undef DDLA_C_TYPED
+
+#define DDLA_GVM_C(P, R)                                                                                          \
+    int ddla_##P##_gemm_vbatched_rc(void* handle, char ta, char tb, int* m, int* n, int* k, const void* alpha,      \
+                                    const void* const* A, int* lda, const void* const* B, int* ldb,                \
+                                    const void* beta, void** C, int* ldc, int batch_count)                         \
+    {                                                                                                              \
+        return gemm_vbatched_mixed_impl<R, false>(handle, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,    \
+                                                  batch_count);                                                    \
+    }                                                                                                              \
+    int ddla_##P##_gemm_vbatched_cr(void* handle, char ta, char tb, int* m, int* n, int* k, const void* alpha,      \
+                                    const void* const* A, int* lda, const void* const* B, int* ldb,                \
+                                    const void* beta, void** C, int* ldc, int batch_count)                         \
+    {                                                                                                              \
+        return gemm_vbatched_mixed_impl<R, true>(handle, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,     \
+                                                 batch_count);                                                     \
+    }
+DDLA_GVM_C(c, float)
+DDLA_GVM_C(z, double)
+#undef DDLA_GVM_C
+
+#define DDLA_GV2M_C(P, R, CODE, TA, TB, T0, TX)                                                               \
+    int ddla_##P##_gemm_vbatched2s_##CODE(DDLA_GEMM_VBATCHED2S_ARGS)                                             \
+    {                                                                                                            \
+        return gemm_vbatched2s_mixed_impl<R, TA, TB, T0, TX>(                                                    \
+            handle, transA_0, transB_0, d_m_0, d_n_0, d_k_0, alpha_0, d_A_0, d_lda_0, d_B_0, d_ldb_0, beta_0,    \
+            d_C_0, d_ldc_0, transA_1, transB_1, d_m_1, d_n_1, d_k_1, alpha_1, d_AB_1, d_lda_1, d_ldb_1, beta_1,  \
+            d_C_1, d_ldc_1, c0_left, batch_count, segment_sizes, segment_count);                                 \
+    }
+#define DDLA_GV2M_C_ALL(P, R)                                                                                    \
+    DDLA_GV2M_C(P, R, rzzr, R, std::complex<R>, std::complex<R>, R)                                              \
+    DDLA_GV2M_C(P, R, zrzr, std::complex<R>, R, std::complex<R>, R)                                              \
+    DDLA_GV2M_C(P, R, rzzz, R, std::complex<R>, std::complex<R>, std::complex<R>)                                \
+    DDLA_GV2M_C(P, R, zrzz, std::complex<R>, R, std::complex<R>, std::complex<R>)                                \
+    DDLA_GV2M_C(P, R, zzzr, std::complex<R>, std::complex<R>, std::complex<R>, R)                                \
+    DDLA_GV2M_C(P, R, rrrz, R, R, R, std::complex<R>)
+DDLA_GV2M_C_ALL(c, float)
+DDLA_GV2M_C_ALL(z, double)
+#undef DDLA_GV2M_C_ALL
+#undef DDLA_GV2M_C
 
 int ddla_d_ppotrs_noalloc(void* handle, char side, char uplo, char trans, int n, int nrhs, const void* A,
                           const int* descA, void* B, const int* descB)

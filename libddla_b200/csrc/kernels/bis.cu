@@ -681,14 +681,16 @@ cudaError_t bis_chain_solve(int n, int nrhs, const float* L, long long ldl, cons
         !tc::encode_colmajor_2d(&mapD, dt, (int)sizeof(T), Dinv, BS, (long long)lay.S * BS, BS, CT, chunk_cols<T>(),
                                 CU_TENSOR_MAP_SWIZZLE_NONE))
         return cudaErrorInvalidValue;
-    static int grid = [&] {
-        cudaFuncSetAttribute(k_bis_chain<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaError_t e = smem_optin(k_bis_chain<T>, smem); e != cudaSuccess) return e;
+    // every CTA of the queue resident at once: SMs of this device x CTAs per SM
+    int grid = 0;
+    {
         int dev = 0, sms = 148, per = 1;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bis_chain<T>, CH_NT, smem);
-        return sms * (per > 0 ? per : 1);
-    }();
+        grid = sms * (per > 0 ? per : 1);
+    }
     const unsigned g = (unsigned)std::min<long long>(grid, c.total);
     const unsigned gv = (unsigned)std::min<long long>(ceil_div((long long)n * CQ, 256), 1184);
     int launches = 0;

@@ -47,6 +47,15 @@ __device__ __forceinline__ bool is_one(double a) { return a == 1.0; }
 __device__ __forceinline__ bool is_one(cf32 a) { return a.x == 1.f && a.y == 0.f; }
 __device__ __forceinline__ bool is_one(cf64 a) { return a.x == 1.0 && a.y == 0.0; }
 
+// element of a real or complex operand, as the output type (a real value
+// widened to complex has no imaginary part, so 'C' on it is 'T')
+template <class T, class E>
+__device__ __forceinline__ T widen_to(E x)
+{
+    if constexpr (Traits<T>::cplx && !Traits<E>::cplx) return from_real<T>(x);
+    else return x;
+}
+
 // op 0 'N', 1 'T', 2 'C'
 template <class T, int OP>
 __device__ __forceinline__ T opv(T v)
@@ -81,11 +90,11 @@ __global__ void __launch_bounds__(256) k_gemm_vbatched_check(int ta, int tb, con
     atomicMax(summary + 2, k);
 }
 
-template <class T, int TA, int TB>
+template <class T, int TA, int TB, class EA = T, class EB = T>
 __global__ void __launch_bounds__(GB_NT) k_gemm_vbatched(const int* __restrict__ M, const int* __restrict__ N,
                                                          const int* __restrict__ K, T alpha,
-                                                         const T* const* __restrict__ A, const int* __restrict__ LDA,
-                                                         const T* const* __restrict__ B, const int* __restrict__ LDB,
+                                                         const EA* const* __restrict__ A, const int* __restrict__ LDA,
+                                                         const EB* const* __restrict__ B, const int* __restrict__ LDB,
                                                          T beta, T* const* __restrict__ C,
                                                          const int* __restrict__ LDC, int batch0)
 {
@@ -110,8 +119,8 @@ __global__ void __launch_bounds__(GB_NT) k_gemm_vbatched(const int* __restrict__
         }
         return;
     }
-    const T* a = A[b];
-    const T* bm = B[b];
+    const EA* a = A[b];
+    const EB* bm = B[b];
     if (a == nullptr || bm == nullptr || c == nullptr) return;
     const long long lda = LDA[b], ldb = LDB[b];
     T acc[4][4];
@@ -127,7 +136,7 @@ __global__ void __launch_bounds__(GB_NT) k_gemm_vbatched(const int* __restrict__
             const int ii = TA == 0 ? idx % GB_M : idx / GB_K, kk = TA == 0 ? idx / GB_M : idx % GB_K;
             const int gi = i0 + ii, gk = k0 + kk;
             T v = zero<T>();
-            if (gi < m && gk < k) v = opv<T, TA>(TA == 0 ? a[gi + gk * lda] : a[gk + gi * lda]);
+            if (gi < m && gk < k) v = opv<T, TA>(widen_to<T>(TA == 0 ? a[gi + gk * lda] : a[gk + gi * lda]));
             sA[kk][ii] = v;
         }
         // op(B)(l, j): 'N' B[l + j ldb], else B[j + l ldb] (conjugated for 'C')
@@ -137,7 +146,7 @@ __global__ void __launch_bounds__(GB_NT) k_gemm_vbatched(const int* __restrict__
             const int kk = TB == 0 ? idx % GB_K : idx / GB_N, jj = TB == 0 ? idx / GB_K : idx % GB_N;
             const int gk = k0 + kk, gj = j0 + jj;
             T v = zero<T>();
-            if (gk < k && gj < n) v = opv<T, TB>(TB == 0 ? bm[gk + gj * ldb] : bm[gj + gk * ldb]);
+            if (gk < k && gj < n) v = opv<T, TB>(widen_to<T>(TB == 0 ? bm[gk + gj * ldb] : bm[gj + gk * ldb]));
             sB[kk][jj] = v;
         }
         __syncthreads();
@@ -179,7 +188,7 @@ int op_code(char t)
     return -1;
 }
 
-template <class T, int TA, int TB>
+template <class T, int TA, int TB, class EA = T, class EB = T>
 cudaError_t launch_t(int max_m, int max_n, const int* M, const int* N, const int* K, T alpha, const void* A,
                      const int* LDA, const void* B, const int* LDB, T beta, void* C, const int* LDC, int batch,
                      cudaStream_t st)
@@ -189,8 +198,8 @@ cudaError_t launch_t(int max_m, int max_n, const int* M, const int* N, const int
     int launches = 0;
     for (int b0 = 0; b0 < batch; b0 += 65535) {
         const int nb = batch - b0 < 65535 ? batch - b0 : 65535;
-        k_gemm_vbatched<T, TA, TB><<<dim3(grid0.x, grid0.y, (unsigned)nb), GB_NT, 0, st>>>(
-            M, N, K, alpha, static_cast<const T* const*>(A), LDA, static_cast<const T* const*>(B), LDB, beta,
+        k_gemm_vbatched<T, TA, TB, EA, EB><<<dim3(grid0.x, grid0.y, (unsigned)nb), GB_NT, 0, st>>>(
+            M, N, K, alpha, static_cast<const EA* const*>(A), LDA, static_cast<const EB* const*>(B), LDB, beta,
             static_cast<T* const*>(C), LDC, b0);
         ++launches;
     }
@@ -214,8 +223,110 @@ cudaError_t launch_typed(int ta, int tb, int max_m, int max_n, const int* M, con
     return cudaErrorInvalidValue;
 }
 
+// one operand real (R), the other complex (T = complex<R>); 'C' on the real one is 'T'
+template <class T, class EA, class EB>
+cudaError_t launch_mixed(int ta, int tb, int max_m, int max_n, const int* M, const int* N, const int* K,
+                         const void* alpha, const void* A, const int* LDA, const void* B, const int* LDB,
+                         const void* beta, void* C, const int* LDC, int batch, cudaStream_t st)
+{
+    const T al = *static_cast<const T*>(alpha), be = *static_cast<const T*>(beta);
+#define DDLAK_GVM(TA_, TB_)                                                                                    \
+    if (ta == TA_ && tb == TB_)                                                                                \
+        return launch_t<T, TA_, TB_, EA, EB>(max_m, max_n, M, N, K, al, A, LDA, B, LDB, be, C, LDC, batch, st);
+    DDLAK_GVM(0, 0) DDLAK_GVM(0, 1) DDLAK_GVM(0, 2)
+    DDLAK_GVM(1, 0) DDLAK_GVM(1, 1) DDLAK_GVM(1, 2)
+    DDLAK_GVM(2, 0) DDLAK_GVM(2, 1) DDLAK_GVM(2, 2)
+#undef DDLAK_GVM
+    return cudaErrorInvalidValue;
+}
+
+// first entry whose product or scaling needs a matrix that is null (the reference's
+// mixed_vbatched_pointer_check, src/BLAS/gemm_mixed.cpp:224-234): bad = 1 + its index
+__global__ void __launch_bounds__(256) k_gemm_vbatched_pointers(const int* __restrict__ M, const int* __restrict__ N,
+                                                                const int* __restrict__ K,
+                                                                const void* const* __restrict__ A,
+                                                                const void* const* __restrict__ B,
+                                                                void* const* __restrict__ C, int alpha_zero,
+                                                                int beta_one, int batch, int* __restrict__ bad)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= batch || M[q] == 0 || N[q] == 0) return;
+    const bool product = !alpha_zero && K[q] != 0;
+    if (!product && beta_one) return;
+    if (!C[q] || (product && (!A[q] || !B[q]))) atomicCAS(bad, 0, q + 1);
+}
+
+// the C0 operand of stage 1 must be C0 as stage 0 writes it (the reference's
+// mixed_vbatched_stage_check, src/BLAS/gemm_mixed.cpp:236-245): bad = 1 + index
+__global__ void __launch_bounds__(256) k_gemm_vbatched_footprint(const int* __restrict__ M0, const int* __restrict__ N0,
+                                                                 const int* __restrict__ LDC0,
+                                                                 const int* __restrict__ M1, const int* __restrict__ N1,
+                                                                 const int* __restrict__ K1,
+                                                                 const int* __restrict__ LD1, int left, int trans,
+                                                                 int batch, int* __restrict__ bad)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= batch || M1[q] == 0 || N1[q] == 0 || K1[q] == 0) return;
+    const int rows = left ? (trans ? K1[q] : M1[q]) : (trans ? N1[q] : K1[q]);
+    const int cols = left ? (trans ? M1[q] : K1[q]) : (trans ? K1[q] : N1[q]);
+    if (rows != M0[q] || cols != N0[q] || LD1[q] != LDC0[q]) atomicCAS(bad, 0, q + 1);
+}
+
 }  // namespace
 }  // namespace ddlak
+
+extern "C" int ddlak_gemm_vbatched_footprint(const int* d_m0, const int* d_n0, const int* d_ldc0, const int* d_m1,
+                                             const int* d_n1, const int* d_k1, const int* d_ld1, int left, int trans,
+                                             int batch, int* d_bad, void* stream)
+{
+    using namespace ddlak;
+    if (batch < 0 || !d_bad) return (int)cudaErrorInvalidValue;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(d_bad, 0, sizeof(int), st);
+    if (e != cudaSuccess || batch == 0) return (int)e;
+    k_gemm_vbatched_footprint<<<(unsigned)ceil_div(batch, 256), 256, 0, st>>>(d_m0, d_n0, d_ldc0, d_m1, d_n1, d_k1,
+                                                                              d_ld1, left, trans, batch, d_bad);
+    note_launches(1);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int ddlak_gemm_vbatched_pointers(const int* d_m, const int* d_n, const int* d_k, const void* const* d_A,
+                                            const void* const* d_B, void* const* d_C, int alpha_zero, int beta_one,
+                                            int batch, int* d_bad, void* stream)
+{
+    using namespace ddlak;
+    if (batch < 0 || !d_bad) return (int)cudaErrorInvalidValue;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(d_bad, 0, sizeof(int), st);
+    if (e != cudaSuccess || batch == 0) return (int)e;
+    k_gemm_vbatched_pointers<<<(unsigned)ceil_div(batch, 256), 256, 0, st>>>(d_m, d_n, d_k, d_A, d_B, d_C, alpha_zero,
+                                                                             beta_one, batch, d_bad);
+    note_launches(1);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int ddlak_gemm_vbatched_mixed(char type, int complex_left, char transA, char transB, int max_m, int max_n,
+                                         const int* d_m, const int* d_n, const int* d_k, const void* alpha,
+                                         const void* d_A, const int* d_lda, const void* d_B, const int* d_ldb,
+                                         const void* beta, void* d_C, const int* d_ldc, int batch, void* stream)
+{
+    using namespace ddlak;
+    const int ta = op_code(transA), tb = op_code(transB);
+    if (ta < 0 || tb < 0 || batch < 0 || !alpha || !beta) return (int)cudaErrorInvalidValue;
+    if (batch == 0 || max_m <= 0 || max_n <= 0) return 0;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (type == 'c')
+        return (int)(complex_left ? launch_mixed<cf32, cf32, float>(ta, tb, max_m, max_n, d_m, d_n, d_k, alpha, d_A,
+                                                                     d_lda, d_B, d_ldb, beta, d_C, d_ldc, batch, st)
+                                  : launch_mixed<cf32, float, cf32>(ta, tb, max_m, max_n, d_m, d_n, d_k, alpha, d_A,
+                                                                     d_lda, d_B, d_ldb, beta, d_C, d_ldc, batch, st));
+    if (type == 'z')
+        return (int)(complex_left ? launch_mixed<cf64, cf64, double>(ta, tb, max_m, max_n, d_m, d_n, d_k, alpha, d_A,
+                                                                      d_lda, d_B, d_ldb, beta, d_C, d_ldc, batch, st)
+                                  : launch_mixed<cf64, double, cf64>(ta, tb, max_m, max_n, d_m, d_n, d_k, alpha, d_A,
+                                                                      d_lda, d_B, d_ldb, beta, d_C, d_ldc, batch, st));
+    return (int)cudaErrorInvalidValue;
+}
 
 extern "C" int ddlak_gemm_vbatched_check(char transA, char transB, const int* d_m, const int* d_n, const int* d_k,
                                          const int* d_lda, const int* d_ldb, const int* d_ldc, int batch,

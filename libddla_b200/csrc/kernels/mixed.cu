@@ -18,6 +18,8 @@
 #include <mutex>
 #include <type_traits>
 
+#include <ddla_kernels.h>
+
 #include "common.cuh"
 #include "ddla_kernels_internal.h"
 #include "diag_factor.cuh"
@@ -820,10 +822,7 @@ cudaError_t mixed_update(float* W, long long ldw, int n, long long t0, long long
 {
     const long long m = (long long)n - t0;
     if (m <= 0) return cudaSuccess;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        cudaFuncSetAttribute(k_mixed_update<TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MU_SMEM);
-    });
+    if (cudaError_t e = smem_optin(k_mixed_update<TF32>, MU_SMEM); e != cudaSuccess) return e;
     CUtensorMap map;
     if (!encode_panel_map(&map, P, (long long)n - pr0, nbk, TF32)) return cudaErrorInvalidValue;
     CUtensorMap wmap;
@@ -840,35 +839,49 @@ cudaError_t mixed_update(float* W, long long ldw, int n, long long t0, long long
     return cudaGetLastError();
 }
 
+// Right-looking factorization in super-steps of G block columns (K = 128 G):
+// within a super-step the chain on the high-priority stream factors its
+// blocks one after the other (block g first takes the update from blocks
+// 0..g-1 of the super-step, left-looking, K = 128 g), then packs the G
+// finished panels into one K = 128 G operand, updates the next super-step's
+// G block columns with it (look-ahead), and hands it to the caller's stream,
+// which updates everything to the right of those in one pass.  The FP32
+// trailing matrix is therefore read and written once per super-step instead
+// of once per block column: G = 2 halves that traffic.  Per super-step the
+// caller's stream waits for the packed panel, the chain waits for the previous
+// super-step's trailing update before its look-ahead update, and the two
+// touch disjoint tiles.
+// P0 / P1: two slots of ddlak_mixed_panel_bytes(n) bytes; a slot holds the
+// packed super-step panel (n x 128 G) and the left-looking operand (n x 128 (G-1)).
 template <bool TF32>
-cudaError_t potrf_mixed_enqueue(float* W, long long ldw, int n, void* P0, void* P1, int* dinfo, int* status,
+cudaError_t potrf_mixed_enqueue(float* W, long long ldw, int n, int G, void* P0, void* P1, int* dinfo, int* status,
                                 cudaStream_t st)
 {
     constexpr int NB = MX_NB;
     const size_t diag_smem = (size_t)NB * (NB + 1) * sizeof(double);
-    static std::once_flag once;
-    std::call_once(once, [&] {
-        cudaFuncSetAttribute(k_potrf_diag_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem);
-    });
+    if (cudaError_t e = smem_optin(k_potrf_diag_mixed, diag_smem); e != cudaSuccess) return e;
     MixedStreams& L = mixed_streams();
     cudaStream_t hi = L.hi;
     void* P[2] = {P0, P1};
+    const long long SW = (long long)G * NB;  // super-step width
 
-    auto diag_panel_pack = [&](int k0, int slot, cudaStream_t s) -> cudaError_t {
+    auto diag_trsm = [&](int k0, cudaStream_t s) -> cudaError_t {
         const int nbk = n - k0 < NB ? n - k0 : NB;
         {
             ProfScope ps(PK_MIXED_OTHER, s, (double)nbk * nbk * nbk / 3.0, 4.0 * nbk * (nbk + 1));
             k_potrf_diag_mixed<<<1, 256, (size_t)nbk * (nbk + 1) * sizeof(double), s>>>(W, ldw, k0, nbk, dinfo);
         }
         note_launches(1);
-        const long long m = (long long)n - k0 - nbk;
-        if (m <= 0) return cudaGetLastError();
-        cudaError_t e = launch_trsm_panel<float, false>(W, ldw, k0, nbk, n, dinfo, s);
-        if (e != cudaSuccess) return e;
-        dim3 grid((unsigned)ceil_div(m, 32), nbk / 32);
+        if ((long long)n - k0 - nbk <= 0) return cudaGetLastError();
+        return launch_trsm_panel<float, false>(W, ldw, k0, nbk, n, dinfo, s);
+    };
+    // rows [pr0, n) x columns [k0, k0 + kw) of W -> K-contiguous operand at Pbuf
+    auto pack = [&](long long pr0, int k0, int kw, void* Pbuf, cudaStream_t s) -> cudaError_t {
+        const long long m = (long long)n - pr0;
+        dim3 grid((unsigned)ceil_div(m, 32), kw / 32);
         {
-            ProfScope ps(PK_MIXED_OTHER, s, 0.0, (double)m * nbk * (4.0 + (TF32 ? 4.0 : 2.0)));
-            k_pack_panel<TF32><<<grid, dim3(32, 8), 0, s>>>(W, ldw, n, (long long)k0 + nbk, k0, nbk, P[slot], dinfo);
+            ProfScope ps(PK_MIXED_OTHER, s, 0.0, (double)m * kw * (4.0 + (TF32 ? 4.0 : 2.0)));
+            k_pack_panel<TF32><<<grid, dim3(32, 8), 0, s>>>(W, ldw, n, pr0, k0, kw, Pbuf, dinfo);
         }
         note_launches(1);
         return cudaGetLastError();
@@ -876,36 +889,53 @@ cudaError_t potrf_mixed_enqueue(float* W, long long ldw, int n, void* P0, void* 
 
     cudaEventRecord(L.start, st);
     cudaStreamWaitEvent(hi, L.start, 0);
-    cudaError_t e = diag_panel_pack(0, 0, hi);
-    if (e != cudaSuccess) return e;
-    cudaEventRecord(L.panel, hi);
-    bool have_rest = false;
+    bool have_rest = false, have_panel = false;
     int step = 0;
-    for (int k0 = 0; k0 + NB < n; k0 += NB, ++step) {
-        const long long t0 = (long long)k0 + NB;
-        const long long m = (long long)n - t0;
-        const int slot = step & 1;
-        cudaStreamWaitEvent(st, L.panel, 0);
-        if (m > NB) {
-            e = mixed_update<TF32>(W, ldw, n, t0 + NB, t0, 0, P[slot], NB, dinfo, status, st);
-            if (e != cudaSuccess) return e;
+    cudaError_t e = cudaSuccess;
+    for (long long k0 = 0; k0 < n; k0 += SW, ++step) {
+        unsigned char* slot = static_cast<unsigned char*>(P[step & 1]);
+        void* Ppanel = slot;
+        void* Pleft = slot + ((size_t)n * SW * 4 + 255) / 256 * 256;
+        // the chain: the super-step's block columns, each after the left-looking
+        // update from the ones before it
+        for (int g = 0; g < G; ++g) {
+            const long long kg = k0 + (long long)g * NB;
+            if (kg >= n) break;
+            if (g > 0) {
+                if ((e = pack(kg, (int)k0, g * NB, Pleft, hi)) != cudaSuccess) return e;
+                const int cols = (long long)n - kg < NB ? (int)(n - kg) : NB;
+                if ((e = mixed_update<TF32>(W, ldw, n, kg, kg, cols, Pleft, g * NB, dinfo, status, hi)) !=
+                    cudaSuccess)
+                    return e;
+            }
+            if ((e = diag_trsm((int)kg, hi)) != cudaSuccess) return e;
         }
+        const long long t0 = k0 + SW;  // first row / column after the super-step
+        if (t0 >= n) break;
+        // all G panels are final: one K = 128 G operand for the updates to the right
+        if ((e = pack(t0, (int)k0, (int)SW, Ppanel, hi)) != cudaSuccess) return e;
+        cudaEventRecord(L.panel, hi);
+        have_panel = true;
+        // look-ahead: the next super-step's block columns, after the previous
+        // super-step's trailing update has reached them
         if (have_rest) cudaStreamWaitEvent(hi, L.rest, 0);
-        if (m > NB) {
+        const int la_cols = (long long)n - t0 < SW ? (int)(n - t0) : (int)SW;
+        if ((e = mixed_update<TF32>(W, ldw, n, t0, t0, la_cols, Ppanel, (int)SW, dinfo, status, hi)) != cudaSuccess)
+            return e;
+        // the rest of the trailing matrix on the caller's stream
+        have_rest = false;
+        if (t0 + SW < n) {
+            cudaStreamWaitEvent(st, L.panel, 0);
+            if ((e = mixed_update<TF32>(W, ldw, n, t0 + SW, t0, 0, Ppanel, (int)SW, dinfo, status, st)) !=
+                cudaSuccess)
+                return e;
             cudaEventRecord(L.rest, st);
             have_rest = true;
-        } else {
-            have_rest = false;
         }
-        const int cols = m < NB ? (int)m : NB;
-        e = mixed_update<TF32>(W, ldw, n, t0, t0, cols, P[slot], NB, dinfo, status, hi);
-        if (e != cudaSuccess) return e;
-        e = diag_panel_pack((int)t0, slot ^ 1, hi);
-        if (e != cudaSuccess) return e;
-        cudaEventRecord(L.panel, hi);
     }
+    (void)have_panel;
+    cudaEventRecord(L.panel, hi);
     cudaStreamWaitEvent(st, L.panel, 0);
-    if (have_rest) cudaStreamWaitEvent(st, L.rest, 0);
     return cudaGetLastError();
 }
 
@@ -914,8 +944,12 @@ cudaError_t potrf_mixed_enqueue(float* W, long long ldw, int n, void* P0, void* 
 
 extern "C" unsigned long long ddlak_mixed_panel_bytes(int n)
 {
-    // one K-contiguous panel copy: n rows x 128 columns of FP32 (the larger operand type)
-    return ((unsigned long long)(n > 0 ? n : 0) * ddlak::MX_NB * 4 + 255) / 256 * 256;
+    // one slot for super-steps of up to DDLAK_MIXED_MAX_GROUP block columns: the packed
+    // panel (n x 128 G) and the left-looking operand (n x 128 (G - 1)), FP32 (the larger
+    // operand type), each 256-byte aligned
+    const unsigned long long rows = (unsigned long long)(n > 0 ? n : 0);
+    const unsigned long long G = DDLAK_MIXED_MAX_GROUP;
+    return (rows * G * ddlak::MX_NB * 4 + 255) / 256 * 256 + (rows * (G - 1) * ddlak::MX_NB * 4 + 255) / 256 * 256;
 }
 
 extern "C" int ddlak_convert_lower(int n, const void* A, long long lda, void* W, long long ldw, double diag_scale,
@@ -939,8 +973,8 @@ extern "C" int ddlak_convert_lower(int n, const void* A, long long lda, void* W,
     return (int)cudaGetLastError();
 }
 
-extern "C" int ddlak_potrf_mixed(char precision, int n, void* W, long long ldw, void* P0, void* P1, int* dinfo,
-                                 int* status, void* stream)
+extern "C" int ddlak_potrf_mixed_grouped(char precision, int group, int n, void* W, long long ldw, void* P0,
+                                         void* P1, int* dinfo, int* status, void* stream)
 {
     using namespace ddlak;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -950,9 +984,16 @@ extern "C" int ddlak_potrf_mixed(char precision, int n, void* W, long long ldw, 
     if (n <= 0) return 0;
     if (ldw % 4 != 0) return (int)cudaErrorInvalidValue;  // keeps every W column 16-byte aligned
     float* w = static_cast<float*>(W);
-    if (precision == 'T') return (int)potrf_mixed_enqueue<true>(w, ldw, n, P0, P1, dinfo, status, st);
-    if (precision == 'B') return (int)potrf_mixed_enqueue<false>(w, ldw, n, P0, P1, dinfo, status, st);
+    if (group < 1 || group > DDLAK_MIXED_MAX_GROUP) return (int)cudaErrorInvalidValue;
+    if (precision == 'T') return (int)potrf_mixed_enqueue<true>(w, ldw, n, group, P0, P1, dinfo, status, st);
+    if (precision == 'B') return (int)potrf_mixed_enqueue<false>(w, ldw, n, group, P0, P1, dinfo, status, st);
     return (int)cudaErrorInvalidValue;
+}
+
+extern "C" int ddlak_potrf_mixed(char precision, int n, void* W, long long ldw, void* P0, void* P1, int* dinfo,
+                                 int* status, void* stream)
+{
+    return ddlak_potrf_mixed_grouped(precision, DDLAK_MIXED_GROUP, n, W, ldw, P0, P1, dinfo, status, stream);
 }
 
 extern "C" int ddlak_symm_residual(int n, int nrhs, const void* A, long long lda, const void* X, long long ldx,
@@ -973,10 +1014,7 @@ extern "C" int ddlak_symm_residual(int n, int nrhs, const void* A, long long lda
         if (encode_f64_map(&amap, static_cast<const double*>(A), n, n, lda, SRD_LD, SR) &&
             encode_f64_map(&xmap, static_cast<const double*>(X), n, nrhs, ldx, SRD_LD, 8)) {
             const size_t smem = symm_residual_dmma_smem();
-            static std::once_flag once_d;
-            std::call_once(once_d, [&] {
-                cudaFuncSetAttribute(k_symm_residual_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            });
+            if (cudaError_t e = smem_optin(k_symm_residual_dmma, smem); e != cudaSuccess) return (int)e;
             ProfScope ps(PK_SYMM_RESIDUAL, st, 2.0 * (double)n * n * nrhs, 4.0 * (double)n * (n + 1));
             k_symm_residual_dmma<<<dim3((unsigned)(N * chunks), 1), 256, smem, st>>>(
                 amap, xmap, n, nrhs, static_cast<const double*>(X), ldx, static_cast<double*>(R), ldr, chunks);
@@ -990,11 +1028,7 @@ extern "C" int ddlak_symm_residual(int n, int nrhs, const void* A, long long lda
         if (encode_f64_map(&amap, static_cast<const double*>(A), n, n, lda, SR, SR) &&
             encode_f64_map(&xmap, static_cast<const double*>(X), n, nrhs, ldx, SR, NC)) {
             const size_t smem = symm_residual_tma_smem<NC>();
-            static std::once_flag once_t;
-            std::call_once(once_t, [&] {
-                cudaFuncSetAttribute(k_symm_residual_tma<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem);
-            });
+            smem_optin(k_symm_residual_tma<NC>, smem);  // a failed raise shows as the launch's error
             dim3 grid((unsigned)(N * chunks), (unsigned)ceil_div(nrhs, NC));
             ProfScope ps(PK_SYMM_RESIDUAL, st, 2.0 * (double)n * n * nrhs, 4.0 * (double)n * (n + 1));
             k_symm_residual_tma<NC><<<grid, 256, smem, st>>>(amap, xmap, n, nrhs, static_cast<const double*>(X),
@@ -1002,10 +1036,7 @@ extern "C" int ddlak_symm_residual(int n, int nrhs, const void* A, long long lda
             return;
         }
         const size_t smem = symm_residual_smem<NC>();
-        static std::once_flag once;
-        std::call_once(once, [&] {
-            cudaFuncSetAttribute(k_symm_residual<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        });
+        smem_optin(k_symm_residual<NC>, smem);  // a failed raise shows as the launch's error
         dim3 grid((unsigned)(N * chunks), (unsigned)ceil_div(nrhs, NC));
         ProfScope ps(PK_SYMM_RESIDUAL, st, 2.0 * (double)n * n * nrhs, 4.0 * (double)n * (n + 1));
         k_symm_residual<NC><<<grid, 256, smem, st>>>(static_cast<const double*>(A), lda, n, nrhs,

@@ -18,6 +18,8 @@
 // returns immediately once info is set, so the first failure is the one kept.
 #include <mutex>
 
+#include <ddla_kernels.h>
+
 #include "common.cuh"
 #include "ddla_kernels_internal.h"
 #include "diag_factor.cuh"
@@ -214,13 +216,9 @@ cudaError_t launch_trsm_panel(T* A, long long lda, int k0, int nbk, int n, const
     constexpr int NQ = potrf_nb<T>() / 32;
     constexpr int PR = sizeof(T) >= 16 ? 4 : 8;
     const size_t panel_smem = (size_t)(NQ * 32) * (NQ * 32 + 1) * sizeof(T);
-    static std::once_flag once;
-    std::call_once(once, [&] {
-        cudaFuncSetAttribute(k_trsm_panel<T, UP, NQ, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)panel_smem);
-    });
     const long long m = (long long)n - k0 - nbk;
     if (m <= 0) return cudaSuccess;
+    if (cudaError_t e = smem_optin(k_trsm_panel<T, UP, NQ, PR>, panel_smem); e != cudaSuccess) return e;
     const double cf = Traits<T>::cplx ? 4.0 : 1.0, md = (double)m, b = nbk;
     ProfScope ps(PK_TRSM_PANEL, s, cf * md * b * b, sizeof(T) * (2.0 * md * b + b * (b + 1) / 2));
     k_trsm_panel<T, UP, NQ, PR><<<(unsigned)ceil_div(m, 8 * PR), 256, panel_smem, s>>>(A, lda, k0, nbk, n, dinfo);
@@ -253,19 +251,15 @@ LookaheadRes& lookahead_res()
 }  // namespace
 
 template <class T, bool UP>
-static cudaError_t potrf_enqueue(T* A, long long lda, int n, int* dinfo, cudaStream_t st)
+static cudaError_t potrf_enqueue(T* A, long long lda, int n, int G, int* dinfo, cudaStream_t st)
 {
     constexpr int NB = potrf_nb<T>();
     constexpr int NQ = NB / 32;
     constexpr int PR = sizeof(T) >= 16 ? 4 : 8;
     const size_t diag_smem = (size_t)NB * (NB + 1) * sizeof(T);
     const size_t panel_smem = (size_t)(NQ * 32) * (NQ * 32 + 1) * sizeof(T);
-    static std::once_flag attr_once;
-    std::call_once(attr_once, [&] {
-        cudaFuncSetAttribute(k_potrf_diag<T, UP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem);
-        cudaFuncSetAttribute(k_trsm_panel<T, UP, NQ, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)panel_smem);
-    });
+    if (cudaError_t e = smem_optin(k_potrf_diag<T, UP>, diag_smem); e != cudaSuccess) return e;
+    if (cudaError_t e = smem_optin(k_trsm_panel<T, UP, NQ, PR>, panel_smem); e != cudaSuccess) return e;
     const double cf = Traits<T>::cplx ? 4.0 : 1.0;  // real flops per multiply-add relative to a real one
     LookaheadRes& L = lookahead_res();
     cudaStream_t hi = L.hi;
@@ -288,74 +282,89 @@ static cudaError_t potrf_enqueue(T* A, long long lda, int n, int* dinfo, cudaStr
         }
         note_launches(1);
     };
-    auto update = [&](int k0, long long t0, int cols, cudaStream_t s) -> cudaError_t {
-        const int nbk = NB;
-        const double md = (double)(n - t0), b = nbk;
+    // C -= L(:, k0 : k0 + kw) L(:, k0 : k0 + kw)^H on the region from row / column t0
+    auto update = [&](int k0, int kw, long long t0, int cols, cudaStream_t s) -> cudaError_t {
+        const double md = (double)(n - t0), b = kw;
         const double cw = cols ? (double)cols : md;
         const double fl = cols ? cf * 2.0 * b * (md * cw - cw * (cw - 1) / 2) : cf * md * (md + 1) * b;
         ProfScope ps(PK_SYRK_UPDATE, s, fl, sizeof(T) * ((cols ? 2.0 * md * cw : md * (md + 1)) + md * b));
-        const cudaError_t e = trailing_update<T, UP>(A, lda, k0, nbk, n, t0, cols, dinfo, s);
+        const cudaError_t e = trailing_update<T, UP>(A, lda, k0, kw, n, t0, cols, dinfo, s);
         note_launches(1);
         return e;
     };
 
-    // fork: the internal stream starts after everything already queued on st
+    // Super-steps of G block columns: the chain on the high-priority stream factors
+    // them one after the other (block g first takes the left-looking update from
+    // blocks 0..g-1 of the super-step), then updates the next super-step's G block
+    // columns (look-ahead); the caller's stream updates everything to their right
+    // with K = G NB in one pass, so the trailing matrix is read and written once
+    // per G block columns.  The caller's stream waits for the super-step's panels;
+    // the chain waits for the previous trailing update before its look-ahead; the
+    // two touch disjoint tiles.
+    const long long SW = (long long)G * NB;
     cudaEventRecord(L.start, st);
     cudaStreamWaitEvent(hi, L.start, 0);
-    diag_and_panel(0, hi);
-    cudaEventRecord(L.panel, hi);
     bool have_rest = false;
-    for (int k0 = 0; k0 + NB < n; k0 += NB) {
-        const long long t0 = (long long)k0 + NB;       // first row of the trailing matrix
-        const long long m = (long long)n - t0;
-        // the rest of the trailing matrix (block columns >= k+2) on st, once panel k exists
-        cudaStreamWaitEvent(st, L.panel, 0);
-        if (m > NB) {
-            const cudaError_t e = update(k0, t0 + NB, 0, st);
-            if (e != cudaSuccess) return e;
+    cudaError_t e = cudaSuccess;
+    for (long long k0 = 0; k0 < n; k0 += SW) {
+        for (int g = 0; g < G; ++g) {
+            const long long kg = k0 + (long long)g * NB;
+            if (kg >= n) break;
+            if (g > 0) {
+                const int cols = (long long)n - kg < NB ? (int)(n - kg) : NB;
+                if ((e = update((int)k0, g * NB, kg, cols, hi)) != cudaSuccess) return e;
+            }
+            diag_and_panel((int)kg, hi);
         }
-        // block column k+1 was last written by the previous rest update
+        const long long t0 = k0 + SW;
+        if (t0 >= n) break;
+        cudaEventRecord(L.panel, hi);
         if (have_rest) cudaStreamWaitEvent(hi, L.rest, 0);
-        if (m > NB) {
+        const int la_cols = (long long)n - t0 < SW ? (int)(n - t0) : (int)SW;
+        if ((e = update((int)k0, (int)SW, t0, la_cols, hi)) != cudaSuccess) return e;
+        have_rest = false;
+        if (t0 + SW < n) {
+            cudaStreamWaitEvent(st, L.panel, 0);
+            if ((e = update((int)k0, (int)SW, t0 + SW, 0, st)) != cudaSuccess) return e;
             cudaEventRecord(L.rest, st);
             have_rest = true;
-        } else {
-            have_rest = false;
         }
-        const int cols = m < NB ? (int)m : NB;
-        const cudaError_t e = update(k0, t0, cols, hi);
-        if (e != cudaSuccess) return e;
-        diag_and_panel((int)t0, hi);
-        cudaEventRecord(L.panel, hi);
     }
     // join
+    cudaEventRecord(L.panel, hi);
     cudaStreamWaitEvent(st, L.panel, 0);
-    if (have_rest) cudaStreamWaitEvent(st, L.rest, 0);
     return cudaGetLastError();
 }
 
 template <class T>
-static cudaError_t potrf_typed(char uplo, int n, void* A, long long lda, int* dinfo, cudaStream_t st)
+static cudaError_t potrf_typed(char uplo, int n, int G, void* A, long long lda, int* dinfo, cudaStream_t st)
 {
-    if (uplo == 'U') return potrf_enqueue<T, true>(static_cast<T*>(A), lda, n, dinfo, st);
-    return potrf_enqueue<T, false>(static_cast<T*>(A), lda, n, dinfo, st);
+    if (uplo == 'U') return potrf_enqueue<T, true>(static_cast<T*>(A), lda, n, G, dinfo, st);
+    return potrf_enqueue<T, false>(static_cast<T*>(A), lda, n, G, dinfo, st);
 }
 
 }  // namespace ddlak
 
-extern "C" int ddlak_potrf(char type, char uplo, int n, void* A, long long lda, int* dinfo, void* stream)
+extern "C" int ddlak_potrf_grouped(char type, char uplo, int group, int n, void* A, long long lda, int* dinfo,
+                                   void* stream)
 {
     using namespace ddlak;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (group < 1 || group > DDLAK_POTRF_MAX_GROUP) return (int)cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(dinfo, 0, sizeof(int), st);
     if (e != cudaSuccess) return (int)e;
     if (n <= 0) return 0;
     switch (type) {
-    case 's': e = potrf_typed<float>(uplo, n, A, lda, dinfo, st); break;
-    case 'd': e = potrf_typed<double>(uplo, n, A, lda, dinfo, st); break;
-    case 'c': e = potrf_typed<cf32>(uplo, n, A, lda, dinfo, st); break;
-    case 'z': e = potrf_typed<cf64>(uplo, n, A, lda, dinfo, st); break;
+    case 's': e = potrf_typed<float>(uplo, n, group, A, lda, dinfo, st); break;
+    case 'd': e = potrf_typed<double>(uplo, n, group, A, lda, dinfo, st); break;
+    case 'c': e = potrf_typed<cf32>(uplo, n, group, A, lda, dinfo, st); break;
+    case 'z': e = potrf_typed<cf64>(uplo, n, group, A, lda, dinfo, st); break;
     default: return (int)cudaErrorInvalidValue;
     }
     return (int)e;
+}
+
+extern "C" int ddlak_potrf(char type, char uplo, int n, void* A, long long lda, int* dinfo, void* stream)
+{
+    return ddlak_potrf_grouped(type, uplo, DDLAK_POTRF_GROUP, n, A, lda, dinfo, stream);
 }

@@ -99,7 +99,9 @@ __device__ __forceinline__ TX widen(TL v)
 // ID: forward substitution only, on the identity (generated in place of B's
 // initial values): X = L^-1.  Chunk c's columns start at row c*RC, so block
 // rows above that one are zero and are neither computed nor waited for.
-template <class TL, class TX, bool UP, bool BT, bool INV = false, bool ID = false>
+// FO: forward substitution only, on B: X = L^-1 B (side 'L') or B L^-H (side
+// 'R'); the forward half of the two-sided solve, every CTA a forward one.
+template <class TL, class TX, bool UP, bool BT, bool INV = false, bool ID = false, bool FO = false>
 __global__ void __launch_bounds__(NT) k_potrs_fused(const TL* __restrict__ A, long long lda, TX* B, long long ldb,
                                                     int n, int nrhs, int nchunks, int* flags, int* ticket,
                                                     int* status, const TX* __restrict__ Dinv)
@@ -122,7 +124,7 @@ __global__ void __launch_bounds__(NT) k_potrs_fused(const TL* __restrict__ A, lo
     const int t = s_t;
     const int chunk = t % nchunks;
     const int step = t / nchunks;
-    const bool fwd = ID || step < N;
+    const bool fwd = ID || FO || step < N;
     const int blk = ID ? step : (fwd ? step : 2 * N - 1 - step);
     int* cflags = flags + (size_t)chunk * 2 * N;  // [0,N) forward, [N,2N) backward
     const long long r0 = (long long)chunk * RC;
@@ -367,26 +369,22 @@ __global__ void __launch_bounds__(NT) k_potrs_fused(const TL* __restrict__ A, lo
     if (threadIdx.x == 0) st_release(&cflags[fwd ? blk : N + blk], 1);
 }
 
-template <class T, bool UP, bool BT, class TL = T, bool INV = false, bool ID = false>
+template <class T, bool UP, bool BT, class TL = T, bool INV = false, bool ID = false, bool FO = false>
 cudaError_t potrs_launch(const TL* A, long long lda, T* B, long long ldb, int n, int nrhs, int* flags, int* ticket,
                          int* status, cudaStream_t st, const T* Dinv = nullptr)
 {
     const int N = (int)ceil_div(n, RB);
     const int nchunks = (int)ceil_div(nrhs, RC);
-    const long long grid = (ID ? 1LL : 2LL) * N * nchunks;
+    const long long grid = (ID || FO ? 1LL : 2LL) * N * nchunks;
     const size_t smem = potrs_smem_bytes<TL, T, INV>();
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_potrs_fused<TL, T, UP, BT, INV, ID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-        attr = true;
-    }
+    if (cudaError_t e = smem_optin(k_potrs_fused<TL, T, UP, BT, INV, ID, FO>, smem); e != cudaSuccess) return e;
     const double cf = Traits<T>::cplx ? 4.0 : 1.0;
     const double nd = n, rd = nrhs;
-    ProfScope ps(PK_POTRS_FUSED, st, ID ? cf * nd * nd * nd / 3.0 : cf * 2.0 * nd * nd * rd,
+    ProfScope ps(PK_POTRS_FUSED, st,
+                 ID ? cf * nd * nd * nd / 3.0 : (FO ? cf * nd * nd * rd : cf * 2.0 * nd * nd * rd),
                  sizeof(TL) * nd * (nd + 1) + sizeof(T) * 4.0 * nd * rd);
-    k_potrs_fused<TL, T, UP, BT, INV, ID><<<(unsigned)grid, NT, smem, st>>>(A, lda, B, ldb, n, nrhs, nchunks, flags,
-                                                                             ticket, status, Dinv);
+    k_potrs_fused<TL, T, UP, BT, INV, ID, FO><<<(unsigned)grid, NT, smem, st>>>(A, lda, B, ldb, n, nrhs, nchunks,
+                                                                                 flags, ticket, status, Dinv);
     note_launches(1);
     return cudaGetLastError();
 }
@@ -402,6 +400,22 @@ cudaError_t potrs_typed(char uplo, char side, int n, int nrhs, const void* A, lo
     if (up) return potrs_launch<T, true, false>(a, lda, b, ldb, n, nrhs, flags, ticket, status, st);
     if (bt) return potrs_launch<T, false, true>(a, lda, b, ldb, n, nrhs, flags, ticket, status, st);
     return potrs_launch<T, false, false>(a, lda, b, ldb, n, nrhs, flags, ticket, status, st);
+}
+
+template <class T>
+cudaError_t forward_typed(char uplo, char side, int n, int nrhs, const void* A, long long lda, void* B,
+                          long long ldb, int* flags, int* ticket, int* status, cudaStream_t st)
+{
+    const T* a = static_cast<const T*>(A);
+    T* b = static_cast<T*>(B);
+    const bool up = uplo == 'U', bt = side == 'R';
+    if (up && bt)
+        return potrs_launch<T, true, true, T, false, false, true>(a, lda, b, ldb, n, nrhs, flags, ticket, status, st);
+    if (up)
+        return potrs_launch<T, true, false, T, false, false, true>(a, lda, b, ldb, n, nrhs, flags, ticket, status, st);
+    if (bt)
+        return potrs_launch<T, false, true, T, false, false, true>(a, lda, b, ldb, n, nrhs, flags, ticket, status, st);
+    return potrs_launch<T, false, false, T, false, false, true>(a, lda, b, ldb, n, nrhs, flags, ticket, status, st);
 }
 
 cudaError_t potrs_dispatch(char type, char uplo, char side, int n, int nrhs, const void* A, long long lda, void* B,
@@ -535,7 +549,9 @@ constexpr int kFixedFlagInts = 2 * (kFixedMaxN / RB) * (kFixedMaxRhs / RC);
 __device__ __align__(256) int g_potrs_fixed_scratch[kFixedHeaderInts + kFixedFlagInts];
 
 // Device address of the array on the current device; looked up once per
-// device (the first call on a device does the lookup, with that device current).
+// device (the first call on a device does the lookup, with that device current)
+// and kept for the process's life, which assumes the device's primary context
+// is never reset (cudaDeviceReset) while the library is in use.
 int* fixed_scratch_ptr(int* err)
 {
     static std::mutex mu;
@@ -600,6 +616,31 @@ extern "C" int ddlak_potrs(char type, char uplo, char side, int n, int nrhs, con
     int* ticket = status + 1;
     int* flags = reinterpret_cast<int*>(static_cast<char*>(work) + 256);
     return (int)potrs_dispatch(type, uplo, side, n, nrhs, A, lda, B, ldb, flags, ticket, status, st);
+}
+
+// X = L^-1 B (side 'L', B n x nrhs) or X = B L^-H (side 'R', B nrhs x n), in place,
+// with the factor read through its L view (uplo 'L': A's lower triangle; 'U': L = U^H):
+// the forward half of ddlak_potrs.  Same scratch (ddlak_potrs_workspace(n, nrhs)) and
+// status word.
+extern "C" int ddlak_forward_solve(char type, char uplo, char side, int n, int nrhs, const void* A, long long lda,
+                                   void* B, long long ldb, void* work, unsigned long long work_bytes, void* stream)
+{
+    using namespace ddlak;
+    if (n <= 0 || nrhs <= 0) return 0;
+    if (!A || !B || work_bytes < ddlak_potrs_workspace(n, nrhs)) return (int)cudaErrorInvalidValue;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(work, 0, ddlak_potrs_workspace(n, nrhs), st);
+    if (e != cudaSuccess) return (int)e;
+    int* status = static_cast<int*>(work);
+    int* ticket = status + 1;
+    int* flags = reinterpret_cast<int*>(static_cast<char*>(work) + 256);
+    switch (type) {
+    case 's': return (int)forward_typed<float>(uplo, side, n, nrhs, A, lda, B, ldb, flags, ticket, status, st);
+    case 'd': return (int)forward_typed<double>(uplo, side, n, nrhs, A, lda, B, ldb, flags, ticket, status, st);
+    case 'c': return (int)forward_typed<cf32>(uplo, side, n, nrhs, A, lda, B, ldb, flags, ticket, status, st);
+    case 'z': return (int)forward_typed<cf64>(uplo, side, n, nrhs, A, lda, B, ldb, flags, ticket, status, st);
+    default: return (int)cudaErrorInvalidValue;
+    }
 }
 
 // W = L^-1 for a lower factor: the fused forward substitution on the identity.

@@ -9,7 +9,9 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <map>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include "profile.h"
@@ -44,6 +46,21 @@ cudaEvent_t get_event()
 void note_launches(int count) { g_launches.fetch_add(count, std::memory_order_relaxed); }
 
 bool profiling() { return g_on.load(std::memory_order_relaxed); }
+
+cudaError_t smem_optin(const void* func, std::size_t bytes)
+{
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, std::size_t> raised;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = raised.find({func, dev});
+    if (it != raised.end() && it->second >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) raised[{func, dev}] = bytes;
+    return e;
+}
 
 ProfScope::ProfScope(int kind, cudaStream_t st, double flops, double bytes) : st_(st), active_(profiling())
 {

@@ -24,6 +24,17 @@ enum ProfKind : int {
 void note_launches(int count);
 bool profiling();
 
+// Raise kernel `func`'s dynamic shared-memory limit to `bytes` on the current
+// device.  cudaFuncSetAttribute applies to one device only, so the raise is
+// recorded per (kernel, device) and made again on every other device; thread
+// safe; returns the attribute call's error, if any.
+cudaError_t smem_optin(const void* func, std::size_t bytes);
+template <class K>
+cudaError_t smem_optin(K* func, std::size_t bytes)
+{
+    return smem_optin(reinterpret_cast<const void*>(func), bytes);
+}
+
 // Brackets the launches made while it lives with two events on st (profiling on only).
 class ProfScope {
 public:

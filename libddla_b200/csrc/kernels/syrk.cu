@@ -10,6 +10,7 @@
 // only i >= j.  Other types use the SIMT kernel in potrf.cu.
 #include "common.cuh"
 #include "ddla_kernels_internal.h"
+#include "profile.h"
 
 namespace ddlak {
 
@@ -181,11 +182,7 @@ cudaError_t launch_dmma(double* A, long long lda, int k0, int nbk, int n, long l
                         cudaStream_t st)
 {
     const size_t smem = DM_NSTAGE * DM_STAGE * sizeof(double);
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_syrk_dmma<UP, VEC2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-    }
+    if (cudaError_t e = smem_optin(k_syrk_dmma<UP, VEC2>, smem); e != cudaSuccess) return e;
     const long long m = (long long)n - t0;
     if (m <= 0) return cudaSuccess;
     const long long t = ceil_div(m, DM_BM);

@@ -352,11 +352,7 @@ cudaError_t vb_launch(int batch, const int* d_n, void* const* d_A, const int* d_
                       int grid, cudaStream_t st)
 {
     constexpr size_t smem = VbSmem<T, NMAX>::bytes;
-    static bool attr = [] {
-        cudaFuncSetAttribute(k_posv_vbatched<T, NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        return true;
-    }();
-    (void)attr;
+    if (cudaError_t e = smem_optin(k_posv_vbatched<T, NMAX>, smem); e != cudaSuccess) return e;
     k_posv_vbatched<T, NMAX><<<grid, VB_NT, smem, st>>>(batch, d_n, reinterpret_cast<T* const*>(d_A), d_lda,
                                                         reinterpret_cast<T* const*>(d_B), d_logdet, d_info, order,
                                                         wsel, counters);
@@ -368,7 +364,7 @@ template <class T, int NMAX>
 int vb_max_grid()
 {
     constexpr size_t smem = VbSmem<T, NMAX>::bytes;
-    cudaFuncSetAttribute(k_posv_vbatched<T, NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (smem_optin(k_posv_vbatched<T, NMAX>, smem) != cudaSuccess) return 0;
     int dev = 0, sms = 0, per = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;

@@ -17,8 +17,8 @@ from .backend import Backend, Communication, Handle  # noqa: F401
 from .layout import ProcessorLayout  # noqa: F401
 from .matrix import DistributedMatrix  # noqa: F401
 from . import autograd, batched  # noqa: F401
-from .ops import (diag_logdet, gather, pdiag_logdet, potrf, potrf_bottom_right, pposv, pposv_mixed, ppotrf,  # noqa: F401
-                  ppotrf_bottom_right, ppotrs, scatter)
+from .ops import (diag_logdet, gather, pdiag_logdet, phegst, potrf, potrf_bottom_right, pposv, pposv_mixed,  # noqa: F401
+                  ppotrf, ppotrf_bottom_right, ppotrs, scatter)
 
 
 def finalize():

@@ -166,6 +166,12 @@ for _p in "sdcz":
         f"ddla_{_p}_pdiag_logdet": (_i, [_vp, _i, _vp, _vp, _vp]),
         f"ddla_{_p}_potrf_bottom_right": (_i, [_vp, _c, _i, _vp, _i, _ip]),
         f"ddla_{_p}_ppotrf_bottom_right": (_i, [_vp, _c, _i, _vp, _vp, _ip]),
+        f"ddla_{_p}_phegst": (_i, [_vp, _c, _i, _vp, _vp, _vp, _vp]),
+        **({f"ddla_{_p}_gemm_vbatched_{v}": (_i, [_vp, _c, _c] + [_vp] * 11 + [_i]) for v in ("rc", "cr")}
+           if _p in "cz" else {}),
+        **({f"ddla_{_p}_gemm_vbatched2s_{v}": (_i, [_vp, _c, _c] + [_vp] * 11 + [_c, _c] + [_vp] * 10
+                                               + [_i, _i, _vp, _i])
+            for v in ("rzzr", "zrzr", "rzzz", "zrzz", "zzzr", "rrrz")} if _p in "cz" else {}),
         f"ddla_{_p}_gemm_vbatched": (_i, [_vp, _c, _c, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                           _i]),
         f"ddla_{_p}_gemm_vbatched2s": (_i, [_vp, _c, _c, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,

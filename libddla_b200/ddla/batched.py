@@ -238,7 +238,19 @@ def gemm_vbatched(handle, transA: str, transB: str, m, n, k, alpha, A_list, lda,
     tensors = [t for t in list(A_list) + list(B_list) + list(C_list) if t is not None]
     if not tensors:
         raise ValueError("gemm_vbatched: at least one matrix is needed to fix the type")
-    sfx = _GV_SFX[str(tensors[0].dtype)]
+    first = lambda xs: next((str(t.dtype) for t in xs if t is not None), None)
+    ta_, tb_, tc_ = first(A_list), first(B_list), first(C_list)
+    kinds = {t for t in (ta_, tb_, tc_) if t is not None}
+    mixed = ""
+    if len(kinds) > 1:
+        # one real and one complex operand, complex output: the mixed overloads
+        if ta_ is not None and tb_ is not None and "complex" in ta_ and "complex" not in tb_:
+            mixed = "_cr"
+        elif ta_ is not None and tb_ is not None and "complex" not in ta_ and "complex" in tb_:
+            mixed = "_rc"
+        else:
+            raise TypeError(f"gemm_vbatched: operand types {ta_}, {tb_}, {tc_} do not form a supported combination")
+    sfx = _GV_SFX[tc_ or str(tensors[0].dtype)]
     dev = tensors[0].device
     batch = len(C_list)
 
@@ -258,7 +270,7 @@ def gemm_vbatched(handle, transA: str, transB: str, m, n, k, alpha, A_list, lda,
     be = np.array([beta], dtype=sdt)
     torch.cuda.synchronize(dev)  # inputs written on torch's stream; the call runs on the handle's
 
-    fn = getattr(C, f"ddla_{sfx}_gemm_vbatched")
+    fn = getattr(C, f"ddla_{sfx}_gemm_vbatched{mixed}")
     C.check_status(fn(handle.ptr, transA.encode(), transB.encode(), _ptr(dm), _ptr(dn), _ptr(dk), al.ctypes.data,
                       _ptr(pa), _ptr(dlda), _ptr(pb), _ptr(dldb), be.ctypes.data, _ptr(pc), _ptr(dldc), batch),
                    "gemm_vbatched")
@@ -278,14 +290,16 @@ def _addr(x):
 
 def gemm_vbatched2s(handle, ops0: str, m0, n0, k0, alpha0, A0, lda0, B0, ldb0, C0, ldc0,
                     ops1: str, m1, n1, k1, alpha1, AB1, lda1, ldb1, beta1, C1, ldc1,
-                    c0_left: bool, segments, dtype, beta0=0) -> None:
+                    c0_left: bool, segments, dtype, beta0=0, pattern: str = "") -> None:
     """The two-stage batched GEMM (ddla_?_gemm_vbatched2s, the reference's
     gemmVbatched2s): per segment, C0_i = alpha0 op(A0_i) op(B0_i), then
     C1_i = alpha1 op(X_i) op(Y_i) + beta1 C1_i with (X, Y) = (C0_i, AB1_i) when
     c0_left, else (AB1_i, C0_i).  ops0 / ops1 are two-letter transpose pairs
     ("NN", "TC", ...); matrix entries are CUDA tensors, int device addresses (C0
     entries of different segments may share storage) or None; dtype is the
-    torch dtype.  Completes before returning."""
+    torch dtype of C1.  pattern (e.g. "rzzr") selects a mixed overload by the
+    element types of (A0, B0, C0, AB1), r real, z complex; alpha0 / beta0 then
+    have C0's type.  Completes before returning."""
     torch = _torch()
     sfx = _GV_SFX[str(dtype)]
     batch = len(C1)
@@ -301,11 +315,17 @@ def gemm_vbatched2s(handle, ops0: str, m0, n0, k0, alpha0, A0, lda0, B0, ldb0, C
     d = [iarr(v) for v in (m0, n0, k0, lda0, ldb0, ldc0, m1, n1, k1, lda1, ldb1, ldc1)]
     p = [parr(v) for v in (A0, B0, C0, AB1, C1)]
     sdt = {"s": np.float32, "d": np.float64, "c": np.complex64, "z": np.complex128}[sfx]
-    sc = [np.array([v], dtype=sdt) for v in (alpha0, beta0, alpha1, beta1)]
+    s0 = sdt
+    if pattern:
+        if sfx not in "cz" or len(pattern) != 4:
+            raise ValueError("gemm_vbatched2s: a mixed pattern needs a complex C1 and four letters")
+        s0 = sdt if pattern[2] == "z" else {"c": np.float32, "z": np.float64}[sfx]
+    sc = [np.array([alpha0], dtype=s0), np.array([beta0], dtype=s0), np.array([alpha1], dtype=sdt),
+          np.array([beta1], dtype=sdt)]
     seg = np.asarray(segments, dtype=np.int32)
     if dev.type == "cuda":
         torch.cuda.synchronize(dev)  # inputs written on torch's stream; the call runs on the handle's
-    fn = getattr(C, f"ddla_{sfx}_gemm_vbatched2s")
+    fn = getattr(C, f"ddla_{sfx}_gemm_vbatched2s" + (f"_{pattern}" if pattern else ""))
     C.check_status(fn(handle.ptr, ops0[0].encode(), ops0[1].encode(), _ptr(d[0]), _ptr(d[1]), _ptr(d[2]),
                       sc[0].ctypes.data, _ptr(p[0]), _ptr(d[3]), _ptr(p[1]), _ptr(d[4]), sc[1].ctypes.data,
                       _ptr(p[2]), _ptr(d[5]), ops1[0].encode(), ops1[1].encode(), _ptr(d[6]), _ptr(d[7]),

@@ -87,6 +87,16 @@ def pdiag_logdet(A: DistributedMatrix, n: int = -1) -> complex:
     return complex(float(out[0]), float(out[1]))
 
 
+def phegst(A: DistributedMatrix, F: DistributedMatrix, uplo: str = "L", n: int = -1) -> DistributedMatrix:
+    """A <- L^-1 A L^-H in place with F holding the Cholesky factor of B (ddla_?_phegst;
+    the reference's phegst on a 1x1 grid).  Returns A."""
+    n = A.n if n < 0 else n
+    f = getattr(C.lib, f"ddla_{A.type_char}_phegst")
+    C.check_status(f(A.handle.ptr, _ch(uplo), int(n), A.data_ptr, A.desc.ctypes.data, F.data_ptr,
+                     F.desc.ctypes.data), f"ddla_{A.type_char}_phegst")
+    return A
+
+
 def diag_logdet(A: DistributedMatrix, n: int = -1) -> complex:
     """Principal log of the product of the diagonal of the leading n x n of A."""
     n = A.n if n < 0 else n

@@ -47,14 +47,38 @@ def se_kernel(n: int, seed: int, lengthscale=0.2, nugget=1e-2, complex_=False, d
     return K
 
 
-def householder_spd(n: int, kappa: float, seed: int, device="cuda"):
-    """A = H1 H2 H3 H4 diag(s) H4 H3 H2 H1 built in place with rank-one updates (torch.addr_)."""
+def householder_factors(n: int, kappa: float, seed: int, device="cuda"):
+    """(s, [v1, v2, v3, v4]) of householder_spd: the spectrum and the reflector vectors."""
     torch = _torch()
     g = torch.Generator(device=device).manual_seed(seed)
     s = torch.pow(torch.tensor(float(kappa), dtype=torch.float64, device=device),
                   -torch.arange(n, device=device, dtype=torch.float64) / max(1, n - 1))
-    A = torch.diag(s)
     vs = [torch.randn(n, generator=g, device=device, dtype=torch.float64) for _ in range(4)]
+    return s, vs
+
+
+def householder_solve(s, vs, B):
+    """A^-1 B = U diag(1/s) U^T B for A = U diag(s) U^T, U = H1 H2 H3 H4 (each H = I - 2 v v^T / v^T v
+    symmetric), applied reflector by reflector: O(n nrhs) work, the exact inverse up to rounding.
+    B: n x nrhs (torch, float64)."""
+    def refl(v, X):
+        return X - (2.0 / float(v @ v)) * torch_outer(v, v @ X)
+
+    torch_outer = lambda v, w: v[:, None] * w[None, :]
+    Y = B
+    for v in vs:  # U^T B = H4 H3 H2 H1 B: H1 first
+        Y = refl(v, Y)
+    Y = Y / s[:, None]
+    for v in reversed(vs):  # U Y = H1 H2 H3 H4 Y: H4 first
+        Y = refl(v, Y)
+    return Y
+
+
+def householder_spd(n: int, kappa: float, seed: int, device="cuda"):
+    """A = H1 H2 H3 H4 diag(s) H4 H3 H2 H1 built in place with rank-one updates (torch.addr_)."""
+    torch = _torch()
+    s, vs = householder_factors(n, kappa, seed, device=device)
+    A = torch.diag(s)
     for v in reversed(vs):
         beta = 2.0 / float(v @ v)
         w = A @ v

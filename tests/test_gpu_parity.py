@@ -410,3 +410,28 @@ def test_diag_logdet_random_vs_oracle(handle):
         ro = restated.diag_logdet(A)
         assert abs(r.real - ro.real) < 1e-10 * abs(ro.real) + 1e-10
         assert abs(math.remainder(r.imag - ro.imag, 2 * math.pi)) < 1e-9
+
+
+def test_two_devices_in_one_process():
+    """Handles on devices 0 and 1 in one process: each device gets its own raise of
+    the kernels' dynamic shared-memory limits (the fused solve and the DMMA update
+    need more than the 48 KB default), so both solve correctly."""
+    import torch
+
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two visible devices")
+    ddla = _ddla()
+    rng = np.random.default_rng(77)
+    n, nrhs = 700, 5
+    G = rng.standard_normal((n, n))
+    A = G @ G.T / n + np.eye(n)
+    B = rng.standard_normal((n, nrhs))
+    for dev in (0, 1, 0):
+        with torch.cuda.device(dev):
+            with ddla.Handle(ddla.Backend.GPU) as h:
+                dA = ddla.DistributedMatrix.from_global_matrix(h, A, mb=128, nb=128)
+                dB = ddla.DistributedMatrix.from_global_matrix(h, B, mb=128, nb=128)
+                X, info = ddla.pposv(dA, dB, "L")
+                assert info == 0
+                Xh = X.to_global_matrix()
+        assert np.max(np.abs(A @ Xh - B)) <= 1e-9 * np.max(np.abs(B))

@@ -38,3 +38,20 @@ def test_gram_and_kernel_families():
     x = W.gp_points(10, 5, device="cpu")
     assert x.shape == (10, 2) and bool(((x >= 0) & (x <= 1)).all())
     assert torch.equal(x, W.gp_points(10, 5, device="cpu"))
+
+
+@pytest.mark.parametrize("kappa", [1e2, 1e6, 1e10])
+def test_householder_exact_inverse(kappa):
+    """householder_solve applies A^-1 = U diag(1/s) U^T from the reflectors: it agrees with a dense
+    solve of the generated A to the accuracy the conditioning allows, and A X reproduces B."""
+    import torch
+
+    n = 160
+    A = W.householder_spd(n, kappa, 11, device="cpu")
+    s, vs = W.householder_factors(n, kappa, 11, device="cpu")
+    B = torch.randn(n, 4, generator=torch.Generator().manual_seed(2), dtype=torch.float64)
+    X = W.householder_solve(s, vs, B)
+    eps = np.finfo(np.float64).eps
+    assert float((A @ X - B).abs().max()) <= 50 * n * eps * float(A.abs().sum(0).max()) * float(X.abs().max())
+    Xd = torch.linalg.solve(A, B)
+    assert float((X - Xd).abs().max() / X.abs().max()) <= 10 * kappa * n * eps

@@ -23,8 +23,11 @@ def _noalloc(C):
     return f
 
 
-@pytest.mark.parametrize("uplo,n,nrhs", [("L", 1000, 7), ("U", 777, 40)])
-def test_noalloc_solve_matches_ppotrs_twice(handle, uplo, n, nrhs):
+# (side, uplo, n, nrhs): both triangles and both sides; nrhs = 256 with n = 333
+# (not a multiple of the 64-row block) fills the array's whole flag stride.
+@pytest.mark.parametrize("side,uplo,n,nrhs", [("L", "L", 1000, 7), ("L", "U", 777, 40), ("R", "L", 500, 9),
+                                              ("R", "U", 333, 256), ("L", "L", 333, 256)])
+def test_noalloc_solve_matches_ppotrs_twice(handle, side, uplo, n, nrhs):
     from libddla_b200 import ddla
 
     C = ddla._c_api
@@ -36,16 +39,17 @@ def test_noalloc_solve_matches_ppotrs_twice(handle, uplo, n, nrhs):
     _, info = ddla.ppotrf(dA, uplo)
     assert info == 0
     for _ in range(2):  # two calls in a row: the shared scratch is reset by each call
-        B = rng.standard_normal((n, nrhs))
+        B = rng.standard_normal((n, nrhs) if side == "L" else (nrhs, n))
         d1 = ddla.DistributedMatrix.from_global_matrix(handle, B, mb=64, nb=64)
-        ddla.ppotrs(dA, d1, uplo)
+        ddla.ppotrs(dA, d1, uplo, side=side)
         d2 = ddla.DistributedMatrix.from_global_matrix(handle, B, mb=64, nb=64)
-        st = f(handle.ptr, b"L", uplo.encode(), b"N", n, nrhs, dA.data_ptr, dA.desc.ctypes.data, d2.data_ptr,
-               d2.desc.ctypes.data)
+        st = f(handle.ptr, side.encode(), uplo.encode(), b"N", n, nrhs, dA.data_ptr, dA.desc.ctypes.data,
+               d2.data_ptr, d2.desc.ctypes.data)
         assert st == 0, C.error_string(st)
         X1, X2 = d1.to_global_matrix(), d2.to_global_matrix()
         assert np.max(np.abs(X1 - X2)) <= 1e-12 * np.max(np.abs(X1))
-        assert np.max(np.abs(A @ X2 - B)) <= 1e-9 * np.max(np.abs(B))
+        R = A @ X2 - B if side == "L" else X2 @ A - B
+        assert np.max(np.abs(R)) <= 1e-9 * np.max(np.abs(B))
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch(handle):
