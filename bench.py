@@ -264,6 +264,131 @@ def vendor_leg(args, torch, A0, B0, backward_error):
                        "calls": "torch.linalg.cholesky_ex + torch.cholesky_solve (cuSOLVER potrf, potrs)"}}
 
 
+def flops_pposv_cplx(n: int, nrhs: int) -> float:
+    return 4.0 * n ** 3 / 3.0 + 8.0 * n * n * nrhs
+
+
+def se_kernel_leg(args, torch, device, h, stream, C):
+    """The SE-kernel configuration: pposv on A = K + 1e-2 I, K a squared-exponential kernel
+    (lengthscale 0.2) on 16384 points uniform in [0,1]^3, nrhs = 64, for double and complex
+    double (K times exp(i k.(x - y)), k ~ N(0, I3)).  Ours: ddla pposv (plain path) through the
+    C ABI, device-timed on the handle's stream with A restored outside the events.  Beside it the
+    reference's GPU arm (cuSOLVER potrf + potrs through torch) and its CPU arm (LAPACK ?potrf +
+    2 ?trsm, one solve on the host cores), the solution's relative difference from the CPU arm,
+    and the factor's scaled backward error ||A - L L^H||_F / (n eps ||A||_F)."""
+    from libddla_b200 import ddla
+    from libddla_b200.workloads import se_kernel
+    from oracle import lapack_arm
+
+    n, nrhs = args.se_n, 64
+    out = {}
+    for p, cplx in (("d", False), ("z", True)):
+        A = se_kernel(n, 0xDD1A0002, complex_=cplx, device=device)  # Hermitian, row-major
+        Acm = A.T.contiguous()  # column-major storage of A
+        dt = A.dtype
+        g = torch.Generator(device=device).manual_seed(0xDD1A0102)
+        Bt = torch.randn(nrhs, n, generator=g, device=device, dtype=torch.float64)
+        if cplx:
+            Bt = torch.complex(Bt, torch.randn(nrhs, n, generator=g, device=device, dtype=torch.float64))
+        Aw, Xw = torch.empty_like(Acm), torch.empty_like(Bt)
+        npdt = np.complex128 if cplx else np.float64
+        dA = ddla.DistributedMatrix.wrap(h, Aw.data_ptr(), n, n, n, npdt, mb=256, nb=256)
+        dX = ddla.DistributedMatrix.wrap(h, Xw.data_ptr(), n, nrhs, n, npdt, mb=256, nb=256)
+        fl = flops_pposv_cplx(n, nrhs) if cplx else flops_pposv(n, nrhs)
+
+        def restore():
+            with torch.cuda.stream(stream):
+                Aw.copy_(Acm)
+                Xw.copy_(Bt)
+
+        times = []
+        for i in range(args.warmup + max(1, min(3, args.steps))):
+            restore()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            _, info = ddla.pposv(dA, dX, "L")
+            e1.record(stream)
+            e1.synchronize()
+            assert info == 0, (p, info)
+            if i >= args.warmup:
+                times.append(e0.elapsed_time(e1))
+        ms = statistics.median(times)
+        L = torch.tril(Aw.T)
+        eps = float(np.finfo(np.float64).eps)
+        R = L @ L.conj().T
+        R -= A
+        bwd = float(torch.linalg.norm(R) / (n * eps * torch.linalg.norm(A)))
+        del R, L
+        X = Xw.T  # n x nrhs
+        # the reference's GPU arm on the same matrix
+        vt = []
+        for i in range(2):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            Lv, vinfo = torch.linalg.cholesky_ex(A)
+            Xv = torch.cholesky_solve(Bt.T, Lv)
+            e1.record()
+            e1.synchronize()
+            vt.append(e0.elapsed_time(e1))
+            del Lv
+        vms = min(vt)
+        # the reference's CPU arm: one solve on the host cores, and the solution agreement
+        Ah = np.asfortranarray(A.cpu().numpy())
+        Bh = np.asfortranarray(Bt.T.cpu().numpy())
+        t0 = time.perf_counter()
+        _, Xref, cinfo = lapack_arm.pposv(Ah, Bh, "L", overwrite=True)
+        cpu_s = time.perf_counter() - t0
+        del Ah
+        Xr = torch.from_numpy(np.ascontiguousarray(Xref)).to(device)
+        rel = float((X - Xr).abs().max() / Xr.abs().max())
+        rel_v = float((Xv - Xr).abs().max() / Xr.abs().max())
+        info_b = lapack_arm.blas_info()
+        out[p] = {"value": fl / (ms * 1e-3) / 1e12, "unit": "TFLOP/s", "ms_per_step": ms,
+                  "factor_backward_error": bwd, "rel_diff_vs_cpu_arm": rel,
+                  "vendor": {"value": fl / (vms * 1e-3) / 1e12, "ms": vms, "rel_diff_vs_cpu_arm": rel_v},
+                  "cpu_arm": {"value": fl / cpu_s / 1e12, "s": cpu_s, "cores": info_b.get("threads"),
+                              "info": int(cinfo)}}
+        del A, Acm, Aw, Xw, Bt, Xv, Xr, X
+        torch.cuda.empty_cache()
+    return {"metric": "pposv TFLOP/s (plain path) on the SE-kernel matrices", "unit": "TFLOP/s",
+            "config": {"workload": f"pposv d and z uplo=L n={n} nrhs={nrhs}, A = K + 1e-2 I, SE kernel l=0.2 on "
+                                   "points U[0,1]^3 (z: K exp(i k.(x-y)), k ~ N(0, I3)), B ~ N(0,1)",
+                       "flops": "d: n^3/3 + 2 n^2 nrhs; z: 4 n^3/3 + 8 n^2 nrhs"}, **out}
+
+
+def kappa_leg(args, torch, device, h, stream, C, mixed_solve_fn):
+    """The Householder family at every kappa of its configuration (1e2, 1e6, 1e10) for both
+    tensor-core precisions: one device-timed mixed solve each, with the refinement report (sweeps,
+    GMRES use, diagonal shift, FP64 fallback), the normwise backward error and the forward error
+    against the exact solution U diag(1/s) U^T B."""
+    from libddla_b200.workloads import householder_factors, householder_solve, householder_spd
+
+    n, nrhs = args.n, args.nrhs
+    out = {}
+    g = torch.Generator(device=device).manual_seed(0xDD1A0103)
+    B0 = torch.randn(nrhs, n, generator=g, device=device, dtype=torch.float64)
+    for kappa in (1e2, 1e6, 1e10):
+        A = householder_spd(n, kappa, 0xDD1A0003, device=device)
+        s, vs = householder_factors(n, kappa, 0xDD1A0003, device=device)
+        Xex = householder_solve(s, vs, B0.T)
+        an = float(A.abs().sum(dim=0).max())
+        for prec in ("B", "T"):
+            ms, info, rep, X = mixed_solve_fn(A, B0, prec)
+            R = B0.T - A @ X.T
+            bwd = float((R.abs().max(dim=0).values / (an * X.T.abs().max(dim=0).values)).max())
+            fwd = float(((X.T - Xex).abs().max(dim=0).values / Xex.abs().max(dim=0).values).max())
+            out[f"{prec} kappa={kappa:g}"] = {
+                "ms": ms, "tflops": flops_pposv(n, nrhs) / (ms * 1e-3) / 1e12, "info": info, "iter": rep["iter"],
+                "gmres": rep["gmres"], "shift": rep["shift"], "fp64_fallback": rep["iter"] < 0,
+                "backward_error": bwd, "forward_error_vs_exact": fwd}
+            del R, X
+        del A, Xex
+        torch.cuda.empty_cache()
+    return {"config": {"workload": f"pposv_mixed d n={n} nrhs={nrhs} A=U diag(s) U^T, s geometric 1..1/kappa",
+                       "forward_error": "max over columns of ||x - x*||_inf / ||x*||_inf, x* = U diag(1/s) U^T b"},
+            **out}
+
+
 def gemm_vbatched_leg(args, torch, device, h, stream, C):
     """Variable-size batched GEMM (gemmVbatched): 2000 entries, m, n, k uniform in [32, 256],
     C_i = A_i B_i + 0.5 C_i, column-major with tight leading dimensions, for s/d/c/z.  Timed
@@ -511,6 +636,9 @@ def gp_leg(args, torch, device):
         ag.gp_nll(X2, y2, th2).sum().backward()
 
     ms_big = timed(big, 1) if not args.no_gp_large else None
+    big_err = None
+    if not args.no_gp_large:
+        big_err = gp_large_gradient_check(torch, device, X2, y2, th2.grad.detach().clone())
     return {"metric": "GP marginal likelihood logdet+grad evaluations/s", "value": rate, "unit": "1/s",
             "ms_per_step": ms, "dtype": "f64",
             "config": {"workload": f"{B} x n={n} SE-kernel GPs, points U[0,1]^2, l=0.3 sigma_f^2=1 sigma^2=1e-2, "
@@ -519,7 +647,33 @@ def gp_leg(args, torch, device):
                                f"({nloop}-matrix sample)"},
             "loop_value": loop_rate, "vs_loop": rate / loop_rate, "torch_batched_value": B / (tb * 1e-3),
             "grad_rel_err_vs_torch_fp64": rel,
-            "single_n16384_f32_ms": ms_big}
+            "single_n16384_f32_ms": ms_big, "single_n16384_f32_grad_check": big_err}
+
+
+def gp_large_gradient_check(torch, device, X, y, grad):
+    """dloss/dtheta of the n=16384 FP32 problem against FP64 torch autograd on the same points, with
+    torch's own FP32 autograd gradient beside it as the error a same-precision computation makes."""
+    def torch_grad(dt):
+        t = torch.tensor([0.3, 1.0, 1e-2], dtype=torch.float64, device=device, requires_grad=True)
+        Xd = X[0].to(dt)
+        r2 = torch.cdist(Xd, Xd).square_()
+        K = t[1].to(dt) * torch.exp(-r2 / (2 * t[0].to(dt) ** 2))
+        del r2
+        K = K + t[2].to(dt) * torch.eye(Xd.shape[0], dtype=dt, device=device)
+        L = torch.linalg.cholesky(K)
+        del K
+        yd = y[0].to(dt)
+        a = torch.cholesky_solve(yd.unsqueeze(-1), L).squeeze(-1)
+        (0.5 * ((yd * a).sum() + 2 * torch.log(torch.diagonal(L)).sum())).backward()
+        return t.grad.detach().clone()
+
+    g64 = torch_grad(torch.float64)
+    torch.cuda.empty_cache()
+    g32 = torch_grad(torch.float32)
+    torch.cuda.empty_cache()
+    rel = lambda g: float(((g - g64).abs() / g64.abs()).max())
+    return {"ours_rel_err_vs_fp64": rel(grad), "torch_f32_rel_err_vs_fp64": rel(g32),
+            "grad": grad.tolist(), "grad_fp64": g64.tolist()}
 
 
 def run_ours(args, rank: int, world: int, local_rank: int):
@@ -612,8 +766,37 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         h.destroy()
         return
 
-    if only == "vendor":
-        leg = vendor_leg(args, torch, A0, B0, backward_error)
+    def mixed_solve_on(A, Bt, prec):
+        """One device-timed mixed solve of A X = B (A n x n symmetric, Bt nrhs x n) -> (ms, info, report, Xt)."""
+        Xt = torch.empty_like(Bt)
+        dA = desc(A.data_ptr(), n, n)
+        dB = desc(Bt.data_ptr(), n, nrhs)
+        dXo = desc(Xt.data_ptr(), n, nrhs)
+        info = ctypes.c_int(0)
+        rep = (ctypes.c_double * 4)()
+        Asave = A.clone()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        C.check_status(C.ddla_d_pposv_mixed(h.ptr, b"L", prec.encode(), n, nrhs, dA.data_ptr, dA.desc.ctypes.data,
+                                            dB.data_ptr, dB.desc.ctypes.data, dXo.data_ptr, dXo.desc.ctypes.data,
+                                            ctypes.byref(info), rep), "pposv_mixed")
+        e1.record(stream)
+        e1.synchronize()
+        A.copy_(Asave)  # the FP64 fallback leaves its factor in A
+        del Asave
+        return (e0.elapsed_time(e1), info.value,
+                {"iter": int(rep[0]), "gmres": int(rep[1]), "shift": rep[2], "backward_error": rep[3]}, Xt)
+
+    if only in ("vendor", "se-kernel", "kappa"):
+        if only == "vendor":
+            leg = vendor_leg(args, torch, A0, B0, backward_error)
+        elif only == "se-kernel":
+            del A0, Apristine
+            torch.cuda.empty_cache()
+            leg = se_kernel_leg(args, torch, device, h, stream, C)
+        else:
+            leg = kappa_leg(args, torch, device, h, stream, C, mixed_solve_on)
         if rank == 0:
             print(json.dumps({"only": only, only: leg}), flush=True)
         h.destroy()
@@ -739,6 +922,16 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                                   "traffic": traffic.get("k_syrk_dmma", {}).get("bytes_per_launch_at_bench"),
                                   "peak_source": "cuBLAS DGEMM 8192^3 best-of-5 measured in this run"}
         line["speedup_mixed_over_plain"] = head["value"] / plain["value"]
+    if not args.no_vendor:
+        line["vendor"] = vendor_leg(args, torch, A0, B0, backward_error)
+        line["vendor"]["plain_over_vendor"] = plain["value"] / line["vendor"]["value"] if plain else None
+        line["vendor"]["mixed_over_vendor"] = head["value"] / line["vendor"]["value"]
+    if not args.no_kappa:
+        line["kappa"] = kappa_leg(args, torch, device, h, stream, C, mixed_solve_on)
+    if not args.no_se:
+        del Apristine
+        torch.cuda.empty_cache()
+        line["se_kernel"] = se_kernel_leg(args, torch, device, h, stream, C)
     if not args.no_batched:
         line["batched"] = batched_leg(args, torch, device, h, stream, C)
     if not args.no_gp:
@@ -765,12 +958,17 @@ def main(argv=None):
     ap.add_argument("--cpu-budget", type=float, default=8.0,
                     help="seconds of CPU work per step of the reference arm's bounded sample")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-vendor", action="store_true")
+    ap.add_argument("--no-kappa", action="store_true")
+    ap.add_argument("--no-se", action="store_true")
+    ap.add_argument("--se-n", type=int, default=16384)
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-gp", action="store_true")
     ap.add_argument("--no-gp-large", action="store_true")
     ap.add_argument("--batched-count", type=int, default=4096)
     ap.add_argument("--gp-batch", type=int, default=256)
-    ap.add_argument("--only", choices=["mixed-B", "mixed-T", "plain", "batched", "gp", "gemm-vbatched", "vendor"],
+    ap.add_argument("--only", choices=["mixed-B", "mixed-T", "plain", "batched", "gp", "gemm-vbatched", "vendor",
+                                                 "se-kernel", "kappa"],
                     default=None,
                     help="run one leg alone (profiling driver); prints that leg's figures only")
     args = ap.parse_args(argv)

@@ -76,6 +76,19 @@ template <typename T>
 void pdiag_logdet(const DdlaHandle_t& handle, int n, const T* A, const int* descA,
                   std::complex<real_type_t<T>>& result);
 
+// pdiag_logdet on a pr x pc grid, split at the reference's one exchange step
+// (src/PBLAS/pdiag_logdet.cpp:41-47, an MPI_Allreduce of four doubles): rank
+// (row, col) computes state = {magnitude, phase, zero, negative parity,
+// nonfinite} over the diagonal entries its local matrix A holds (descA checked
+// against the pr x pc grid); the caller sums the five doubles over the ranks
+// (any all-reduce) and pdiag_logdet_finish turns the sums into log det, throwing
+// std::domain_error on every rank when any rank saw a nonfinite entry.  No
+// reference counterpart as separate entry points.
+template <typename T>
+void pdiag_logdet_local(const DdlaHandle_t& handle, int n, const T* A, const int* descA, int pr, int pc, int row,
+                        int col, double state[5]);
+void pdiag_logdet_finish(const double total[5], double& re, double& im);
+
 // A batch of GEMMs of differing sizes (reference ddla.h:1836-1849,
 // src/BLAS/gemm_vbatched.cpp:349-399): for b < batch_count,
 //   C_b = alpha op(A_b) op(B_b) + beta C_b,  op(A_b) d_m[b] x d_k[b],

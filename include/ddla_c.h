@@ -125,6 +125,23 @@ int ddla_s_pdiag_logdet(void* handle, int n, const void* A, const int* descA, vo
 int ddla_d_pdiag_logdet(void* handle, int n, const void* A, const int* descA, void* result);
 int ddla_c_pdiag_logdet(void* handle, int n, const void* A, const int* descA, void* result);
 int ddla_z_pdiag_logdet(void* handle, int n, const void* A, const int* descA, void* result);
+/* pdiag_logdet on a pr x pc grid, split at the reference's one exchange step
+ * (src/PBLAS/pdiag_logdet.cpp:41-47, MPI_Allreduce of four doubles; no C export
+ * there): ddla_?_pdiag_logdet_local writes this rank's state[5] = {magnitude,
+ * phase, zero, negative parity, nonfinite} over the diagonal entries its local
+ * matrix holds (descA checked against the pr x pc grid, rank (row, col)); the
+ * caller sums the five doubles over all ranks; ddla_c_pdiag_logdet_finish turns
+ * the sums into the log-determinant (result: two floats if single, else two
+ * doubles), status 6 "nonfinite diagonal" on every rank if any rank saw one. */
+int ddla_s_pdiag_logdet_local(void* handle, int n, const void* A, const int* descA, int pr, int pc, int row, int col,
+                              double* state);
+int ddla_d_pdiag_logdet_local(void* handle, int n, const void* A, const int* descA, int pr, int pc, int row, int col,
+                              double* state);
+int ddla_c_pdiag_logdet_local(void* handle, int n, const void* A, const int* descA, int pr, int pc, int row, int col,
+                              double* state);
+int ddla_z_pdiag_logdet_local(void* handle, int n, const void* A, const int* descA, int pr, int pc, int row, int col,
+                              double* state);
+int ddla_c_pdiag_logdet_finish(const double* total, int single, void* result);
 /* phegst (reference include/ddla/ddla.h:2560-2562, no C export there): the
  * type-1 Hermitian-definite reduction of A with the factor held in F */
 int ddla_s_phegst(void* handle, char uplo, int n, void* A, const int* descA, const void* F, const int* descF);
@@ -298,6 +315,21 @@ int ddla_d_gp_nll_grad_batched(void* handle, int batch, int n, int d, const doub
  * ddlak_profile_read in ddla_kernels.h). */
 int ddla_c_get_stream(void* handle, void** stream);
 long long ddla_c_launch_count(void);
+
+/* Testing aids for the failure paths (no reference counterpart in the C ABI;
+ * the reference injects allocation failures with an LD_PRELOAD shim,
+ * tests/pblas_alloc_failure.cpp, which cannot reach this library because it
+ * links the CUDA runtime statically).  ddla_c_fail_allocation(n) makes the
+ * n-th device or pinned allocation from now on (routine workspace,
+ * ddla_c_malloc, the handle's pinned word) fail as out of memory, once;
+ * n <= 0 disarms.  ddla_c_live_workspaces is the number of routine workspaces
+ * not yet released (0 between calls).  ddla_c_set_wait_budget sets the clock
+ * budget (SM cycles; <= 0 restores the default of about 2 s) after which a
+ * kernel's wait on another CTA's flag gives up and the routine reports a
+ * timeout, on the handle's device. */
+int ddla_c_fail_allocation(long long nth);
+long long ddla_c_live_workspaces(void);
+int ddla_c_set_wait_budget(void* handle, long long cycles);
 void ddla_c_profile_enable(int on);
 int ddla_c_profile_read(int kind, double* ms, long long* launches, double* flops, double* bytes, int reset);
 

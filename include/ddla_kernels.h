@@ -32,7 +32,7 @@ int ddlak_potrf(char type, char uplo, int n, void* A, long long lda, int* dinfo,
  * matrix is updated once per super-step with K = group * block width.
  * ddlak_potrf uses DDLAK_POTRF_GROUP; ddlak_potrf_grouped takes 1 ..
  * DDLAK_POTRF_MAX_GROUP (same results up to rounding). */
-#define DDLAK_POTRF_GROUP 2
+#define DDLAK_POTRF_GROUP 4
 #define DDLAK_POTRF_MAX_GROUP 8
 int ddlak_potrf_grouped(char type, char uplo, int group, int n, void* A, long long lda, int* dinfo, void* stream);
 
@@ -138,13 +138,22 @@ unsigned long long ddlak_logdet_workspace(void);
  * {double magnitude; double phase; int flags} at the start of work. */
 int ddlak_diag_logsum(char type, int n, const void* A, long long lda, void* work, void* stream);
 
+/* The same partial state over the diagonal entries that rank (row, col) of a
+ * pr x pc block-cyclic grid holds in its local matrix A (leading dimension lld,
+ * local_rows x local_cols; blocks mb x nb, source process (rsrc, csrc)), with
+ * the reference's item -> global-index mapping (src/diag_logdet_impl.h:55-74,
+ * src/PBLAS/pdiag_logdet.cpp:26-37).  Summing the ranks' states and finishing
+ * gives pdiag_logdet of the distributed matrix. */
+int ddlak_diag_logsum_grid(char type, int n, const void* A, long long lld, int local_rows, int local_cols, int mb,
+                           int nb, int pr, int pc, int row, int col, int rsrc, int csrc, void* work, void* stream);
+
 /* ---- mixed precision (ddla::pposv_mixed; no reference counterpart) ------ */
 
 /* Super-steps of the mixed factorization: block columns of 128 factored on the
  * look-ahead chain before one K = 128 * group trailing update of the rest
  * (ddlak_potrf_mixed uses DDLAK_MIXED_GROUP; ddlak_potrf_mixed_grouped takes
  * 1 .. DDLAK_MIXED_MAX_GROUP). */
-#define DDLAK_MIXED_GROUP 2
+#define DDLAK_MIXED_GROUP 4
 #define DDLAK_MIXED_MAX_GROUP 4
 
 /* Bytes of one of the two panel-operand slots of an order-n factorization
@@ -290,6 +299,15 @@ int ddlak_adjoint_contract(char type, int mode, int batch, int n, const void* W,
 
 /* Number of kernel launches the layer has made in this process. */
 long long ddlak_launch_count(void);
+
+/* Clock budget, in SM cycles, after which a kernel's wait on another CTA's flag
+ * gives up: the kernel records DDLAK_WAIT_TIMEOUT (1) in its status word and
+ * returns, and the host routine reports the timeout (std::runtime_error in the
+ * C++ API, status 6 in the C ABI).  cycles <= 0 restores the default, 4e9
+ * (about 2 s at 1.9 GHz).  Applies to the current device for every kernel of
+ * the library; synchronous with respect to the device. */
+int ddlak_set_wait_budget(long long cycles);
+long long ddlak_get_wait_budget(void);
 
 /* Per-kernel CUDA-event timing.  While enabled, every launcher brackets its
  * kernels with events on its stream and records the launch's algorithmic

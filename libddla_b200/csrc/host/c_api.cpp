@@ -136,6 +136,17 @@ int pdiag_logdet_impl(void* handle, int n, const void* A, const int* descA, void
 }
 
 template <class T>
+int pdiag_logdet_local_impl(void* handle, int n, const void* A, const int* descA, int pr, int pc, int row, int col,
+                            double* state)
+{
+    return run(handle, [&](ddla::DdlaHandle_t h) -> int {
+        if (state == nullptr) return ST_INVALID_VALUE;
+        ddla::pdiag_logdet_local<T>(h, n, static_cast<const T*>(A), descA, pr, pc, row, col, state);
+        return ST_SUCCESS;
+    });
+}
+
+template <class T>
 int gemm_vbatched_impl(void* handle, char ta, char tb, int* d_m, int* d_n, int* d_k, const void* alpha,
                        const void* const* d_A, int* d_lda, const void* const* d_B, int* d_ldb, const void* beta,
                        void** d_C, int* d_ldc, int batch_count)
@@ -497,6 +508,11 @@ int ddla_c_bcast_dims(int, int* m, int* n, int* type_char, int root)
     {                                                                                                                \
         return pdiag_logdet_impl<T>(handle, n, A, descA, result);                                                    \
     }                                                                                                                \
+    int ddla_##P##_pdiag_logdet_local(void* handle, int n, const void* A, const int* descA, int pr, int pc,       \
+                                      int row, int col, double* state)                                             \
+    {                                                                                                                \
+        return pdiag_logdet_local_impl<T>(handle, n, A, descA, pr, pc, row, col, state);                            \
+    }                                                                                                                \
     int ddla_##P##_gemm_vbatched(void* handle, char ta, char tb, int* d_m, int* d_n, int* d_k, const void* alpha,  \
                                  const void* const* d_A, int* d_lda, const void* const* d_B, int* d_ldb,             \
                                  const void* beta, void** d_C, int* d_ldc, int batch_count)                          \
@@ -594,6 +610,35 @@ int ddla_c_get_stream(void* handle, void** stream)
     return ST_SUCCESS;
 }
 long long ddla_c_launch_count(void) { return ddlak_launch_count(); }
+
+int ddla_c_pdiag_logdet_finish(const double* total, int single, void* result)
+{
+    if (total == nullptr || result == nullptr) return ST_INVALID_VALUE;
+    return guarded("ddla_c_pdiag_logdet_finish", [&]() -> int {
+        double re = 0, im = 0;
+        ddla::pdiag_logdet_finish(total, re, im);
+        if (single) {
+            const float r[2] = {static_cast<float>(re), static_cast<float>(im)};
+            std::memcpy(result, r, sizeof(r));
+        } else {
+            const double r[2] = {re, im};
+            std::memcpy(result, r, sizeof(r));
+        }
+        return ST_SUCCESS;
+    });
+}
+int ddla_c_fail_allocation(long long nth)
+{
+    ddla::detail::arm_allocation_failure(nth);
+    return ST_SUCCESS;
+}
+long long ddla_c_live_workspaces(void) { return ddla::detail::live_workspaces(); }
+int ddla_c_set_wait_budget(void* handle, long long cycles)
+{
+    if (handle == nullptr) return ST_INVALID_HANDLE;
+    if (cudaSetDevice(H(handle)->device) != cudaSuccess) return ST_INTERNAL_ERROR;
+    return ddlak_set_wait_budget(cycles) == 0 ? ST_SUCCESS : ST_INTERNAL_ERROR;
+}
 void ddla_c_profile_enable(int on) { ddlak_profile_enable(on); }
 int ddla_c_profile_read(int kind, double* ms, long long* launches, double* flops, double* bytes, int reset)
 {

@@ -365,7 +365,81 @@ void pdiag_logdet(const DdlaHandle_t& h, int n, const T* a, const int* desc, std
     logdet_core<T>(h, n, a, desc[DDLA_LLD_], result, "pdiag_logdet");
 }
 
+// One rank's share of pdiag_logdet on a pr x pc grid (src/PBLAS/pdiag_logdet.cpp:11-48):
+// the descriptor is checked against that grid (not the handle's), then the
+// DiagLogTerm / DiagLogJoin reduction runs over the diagonal entries the rank
+// holds.  state = {magnitude, phase, zero, negative parity, nonfinite}: the four
+// doubles the reference all-reduces (pdiag_logdet.cpp:41-45) plus the nonfinite
+// flag, which the reference raises on the rank that sees it before the
+// reduction; carried through the sum, it lets every rank raise together.
+template <typename T>
+void pdiag_logdet_local(const DdlaHandle_t& h, int n, const T* a, const int* desc, int pr, int pc, int row, int col,
+                        double state[5])
+{
+    detail::require_gpu(h, "pdiag_logdet");
+    if (desc == nullptr) throw std::invalid_argument("ddla: null ScaLAPACK descriptor");
+    if (pr <= 0 || pc <= 0 || row < 0 || row >= pr || col < 0 || col >= pc)
+        throw std::invalid_argument("pdiag_logdet: grid coordinates outside the grid");
+    if (desc[DDLA_DTYPE_] != DDLA_BLOCK_CYCLIC_2D || desc[DDLA_M_] < 0 || desc[DDLA_N_] < 0 || desc[DDLA_MB_] <= 0 ||
+        desc[DDLA_NB_] <= 0 || desc[DDLA_RSRC_] < 0 || desc[DDLA_RSRC_] >= pr || desc[DDLA_CSRC_] < 0 ||
+        desc[DDLA_CSRC_] >= pc)
+        throw std::invalid_argument("pdiag_logdet: descriptor does not describe a matrix on this grid");
+    const int rows = num_loc(desc[DDLA_M_], desc[DDLA_MB_], row, desc[DDLA_RSRC_], pr);
+    if (desc[DDLA_LLD_] < std::max(1, rows))
+        throw std::invalid_argument("pdiag_logdet: LLD_ smaller than the local row count");
+    if (n < 0 || n > desc[DDLA_M_] || n > desc[DDLA_N_])
+        throw std::invalid_argument("pdiag_logdet: order exceeds descriptor");
+    const int lr = num_loc(n, desc[DDLA_MB_], row, desc[DDLA_RSRC_], pr);
+    const int lc = num_loc(n, desc[DDLA_NB_], col, desc[DDLA_CSRC_], pc);
+    if (lr > 0 && lc > 0 && !a) throw std::invalid_argument("pdiag_logdet: null local matrix");
+    if (lr > 0 && lc > 0) {
+        const auto last = std::uint64_t(lc - 1) * std::uint64_t(desc[DDLA_LLD_]) + std::uint64_t(lr) - 1;
+        if (last > std::uint64_t(std::numeric_limits<std::ptrdiff_t>::max()) / sizeof(T))
+            throw std::overflow_error("pdiag_logdet: matrix address span is not representable");
+    }
+    struct {
+        double mag, phase;
+        int flags, pad;
+    } st{};
+    if (lr > 0 && lc > 0) {
+        detail::DeviceScratch work(h, static_cast<std::size_t>(ddlak_logdet_workspace()));
+        detail::kernel_check(ddlak_diag_logsum_grid(tcode<T>(), n, a, desc[DDLA_LLD_], lr, lc, desc[DDLA_MB_],
+                                                    desc[DDLA_NB_], pr, pc, row, col, desc[DDLA_RSRC_],
+                                                    desc[DDLA_CSRC_], work.data(), h->stream),
+                             "pdiag_logdet kernels");
+        detail::cuda_check(cudaMemcpyAsync(h->host_word, work.data(), sizeof(st), cudaMemcpyDeviceToHost, h->stream),
+                           "logdet read-back");
+        detail::cuda_check(cudaStreamSynchronize(h->stream), "stream synchronisation");
+        std::memcpy(&st, h->host_word, sizeof(st));
+    }
+    state[0] = st.mag;
+    state[1] = st.phase;
+    state[2] = double((st.flags & 2) != 0);
+    state[3] = double((st.flags & 4) != 0);
+    state[4] = double((st.flags & 1) != 0);
+}
+
+// finish_diagonal_log of the summed states (src/diag_logdet_impl.h:104-113;
+// pdiag_logdet.cpp:46-47): zero wins, else the negative-real parity adds pi and
+// the phase is wrapped to (-pi, pi]; a nonfinite entry on any rank throws.
+void pdiag_logdet_finish(const double total[5], double& re, double& im)
+{
+    if (total[4] != 0) throw std::domain_error("pdiag_logdet: nonfinite diagonal");
+    if (total[2] != 0) {
+        re = -std::numeric_limits<double>::infinity();
+        im = 0;
+        return;
+    }
+    const double pi = std::acos(-1.0);
+    double phase = std::remainder(total[1] + (static_cast<long long>(total[3]) & 1) * pi, 2 * pi);
+    if (phase <= -pi) phase = pi;
+    re = total[0];
+    im = phase;
+}
+
 #define DDLA_INSTANTIATE(T)                                                                                          \
+    template void pdiag_logdet_local<T>(const DdlaHandle_t&, int, const T*, const int*, int, int, int, int,          \
+                                        double*);                                                                    \
     template void ppotrf<T>(const DdlaHandle_t&, char, int, T*, int, int, const int*, int&);                         \
     template void ppotrs<T>(const DdlaHandle_t&, char, char, char, int, int, const T*, const int*, T*, const int*); \
     template void pposv<T>(const DdlaHandle_t&, char, char, char, int, int, T*, int, int, const int*, T*, int, int, \

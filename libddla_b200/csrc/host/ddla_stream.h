@@ -39,6 +39,7 @@ inline void cuda_check(cudaError_t e, const char* what)
 inline void kernel_check(int e, const char* what) { cuda_check(static_cast<cudaError_t>(e), what); }
 
 void require_gpu(const DdlaHandle_t& h, const char* routine);
+void note_workspace(int delta);
 void check_desc(const int* desc, const DdlaHandle_t& handle);
 void remember_cuda_error(cudaError_t e);
 
@@ -57,17 +58,35 @@ inline T* take(char*& cursor, std::size_t count)
     return p;
 }
 
+// Testing aid for the allocation-failure paths (the reference reaches them with
+// an LD_PRELOAD allocator shim, tests/pblas_alloc_failure.cpp; with the CUDA
+// runtime linked statically the shim cannot reach this library's calls, so
+// the hook sits at the library's own allocation points).  When armed with n,
+// the n-th device or pinned allocation from then on (workspace, ddlaMalloc,
+// ddlaMallocHost, the handle's pinned word) fails as cudaErrorMemoryAllocation
+// and the hook disarms.  live_workspaces() counts workspace allocations not
+// yet released.
+void arm_allocation_failure(long long nth);
+bool allocation_fails();
+long long live_workspaces();
+
 // Stream-ordered device scratch owned for the duration of one call
 // (the reference allocates per call with cudaMallocAsync, ddla_handle_t.cpp:322-338).
 class DeviceScratch {
 public:
     DeviceScratch(const DdlaHandle_t& h, std::size_t bytes) : h_(h), bytes_(bytes)
     {
-        if (bytes_) cuda_check(cudaMallocAsync(&p_, bytes_, h_->stream), "workspace allocation");
+        if (!bytes_) return;
+        if (allocation_fails()) cuda_check(cudaErrorMemoryAllocation, "workspace allocation");
+        cuda_check(cudaMallocAsync(&p_, bytes_, h_->stream), "workspace allocation");
+        note_workspace(+1);
     }
     ~DeviceScratch()
     {
-        if (p_) cudaFreeAsync(p_, h_->stream);
+        if (p_) {
+            cudaFreeAsync(p_, h_->stream);
+            note_workspace(-1);
+        }
     }
     DeviceScratch(const DeviceScratch&) = delete;
     DeviceScratch& operator=(const DeviceScratch&) = delete;

@@ -2,6 +2,7 @@
 // src/ddla_stream.cpp, restricted to a GPU handle on a 1x1 grid).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -47,6 +48,25 @@ bool is_device_pointer(const void* p)
 
 namespace detail {
 void remember_cuda_error(cudaError_t e) { g_last_cuda_message = cudaGetErrorString(e); }
+
+namespace {
+std::atomic<long long> g_alloc_countdown{0};  // 0: disarmed
+std::atomic<long long> g_live_workspaces{0};
+}  // namespace
+
+void arm_allocation_failure(long long nth) { g_alloc_countdown.store(nth > 0 ? nth : 0); }
+
+bool allocation_fails()
+{
+    long long c = g_alloc_countdown.load();
+    while (c > 0) {
+        if (g_alloc_countdown.compare_exchange_weak(c, c - 1)) return c == 1;
+    }
+    return false;
+}
+
+void note_workspace(int delta) { g_live_workspaces.fetch_add(delta); }
+long long live_workspaces() { return g_live_workspaces.load(); }
 
 void require_gpu(const DdlaHandle_t& h, const char* routine)
 {
@@ -124,7 +144,9 @@ static ddlaStatus_t set_impl(DdlaHandle_t handle, const MPI_Comm& comm, int npro
         const cudaError_t e2 = cudaStreamCreateWithFlags(&handle->stream, cudaStreamNonBlocking);
         if (e2 != cudaSuccess) return from_cuda(e2);
         handle->owns_stream = true;
-        const cudaError_t e3 = cudaMallocHost(reinterpret_cast<void**>(&handle->host_word), 64);
+        const cudaError_t e3 = detail::allocation_fails()
+                                   ? cudaErrorMemoryAllocation
+                                   : cudaMallocHost(reinterpret_cast<void**>(&handle->host_word), 64);
         if (e3 != cudaSuccess) {  // leave the handle as it was, so a retry starts clean
             cudaStreamDestroy(handle->stream);
             handle->stream = nullptr;
@@ -207,6 +229,7 @@ ddlaStatus_t ddlaMalloc(const DdlaHandle_t& handle, void** ptr, std::size_t byte
         *ptr = nullptr;
         return ddlaStatus_t::DDLA_STATUS_SUCCESS;
     }
+    if (detail::allocation_fails()) return from_cuda(cudaErrorMemoryAllocation);
     cudaSetDevice(handle->device);
     return from_cuda(cudaMallocAsync(ptr, bytes, handle->stream));
 }
@@ -224,6 +247,7 @@ ddlaStatus_t ddlaMallocHost(const DdlaHandle_t& handle, void** ptr, std::size_t 
         *ptr = nullptr;
         return ddlaStatus_t::DDLA_STATUS_SUCCESS;
     }
+    if (detail::allocation_fails()) return from_cuda(cudaErrorMemoryAllocation);
     return from_cuda(cudaMallocHost(ptr, bytes));
 }
 ddlaStatus_t ddlaFreeHost(const DdlaHandle_t& handle, void* ptr)

@@ -112,7 +112,22 @@ enum : int {
     DDLAK_WAIT_TIMEOUT = 1,
 };
 
-__device__ __forceinline__ long long wait_budget_cycles() { return 4000000000LL; }  // about 2 s at 1.9 GHz
+// The clock budget of a flag wait, in SM clock cycles (default 4e9, about 2 s at
+// 1.9 GHz).  Every translation unit holds its own copy; ddlak_set_wait_budget
+// sets all of them on the current device through the setters registered below.
+constexpr long long kDefaultWaitBudget = 4000000000LL;
+static __device__ long long g_wait_budget = kDefaultWaitBudget;
+__device__ __forceinline__ long long wait_budget_cycles() { return *(volatile const long long*)&g_wait_budget; }
+
+// Host side: registry of the per-translation-unit setters (profile.cu).
+bool register_wait_budget_setter(cudaError_t (*setter)(long long));
+namespace {
+inline cudaError_t set_tu_wait_budget(long long cycles)
+{
+    return cudaMemcpyToSymbol(g_wait_budget, &cycles, sizeof cycles);
+}
+[[maybe_unused]] const bool g_wait_budget_registered = register_wait_budget_setter(&set_tu_wait_budget);
+}  // namespace
 
 __device__ __forceinline__ int ld_acquire(const int* p)
 {
@@ -136,15 +151,18 @@ __device__ __forceinline__ void red_release_add(int* p, int v)
 __device__ __forceinline__ bool bounded_wait_geq(const int* flag, int want, int* status)
 {
     if (ld_acquire(flag) >= want) return true;
-    // a short tight spin first: the producer is usually microseconds away
-    for (int it = 0; it < 4096; ++it)
-        if (ld_acquire(flag) >= want) return true;
     const long long t0 = clock64();
+    const long long budget = wait_budget_cycles();
+    // a short tight spin first: the producer is usually microseconds away
+    for (int it = 0; it < 4096; ++it) {
+        if (ld_acquire(flag) >= want) return true;
+        if ((it & 63) == 63 && clock64() - t0 > budget) break;
+    }
     unsigned ns = 32;
     while (true) {
         if (ld_acquire(flag) >= want) return true;
         if (ld_acquire(status) != DDLAK_OK) return false;
-        if (clock64() - t0 > wait_budget_cycles()) {
+        if (clock64() - t0 > budget) {
             atomicCAS(status, DDLAK_OK, DDLAK_WAIT_TIMEOUT);
             return false;
         }

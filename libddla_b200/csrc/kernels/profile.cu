@@ -14,6 +14,7 @@
 #include <utility>
 #include <vector>
 
+#include "common.cuh"
 #include "profile.h"
 
 namespace ddlak {
@@ -46,6 +47,27 @@ cudaEvent_t get_event()
 void note_launches(int count) { g_launches.fetch_add(count, std::memory_order_relaxed); }
 
 bool profiling() { return g_on.load(std::memory_order_relaxed); }
+
+namespace {
+std::mutex& setter_mu()
+{
+    static std::mutex mu;
+    return mu;
+}
+std::vector<cudaError_t (*)(long long)>& setters()
+{
+    static std::vector<cudaError_t (*)(long long)> v;
+    return v;
+}
+std::atomic<long long> g_budget{4000000000LL};
+}  // namespace
+
+bool register_wait_budget_setter(cudaError_t (*setter)(long long))
+{
+    std::lock_guard<std::mutex> lk(setter_mu());
+    setters().push_back(setter);
+    return true;
+}
 
 cudaError_t smem_optin(const void* func, std::size_t bytes)
 {
@@ -119,3 +141,19 @@ extern "C" int ddlak_profile_read(int kind, double* ms, long long* launches, dou
     if (bytes) *bytes = b;
     return 0;
 }
+
+// Clock budget (SM cycles) after which a kernel's flag wait gives up and
+// records DDLAK_WAIT_TIMEOUT; cycles <= 0 restores the default (4e9, about
+// 2 s).  Applies to the current device, for every kernel of the library.
+extern "C" int ddlak_set_wait_budget(long long cycles)
+{
+    using namespace ddlak;
+    const long long c = cycles > 0 ? cycles : kDefaultWaitBudget;
+    std::lock_guard<std::mutex> lk(setter_mu());
+    for (auto f : setters())
+        if (cudaError_t e = f(c); e != cudaSuccess) return (int)e;
+    g_budget.store(c);
+    return 0;
+}
+
+extern "C" long long ddlak_get_wait_budget(void) { return ddlak::g_budget.load(); }

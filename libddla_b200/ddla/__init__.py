@@ -17,8 +17,9 @@ from .backend import Backend, Communication, Handle  # noqa: F401
 from .layout import ProcessorLayout  # noqa: F401
 from .matrix import DistributedMatrix  # noqa: F401
 from . import autograd, batched  # noqa: F401
-from .ops import (diag_logdet, gather, pdiag_logdet, phegst, potrf, potrf_bottom_right, pposv, pposv_mixed,  # noqa: F401
-                  ppotrf, ppotrf_bottom_right, ppotrs, scatter)
+from .ops import (diag_logdet, gather, pdiag_logdet, pdiag_logdet_finish, pdiag_logdet_grid,  # noqa: F401
+                  pdiag_logdet_local, phegst, potrf, potrf_bottom_right, pposv, pposv_mixed, ppotrf,
+                  ppotrf_bottom_right, ppotrs, scatter)
 
 
 def finalize():

@@ -137,6 +137,10 @@ _SIGS = {
     "ddla_d_pposv_mixed": (_i, [_vp, _c, _c, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _ip, _dp]),
     "ddla_c_get_stream": (_i, [_vp, ctypes.POINTER(_vp)]),
     "ddla_c_launch_count": (_ll, []),
+    "ddla_c_pdiag_logdet_finish": (_i, [_vp, _i, _vp]),
+    "ddla_c_fail_allocation": (_i, [_ll]),
+    "ddla_c_live_workspaces": (_ll, []),
+    "ddla_c_set_wait_budget": (_i, [_vp, _ll]),
     "ddla_c_profile_enable": (None, [_i]),
     "ddla_c_profile_read": (_i, [_i, _dp, _llp, _dp, _dp, _i]),
     "ddla_vbatched_plan_run": (_i, [_vp]),
@@ -164,6 +168,7 @@ for _p in "sdcz":
         f"ddla_{_p}_potrf": (_i, [_vp, _c, _i, _vp, _i, _vp]),
         f"ddla_{_p}_diag_logdet": (_i, [_vp, _i, _vp, _i, _vp]),
         f"ddla_{_p}_pdiag_logdet": (_i, [_vp, _i, _vp, _vp, _vp]),
+        f"ddla_{_p}_pdiag_logdet_local": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _i, _vp]),
         f"ddla_{_p}_potrf_bottom_right": (_i, [_vp, _c, _i, _vp, _i, _ip]),
         f"ddla_{_p}_ppotrf_bottom_right": (_i, [_vp, _c, _i, _vp, _vp, _ip]),
         f"ddla_{_p}_phegst": (_i, [_vp, _c, _i, _vp, _vp, _vp, _vp]),

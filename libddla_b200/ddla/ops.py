@@ -87,6 +87,49 @@ def pdiag_logdet(A: DistributedMatrix, n: int = -1) -> complex:
     return complex(float(out[0]), float(out[1]))
 
 
+def pdiag_logdet_local(handle, type_char: str, n: int, a_ptr: int, desc, grid) -> np.ndarray:
+    """This rank's pdiag_logdet state {magnitude, phase, zero, negative parity, nonfinite} over the
+    diagonal entries its local matrix (device pointer a_ptr, int[9] descriptor desc) holds, for rank
+    (row, col) of a pr x pc grid, grid = (pr, pc, row, col) (ddla_?_pdiag_logdet_local)."""
+    pr, pc, row, col = (int(v) for v in grid)
+    d = np.ascontiguousarray(desc, dtype=np.int32)
+    state = np.zeros(5, dtype=np.float64)
+    f = getattr(C.lib, f"ddla_{type_char}_pdiag_logdet_local")
+    C.check_status(f(handle.ptr, int(n), a_ptr, d.ctypes.data, pr, pc, row, col, state.ctypes.data),
+                   f"ddla_{type_char}_pdiag_logdet_local")
+    return state
+
+
+def pdiag_logdet_finish(total, single: bool = False) -> complex:
+    """log det from the states summed over every rank (ddla_c_pdiag_logdet_finish); raises on every
+    rank when any rank saw a nonfinite diagonal entry."""
+    t = np.ascontiguousarray(total, dtype=np.float64)
+    if t.shape != (5,):
+        raise ValueError("pdiag_logdet_finish: five summed doubles expected")
+    out = np.zeros(2, dtype=np.float32 if single else np.float64)
+    C.check_status(C.ddla_c_pdiag_logdet_finish(t.ctypes.data, int(bool(single)), out.ctypes.data),
+                   "ddla_c_pdiag_logdet_finish")
+    return complex(float(out[0]), float(out[1]))
+
+
+def pdiag_logdet_grid(handle, type_char: str, n: int, a_ptr: int, desc, grid, group=None,
+                      local_state=None) -> complex:
+    """pdiag_logdet of a matrix distributed block-cyclically over the ranks of a torch.distributed
+    group arranged as a pr x pc grid: this rank's state (ddla_?_pdiag_logdet_local, or `local_state`
+    when the caller already has it), ONE all-reduce (sum) of its five doubles -- the reference's
+    MPI_Allreduce of src/PBLAS/pdiag_logdet.cpp:45 -- and the finish.  Every rank of the group must
+    call it; all get the same result (or all raise)."""
+    import torch
+    import torch.distributed as dist
+
+    state = local_state if local_state is not None else pdiag_logdet_local(handle, type_char, n, a_ptr, desc, grid)
+    backend = dist.get_backend(group)
+    dev = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
+    t = torch.as_tensor(np.asarray(state, dtype=np.float64), device=dev).clone()
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return pdiag_logdet_finish(t.cpu().numpy(), single=type_char in "sc")
+
+
 def phegst(A: DistributedMatrix, F: DistributedMatrix, uplo: str = "L", n: int = -1) -> DistributedMatrix:
     """A <- L^-1 A L^-H in place with F holding the Cholesky factor of B (ddla_?_phegst;
     the reference's phegst on a 1x1 grid).  Returns A."""

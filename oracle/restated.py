@@ -215,3 +215,51 @@ def phegst(a: np.ndarray, factor: np.ndarray, uplo: str = "L", n: int | None = N
     herm_complete(w, uplo, n)
     a[:n, :n] = w.astype(a.dtype)
     return a
+
+
+def block_cyclic_local(a: np.ndarray, mb: int, nb: int, pr: int, pc: int, row: int, col: int,
+                       rsrc: int = 0, csrc: int = 0) -> np.ndarray:
+    """The local matrix rank (row, col) of a pr x pc grid holds of the global matrix a, ScaLAPACK
+    block-cyclic with mb x nb blocks from source process (rsrc, csrc): global (i, j) is local
+    (i // (mb pr) * mb + i % mb, j // (nb pc) * nb + j % nb) on the rank owning row block i // mb
+    and column block j // nb (the index maps of the reference's include/ddla/ddla_desc.h:10-38)."""
+    m, n = a.shape
+    rows = [i for i in range(m) if (rsrc + i // mb) % pr == row]
+    cols = [j for j in range(n) if (csrc + j // nb) % pc == col]
+    return np.asfortranarray(a[np.ix_(rows, cols)]) if rows and cols else np.zeros((len(rows), len(cols)), a.dtype)
+
+
+def diag_log_local_state(local: np.ndarray, n: int, mb: int, nb: int, pr: int, pc: int, row: int, col: int,
+                         rsrc: int = 0, csrc: int = 0) -> np.ndarray:
+    """One rank's pdiag_logdet state {magnitude, phase, zero, negative parity, nonfinite}: the
+    reference's DiagLogTerm over the items of its layout (src/diag_logdet_impl.h:50-94: items walk
+    the local rows when pr >= pc, else the local columns; item -> global g -> local entry; entries
+    of other ranks contribute nothing), joined in order by DiagLogJoin (:42-48)."""
+    along_rows = pr >= pc
+    lr, lc = local.shape
+    count = 0 if lr == 0 or lc == 0 else (lr if along_rows else lc)
+    block, peers = (mb, pr) if along_rows else (nb, pc)
+    coord, src = (row, rsrc) if along_rows else (col, csrc)
+    offset = (coord - src + peers) % peers
+    mag = phase = 0.0
+    flags = 0
+    for item in range(count):
+        g = (item // block * peers + offset) * block + item % block
+        if g >= n or (rsrc + g // mb) % pr != row or (csrc + g // nb) % pc != col:
+            continue
+        v = complex(local[g // (mb * pr) * mb + g % mb, g // (nb * pc) * nb + g % nb])
+        x, y = v.real, v.imag
+        if not (np.isfinite(x) and np.isfinite(y)):
+            t = (0.0, 0.0, 1)
+        else:
+            ax, ay = abs(x), abs(y)
+            hi, lo = max(ax, ay), min(ax, ay)
+            if hi == 0:
+                t = (0.0, 0.0, 2)
+            else:
+                m_ = float(np.log(hi) + 0.5 * np.log1p((lo / hi) ** 2))
+                t = (m_, 0.0, 4 if x < 0 else 0) if y == 0 else (m_, float(np.arctan2(y, x)), 0)
+        mag += t[0]
+        phase += t[1]
+        flags = ((flags | t[2]) & 3) | ((flags ^ t[2]) & 4)
+    return np.array([mag, phase, float(flags & 2 != 0), float(flags & 4 != 0), float(flags & 1 != 0)])
