@@ -32,7 +32,7 @@ int ddlak_potrf(char type, char uplo, int n, void* A, long long lda, int* dinfo,
  * matrix is updated once per super-step with K = group * block width.
  * ddlak_potrf uses DDLAK_POTRF_GROUP; ddlak_potrf_grouped takes 1 ..
  * DDLAK_POTRF_MAX_GROUP (same results up to rounding). */
-#define DDLAK_POTRF_GROUP 4
+#define DDLAK_POTRF_GROUP 8
 #define DDLAK_POTRF_MAX_GROUP 8
 int ddlak_potrf_grouped(char type, char uplo, int group, int n, void* A, long long lda, int* dinfo, void* stream);
 

@@ -40,6 +40,23 @@ __device__ __forceinline__ T shfl(T v, int src)
 
 namespace diagf {
 
+// 1/d for the pivots on the column chain: the hardware's approximate reciprocal
+// (rcp.approx.ftz.f64, about single precision) refined by two Newton-Raphson
+// steps r <- r + r (1 - d r), each of which squares the relative error, so the
+// result is within an ulp or two of 1/d for the positive normal pivots this is
+// used on (a non-positive pivot stops the factorization before its reciprocal
+// is used).  Cheaper on the chain than the correctly rounded division.
+__device__ __forceinline__ double recip_pivot(double d)
+{
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+    double e = fma(-d, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-d, r, 1.0);
+    return fma(r, e, r);
+}
+__device__ __forceinline__ float recip_pivot(float d) { return 1.0f / d; }
+
 constexpr int PW = 32;    // panel width
 constexpr int MAXN = 128;  // largest block
 constexpr int UP = (MAXN - PW) / 16;  // row groups of the trailing update (6)
@@ -58,7 +75,7 @@ __device__ __forceinline__ void panel_diag(T* s, int ld, int c0, int w, int lane
     for (int k = 0; k < PW; ++k) a[k] = (i < w && k <= i) ? s[(c0 + i) + (c0 + k) * ld] : zero<T>();
     // column 0 and its pivot's reciprocal
     colbuf[0][i] = a[0];
-    if (i == 0) s_inv[0] = R(1) / re(a[0]);
+    if (i == 0) s_inv[0] = recip_pivot(re(a[0]));
     __syncwarp();
     int fail = 0;
     R dpiv = R(0);
@@ -77,7 +94,10 @@ __device__ __forceinline__ void panel_diag(T* s, int ld, int c0, int w, int lane
                     // the next column first, so its publication overlaps the rest of the step
                     a[j + 1] = fms(a[j + 1], tj, cj(cv[j + 1]));
                     colbuf[(j + 1) & 1][i] = a[j + 1];
-                    if (i == j + 1) s_inv[(j + 1) & 1] = R(1) / re(a[j + 1]);
+                    // every lane takes its own reciprocal (no divergent branch on the chain);
+                    // lane j + 1's is the next pivot's
+                    const R rn = recip_pivot(re(a[j + 1]));
+                    if (i == j + 1) s_inv[(j + 1) & 1] = rn;
 #pragma unroll
                     for (int k = j + 2; k < PW; ++k) a[k] = fms(a[k], tj, cj(cv[k]));
                 }

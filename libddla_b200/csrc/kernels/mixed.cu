@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(256) k_pack_panel(const float* __restrict__ W,
 // [t0, t0+cols)).  128 threads: thread 0 issues TMA, thread 32 issues MMA,
 // all four warps run the epilogue on their 32 TMEM lanes.
 // ---------------------------------------------------------------------------
-constexpr int MU_STAGES = 2;
+constexpr int MU_STAGES = 2;  // 3 stages measured no faster, 4 slower (one CTA per SM)
 constexpr int MU_TILE_BYTES = 128 * 128;  // 128 rows x 128 bytes
 constexpr size_t MU_SMEM = (size_t)MU_STAGES * 2 * MU_TILE_BYTES + 1024;
 

@@ -17,6 +17,7 @@
 // positive definite (diagonal value <= 0 or NaN), 0 on success.  Every kernel
 // returns immediately once info is set, so the first failure is the one kept.
 #include <mutex>
+#include <type_traits>
 
 #include <ddla_kernels.h>
 
@@ -68,50 +69,73 @@ __global__ void __launch_bounds__(256) k_trsm_panel(T* __restrict__ A, long long
     __syncthreads();
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long row0 = (long long)k0 + nbk + ((long long)blockIdx.x * (blockDim.x >> 5) + warp) * PR;
-    if (row0 >= n) return;
-    T p[PR][NQ];
+    // persistent over row groups of 8 warps x PR rows: L11 is loaded once per CTA
+    const long long ngroups = ceil_div((long long)n - k0 - nbk, 8LL * PR);
+    for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+        const long long row0 = (long long)k0 + nbk + (grp * (blockDim.x >> 5) + warp) * PR;
+        if (row0 >= n) continue;
+        T p[PR][NQ];
 #pragma unroll
-    for (int r = 0; r < PR; ++r)
+        for (int r = 0; r < PR; ++r)
 #pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-            const long long i = row0 + r;
-            const int c = q * 32 + lane;
-            p[r][q] = (i < n && c < nbk) ? lview_ld<T, UP>(A, lda, i, k0 + c) : zero<T>();
-        }
+            for (int q = 0; q < NQ; ++q) {
+                const long long i = row0 + r;
+                const int c = q * 32 + lane;
+                p[r][q] = (i < n && c < nbk) ? lview_ld<T, UP>(A, lda, i, k0 + c) : zero<T>();
+            }
 
 #pragma unroll
-    for (int qj = 0; qj < NQ; ++qj) {
-        for (int jj = 0; jj < 32; ++jj) {
-            const int j = qj * 32 + jj;
-            if (j >= nbk) break;
-            const R rjj = s_rinv[j];
-            T x[PR];
+        for (int qj = 0; qj < NQ; ++qj) {
+            for (int jj = 0; jj < 32; ++jj) {
+                const int j = qj * 32 + jj;
+                if (j >= nbk) break;
+                const R rjj = s_rinv[j];
+                T x[PR];
 #pragma unroll
-            for (int r = 0; r < PR; ++r) {
-                const T v = scal(p[r][qj], rjj);
-                if (lane == jj) p[r][qj] = v;
-                x[r] = shfl(v, jj);
-            }
+                for (int r = 0; r < PR; ++r) {
+                    const T v = scal(p[r][qj], rjj);
+                    if (lane == jj) p[r][qj] = v;
+                    x[r] = shfl(v, jj);
+                }
 #pragma unroll
-            for (int q = qj; q < NQ; ++q) {
-                const int c = q * 32 + lane;
-                if (c > j) {
-                    const T lcj = cj(l11[c + j * ldl]);
+                for (int q = qj; q < NQ; ++q) {
+                    const int c = q * 32 + lane;
+                    if (c > j) {
+                        const T lcj = cj(l11[c + j * ldl]);
 #pragma unroll
-                    for (int r = 0; r < PR; ++r) p[r][q] = fms(p[r][q], x[r], lcj);
+                        for (int r = 0; r < PR; ++r) p[r][q] = fms(p[r][q], x[r], lcj);
+                    }
                 }
             }
         }
+#pragma unroll
+        for (int r = 0; r < PR; ++r)
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+                const long long i = row0 + r;
+                const int c = q * 32 + lane;
+                if (i < n && c < nbk) lview_st<T, UP>(A, lda, i, k0 + c, p[r][q]);
+            }
     }
-#pragma unroll
-    for (int r = 0; r < PR; ++r)
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-            const long long i = row0 + r;
-            const int c = q * 32 + lane;
-            if (i < n && c < nbk) lview_st<T, UP>(A, lda, i, k0 + c, p[r][q]);
-        }
+}
+
+// Grid of the panel solve: every row group once, at most as many CTAs as fit on
+// the device at once (the kernel loops over row groups).
+template <class K>
+long long trsm_grid(K* kernel, size_t smem, long long groups)
+{
+    static std::mutex mu;
+    static int cap[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return groups;
+    std::lock_guard<std::mutex> lk(mu);
+    if (cap[dev] == 0) {
+        int sms = 148, per = 1;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 256, smem);
+        cap[dev] = sms * (per > 0 ? per : 1);
+    }
+    return groups < cap[dev] ? groups : cap[dev];
 }
 
 // ---------------------------------------------------------------------------
@@ -221,7 +245,8 @@ cudaError_t launch_trsm_panel(T* A, long long lda, int k0, int nbk, int n, const
     if (cudaError_t e = smem_optin(k_trsm_panel<T, UP, NQ, PR>, panel_smem); e != cudaSuccess) return e;
     const double cf = Traits<T>::cplx ? 4.0 : 1.0, md = (double)m, b = nbk;
     ProfScope ps(PK_TRSM_PANEL, s, cf * md * b * b, sizeof(T) * (2.0 * md * b + b * (b + 1) / 2));
-    k_trsm_panel<T, UP, NQ, PR><<<(unsigned)ceil_div(m, 8 * PR), 256, panel_smem, s>>>(A, lda, k0, nbk, n, dinfo);
+    const long long grid = trsm_grid(k_trsm_panel<T, UP, NQ, PR>, panel_smem, ceil_div(m, 8 * PR));
+    k_trsm_panel<T, UP, NQ, PR><<<(unsigned)grid, 256, panel_smem, s>>>(A, lda, k0, nbk, n, dinfo);
     note_launches(1);
     return cudaGetLastError();
 }
@@ -277,8 +302,8 @@ static cudaError_t potrf_enqueue(T* A, long long lda, int n, int G, int* dinfo, 
         const double md = (double)m;
         {
             ProfScope ps(PK_TRSM_PANEL, s, cf * md * b * b, sizeof(T) * (2.0 * md * b + b * (b + 1) / 2));
-            k_trsm_panel<T, UP, NQ, PR><<<(unsigned)ceil_div(m, 8 * PR), 256, panel_smem, s>>>(A, lda, k0, nbk, n,
-                                                                                                dinfo);
+            const long long grid = trsm_grid(k_trsm_panel<T, UP, NQ, PR>, panel_smem, ceil_div(m, 8 * PR));
+            k_trsm_panel<T, UP, NQ, PR><<<(unsigned)grid, 256, panel_smem, s>>>(A, lda, k0, nbk, n, dinfo);
         }
         note_launches(1);
     };
