@@ -26,6 +26,7 @@
 
 #include "common.cuh"
 #include "profile.h"
+#include "tc_common.cuh"
 
 namespace ddlak {
 namespace {
@@ -445,11 +446,226 @@ int trtri_t(int batch, int n, const void* L, long long ldl, long long lstride, v
     return (int)cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// The FP64 contraction (not DIRECT) on the FP64 tensor cores: the same tiles
+// and epilogues, C(i, j) = sum_k W(k, i) W(k, j) by DMMA (mma.sync m8n8k4 f64,
+// 8 warps of 64 x 32).  Operand slices arrive by TMA from the batch of W seen as
+// a 3-D tensor: per stage the columns i0 .. i0+127 and j0 .. j0+127 over 32 k,
+// as boxes of 36 k (the 4 extra pad the shared rows to 36 doubles, which keeps
+// the fragment reads conflict free) x 128 columns, 3 stages.  W's strictly upper
+// triangle is not written by the inversion, so the chunks that reach it (k <
+// i0 + 128) are masked in shared memory.  A stage's arrival wait is bounded: if
+// it gives up the tile's result is NaN (the gradient comes back NaN) after a
+// bounded wait for the copies still in flight.
+// ---------------------------------------------------------------------------
+constexpr int AD_BK = 32, AD_LDK = 36, AD_NS = 3;
+constexpr int AD_BOX = CT_TILE * AD_LDK;
+constexpr unsigned AD_BOX_BYTES = AD_BOX * 8u;  // 36864
+constexpr size_t AD_SMEM = (size_t)AD_NS * 2 * AD_BOX_BYTES + 128;
+
+__device__ int g_adjoint_status;
+
+__device__ __forceinline__ void dmma_f64(double& d0, double& d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(CT_NT, 1)
+    k_adjoint_contract_dmma(const __grid_constant__ CUtensorMap wmap, int n, const double* __restrict__ alpha_g,
+                            long long astride, const double* __restrict__ X, int d, long long xstride,
+                            const double* __restrict__ theta, int tstride, double* __restrict__ partial,
+                            double* __restrict__ G, long long ldg, long long gstride)
+{
+    extern __shared__ __align__(128) unsigned char ad_raw[];
+    __shared__ __align__(8) uint64_t full[AD_NS];
+    __shared__ double red[3][CT_NT / 32];
+    const int m = blockIdx.y, tile = blockIdx.x;
+    int ti, tj;
+    tile_of_lower(tile, ti, tj);
+    const int i0 = ti * CT_TILE, j0 = tj * CT_TILE;
+    double* sm = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(ad_raw) + 127) & ~uintptr_t(127));
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int wm = warp >> 2, wn = warp & 3;
+    const int g = lane >> 2, q = lane & 3;
+    const int kbeg = i0, nch = (n - kbeg + AD_BK - 1) / AD_BK;
+    auto issue = [&](int c) {
+        const int s = c % AD_NS;
+        double* st = sm + (size_t)s * 2 * AD_BOX;
+        tc::mbar_expect_tx(&full[s], 2 * AD_BOX_BYTES);
+        tc::tma_load_3d(st, &wmap, &full[s], kbeg + c * AD_BK, i0, m);
+        tc::tma_load_3d(st + AD_BOX, &wmap, &full[s], kbeg + c * AD_BK, j0, m);
+    };
+    if (t == 0) {
+        for (int s = 0; s < AD_NS; ++s) tc::mbar_init(&full[s], 1);
+        tc::mbar_fence_init();
+        tc::prefetch_tmap(&wmap);
+        for (int c = 0; c < AD_NS && c < nch; ++c) issue(c);
+    }
+    __syncthreads();
+    double acc[8][4][2];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    bool ok = true;
+    int consumed = 0;
+    for (int c = 0; c < nch; ++c) {
+        const int s = c % AD_NS;
+        ok = __syncthreads_and(tc::mbar_wait(&full[s], (uint32_t)((c / AD_NS) & 1), &g_adjoint_status, 0x61));
+        if (!ok) break;
+        consumed = c + 1;
+        double* Wi = sm + (size_t)s * 2 * AD_BOX;
+        double* Wj = Wi + AD_BOX;
+        const int k0 = kbeg + c * AD_BK;
+        if (k0 < i0 + CT_TILE) {
+            // zero W(k, col) for k < col (the unwritten upper triangle) in this chunk
+            for (int e = t; e < CT_TILE * AD_BK; e += CT_NT) {
+                const int cl = e / AD_BK, kl = e % AD_BK;
+                if (k0 + kl < i0 + cl) Wi[cl * AD_LDK + kl] = 0.0;
+                if (ti == tj && k0 + kl < j0 + cl) Wj[cl * AD_LDK + kl] = 0.0;
+            }
+            tc::fence_proxy_async_smem();
+            __syncthreads();
+        }
+#pragma unroll
+        for (int kk = 0; kk < AD_BK; kk += 4) {
+            double af[8], bf[4];
+#pragma unroll
+            for (int a = 0; a < 8; ++a) af[a] = Wi[(wm * 64 + a * 8 + g) * AD_LDK + kk + q];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) bf[b] = Wj[(wn * 32 + b * 8 + g) * AD_LDK + kk + q];
+#pragma unroll
+            for (int a = 0; a < 8; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) dmma_f64(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+        }
+        __syncthreads();
+        if (t == 0 && c + AD_NS < nch) issue(c + AD_NS);
+    }
+    if (!ok) {
+        if (t == 0)
+            for (int c = consumed; c < nch && c < consumed + AD_NS; ++c)
+                (void)tc::mbar_wait(&full[c % AD_NS], (uint32_t)((c / AD_NS) & 1), &g_adjoint_status, 0x62);
+        __syncthreads();
+        const double nan = __longlong_as_double(0x7ff8000000000000LL);
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = nan;
+    }
+    const double* al = alpha_g + m * astride;
+    auto row_of = [&](int a) { return i0 + wm * 64 + a * 8 + g; };
+    auto col_of = [&](int b, int e) { return j0 + wn * 32 + b * 8 + 2 * q + e; };
+    if constexpr (MODE == 1) {
+        double* gm = G + m * gstride;
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int i = row_of(a), j = col_of(b, e);
+                    if (i < n && j <= i) {
+                        const double ab = 0.5 * (acc[a][b][e] - al[i] * al[j]);
+                        gm[i + (long long)j * ldg] = ab;
+                        gm[j + (long long)i * ldg] = ab;
+                    }
+                }
+    } else {
+        const double* th = theta + (long long)m * tstride;
+        const double l = th[0], sf2 = th[1];
+        const double inv2l2 = 0.5 / (l * l), invl3 = 1.0 / (l * l * l);
+        const double* x = X + m * xstride;
+        double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            const int i = row_of(a);
+            if (i >= n) continue;
+            const double ai = al[i];
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int j = col_of(b, e);
+                    if (j > i) continue;
+                    const double ab = 0.5 * (acc[a][b][e] - ai * al[j]);
+                    const double w = i == j ? 1.0 : 2.0;
+                    double r2 = 0.0;
+                    for (int cc = 0; cc < d; ++cc) {
+                        const double dx = x[(long long)i * d + cc] - x[(long long)j * d + cc];
+                        r2 += dx * dx;
+                    }
+                    const double ex = exp(-r2 * inv2l2);
+                    g0 += w * ab * sf2 * ex * r2 * invl3;  // dA/dl
+                    g1 += w * ab * ex;                     // dA/dsigma_f^2
+                    if (i == j) g2 += ab;                  // dA/dsigma^2
+                }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            g0 += __shfl_xor_sync(0xffffffffu, g0, o);
+            g1 += __shfl_xor_sync(0xffffffffu, g1, o);
+            g2 += __shfl_xor_sync(0xffffffffu, g2, o);
+        }
+        if (lane == 0) {
+            red[0][warp] = g0;
+            red[1][warp] = g1;
+            red[2][warp] = g2;
+        }
+        __syncthreads();
+        if (t < 3) {
+            double sum = 0.0;
+            for (int w = 0; w < CT_NT / 32; ++w) sum += red[t][w];
+            partial[((long long)m * gridDim.x + tile) * 3 + t] = sum;
+        }
+    }
+}
+
+// The DMMA contraction when W's layout suits TMA (16-byte aligned base, even
+// ldw and matrix stride); false (nothing launched) otherwise.
+bool contract_dmma(int mode, int batch, int n, const double* W, long long ldw, long long wstride, const double* alpha,
+                   long long astride, const double* X, int d, long long xstride, const double* theta, int tstride,
+                   double* partial, double* grad, double* G, long long ldg, long long gstride, cudaStream_t st,
+                   cudaError_t* err)
+{
+    CUtensorMap wmap;
+    if (!tc::encode_colmajor_3d(&wmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, W, n, n, ldw, batch, wstride, AD_LDK,
+                                CT_TILE))
+        return false;
+    const int nt = (n + CT_TILE - 1) / CT_TILE;
+    const int ntiles = nt * (nt + 1) / 2;
+    dim3 grid(ntiles, batch);
+    if (mode == 0) {
+        if ((*err = smem_optin(k_adjoint_contract_dmma<0>, AD_SMEM)) != cudaSuccess) return true;
+        k_adjoint_contract_dmma<0><<<grid, CT_NT, AD_SMEM, st>>>(wmap, n, alpha, astride, X, d, xstride, theta,
+                                                                 tstride, partial, nullptr, 0, 0);
+        k_adjoint_reduce<<<batch, 32, 0, st>>>(ntiles, partial, grad);
+        note_launches(2);
+    } else {
+        if ((*err = smem_optin(k_adjoint_contract_dmma<1>, AD_SMEM)) != cudaSuccess) return true;
+        k_adjoint_contract_dmma<1><<<grid, CT_NT, AD_SMEM, st>>>(wmap, n, alpha, astride, nullptr, 0, 0, nullptr, 0,
+                                                                 nullptr, G, ldg, gstride);
+        note_launches(1);
+    }
+    *err = cudaGetLastError();
+    return true;
+}
+
 template <class T, bool DIRECT>
 int contract_t(int mode, int batch, int n, const void* W, long long ldw, long long wstride, const void* alpha,
                long long astride, const void* X, int d, long long xstride, const double* theta, int tstride,
                double* partial, double* grad, void* G, long long ldg, long long gstride, cudaStream_t st)
 {
+    if constexpr (std::is_same<T, double>::value && !DIRECT) {
+        cudaError_t e = cudaSuccess;
+        if (contract_dmma(mode, batch, n, static_cast<const double*>(W), ldw, wstride,
+                          static_cast<const double*>(alpha), astride, static_cast<const double*>(X), d, xstride, theta,
+                          tstride, partial, grad, static_cast<double*>(G), ldg, gstride, st, &e))
+            return (int)e;
+    }
     const int nt = (n + CT_TILE - 1) / CT_TILE;
     const int ntiles = nt * (nt + 1) / 2;
     dim3 grid(ntiles, batch);
@@ -494,7 +710,7 @@ extern "C" int ddlak_trtri_batched(char type, int batch, int n, const void* L, l
     if (n > TR_NMAX || !L || !W || ldl < n || ldw < n) return (int)cudaErrorInvalidValue;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const double nn = n;
-    ProfScope ps(PK_ADJOINT, st, batch * nn * nn * nn / 3.0, batch * nn * nn * (type == 'd' ? 8.0 : 4.0));
+    ProfScope ps(PK_TRTRI, st, batch * nn * nn * nn / 3.0, batch * nn * nn * (type == 'd' ? 8.0 : 4.0));
     if (type == 'd') return trtri_t<double>(batch, n, L, ldl, lstride, W, ldw, wstride, st);
     if (type == 's') return trtri_t<float>(batch, n, L, ldl, lstride, W, ldw, wstride, st);
     return (int)cudaErrorInvalidValue;

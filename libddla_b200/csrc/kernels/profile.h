@@ -18,7 +18,8 @@ enum ProfKind : int {
     PK_SYMM_RESIDUAL = 7,
     PK_BATCHED = 8,
     PK_ADJOINT = 9,
-    PK_COUNT = 10
+    PK_TRTRI = 10,
+    PK_COUNT = 11
 };
 
 void note_launches(int count);

@@ -49,6 +49,38 @@ inline bool encode_colmajor_2d(CUtensorMap* map, CUtensorMapDataType dt, int esi
               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Host: a 3-D tiled TMA map over a batch of column-major matrices: `rows` x
+// `cols` elements of `esize` bytes, columns `ld` elements apart, matrices
+// `mstride` elements apart, `batch` of them; box box_rows x box_cols x 1, zero
+// fill outside.  False when the entry point is missing or the encoding is
+// rejected (alignment of the base, of ld and of mstride to 16 bytes, ...).
+inline bool encode_colmajor_3d(CUtensorMap* map, CUtensorMapDataType dt, int esize, const void* p, long long rows,
+                               long long cols, long long ld, long long batch, long long mstride, int box_rows,
+                               int box_cols)
+{
+    using Fn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+                            const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                            CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static Fn fn = [] {
+        void* q = nullptr;
+        cudaDriverEntryPointQueryResult r;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &q, cudaEnableDefault, &r) == cudaSuccess &&
+            r == cudaDriverEntryPointSuccess)
+            return reinterpret_cast<Fn>(q);
+        return static_cast<Fn>(nullptr);
+    }();
+    if (!fn || (reinterpret_cast<uintptr_t>(p) & 15) || ((ld * esize) & 15) || ((mstride * esize) & 15) || rows < 1 ||
+        cols < 1 || batch < 1)
+        return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)rows, (cuuint64_t)cols, (cuuint64_t)batch};
+    const cuuint64_t strides[2] = {(cuuint64_t)(ld * esize), (cuuint64_t)(mstride * esize)};
+    const cuuint32_t box[3] = {(cuuint32_t)box_rows, (cuuint32_t)box_cols, 1u};
+    const cuuint32_t estr[3] = {1u, 1u, 1u};
+    return fn(map, dt, 3, const_cast<void*>(p), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // ---- mbarrier ---------------------------------------------------------------
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
 {
@@ -88,6 +120,14 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
         "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
             smem_u32(dst)),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::
+            "r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
         : "memory");
 }
 // Prefetch a 2-D box into L2 (no shared-memory destination, no completion)
