@@ -103,6 +103,27 @@ def householder_spd_host(n: int, kappa: float, seed: int) -> np.ndarray:
     return A
 
 
+def householder_spd_host_lower(n: int, kappa: float, seed: int) -> np.ndarray:
+    """The same family as householder_spd_host, column-major, with only the lower triangle
+    defined (the upper one is zero): each reflector is one symmetric matrix-vector product
+    and one symmetric rank-2 update, H A H = A - beta (v w'^T + w' v^T) with w = A v and
+    w' = w - (beta v^T w / 2) v, through the multithreaded BLAS, so that full-size
+    matrices (n = 32768, 8.6 GB) take seconds and no n x n temporaries."""
+    import scipy.linalg.blas as blas
+
+    rng = np.random.default_rng(seed)
+    s = float(kappa) ** (-np.arange(n) / max(1, n - 1))
+    A = np.zeros((n, n), dtype=np.float64, order="F")
+    A[np.arange(n), np.arange(n)] = s
+    vs = [rng.standard_normal(n) for _ in range(4)]
+    for v in reversed(vs):
+        beta = 2.0 / float(v @ v)
+        w = blas.dsymv(1.0, A, v, lower=1)
+        w = w - (0.5 * beta * float(v @ w)) * v
+        A = blas.dsyr2(-beta, v, w, lower=1, a=A, overwrite_a=1)
+    return A
+
+
 def batched_sizes(count: int, seed: int, lo=16, hi=512) -> np.ndarray:
     return np.random.default_rng(seed).integers(lo, hi + 1, size=count)
 

@@ -2,7 +2,8 @@
 of the path timed on the host cores.  It runs without a GPU, so its JSON line is
 checked here: one line from rank 0 with the metric, unit and direction of the
 GPU arm, a cpu_baseline block describing the sample, an e2e block with no
-host-device traffic; other ranks print nothing and exit 0."""
+host-device traffic, and every timed step a full solve of the GPU arm's
+workload (here at n = 2048 to keep the test short); other ranks print nothing and exit 0."""
 import json
 import os
 import subprocess
@@ -16,7 +17,7 @@ def _run(env_extra):
     env = dict(os.environ)
     env.update(env_extra)
     return subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0",
-                           "--cpu-budget", "0.5"],
+                           "--n", "2048"],
                           cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
 
 
@@ -36,7 +37,9 @@ def test_reference_arm_prints_one_contract_line():
     assert cb["cores"] >= 1 and "dpotrf" in cb["sample"]
     e = d["e2e"]
     assert e["value"] == d["value"] and e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
-    assert d["config"]["workload"].startswith("pposv d n=")
+    # the GPU arm's workload string: the same configuration, timed at full size
+    assert d["config"]["workload"] == "pposv d uplo=L n=2048 nrhs=8 A=U diag(s) U^T kappa=1e+06"
+    assert "1 full solves at n=2048" in cb["sample"]
 
 
 def test_reference_arm_other_ranks_are_silent():

@@ -19,6 +19,11 @@ def test_householder_family_spectrum(kappa):
         ev = np.linalg.eigvalsh(A)
         assert np.allclose(ev, s, rtol=1e-9, atol=1e-13), (kappa, ev[:3], s[:3])
         assert abs(ev[-1] / ev[0] / kappa - 1) < 1e-4
+    # the reference arm's full-size generator: the same matrix, lower triangle only
+    Lw = W.householder_spd_host_lower(n, kappa, 0xDD1A0003)
+    assert Lw.flags.f_contiguous and not np.triu(Lw, 1).any()
+    Af = W.householder_spd_host(n, kappa, 0xDD1A0003)
+    assert np.allclose(np.tril(Af), Lw, rtol=0, atol=1e-15)
     a = W.householder_spd(n, kappa, 7, device="cpu")
     assert bool((a == W.householder_spd(n, kappa, 7, device="cpu")).all())
 
