@@ -5,7 +5,10 @@
 // memory 130-204, synchronisation 252-300, grid accessors 307-337,
 // DDLA_CHECK 343-352).  This library is built for B200 GPUs only: the GPU
 // backend is available when a CUDA device is visible, the CPU backend is never
-// available (there is no CPU fallback), and the process grid is 1x1.
+// available (there is no CPU fallback).  Without MPI in this build, a process
+// grid of more than one rank is formed by ddlaSetLocalGroup (ranks that are
+// threads of one process) or ddlaSetNccl (ranks that are processes joined by
+// NCCL); ddlaSet itself serves the 1x1 grid.
 #ifndef DDLA_HANDLE_T_H
 #define DDLA_HANDLE_T_H
 
@@ -41,6 +44,25 @@ ddlaStatus_t ddlaInit(DdlaHandle_t& handle, DdlaBackend requested_backend);
 ddlaStatus_t ddlaSet(DdlaHandle_t handle, const MPI_Comm& comm = MPI_COMM_WORLD, char major = 'R');
 ddlaStatus_t ddlaSet(DdlaHandle_t handle, const MPI_Comm& comm, int nprows, int npcols, char major = 'R');
 ddlaStatus_t ddlaDestroy(DdlaHandle_t& handle);
+
+// Process grids of more than one rank, one rank per GPU (the handle's device),
+// rank -> (row, col) by `major` as ddlaRankToRc.  Every rank of the grid calls
+// the distributed routines (ppotrf, ppotrs side 'L', pposv side 'L',
+// pdiag_logdet) with its local block-cyclic piece and the common descriptor.
+//   Local group: the ranks are threads of this process.  A collective whose
+//   members do not all arrive within timeout_s seconds raises
+//   std::runtime_error on the ranks that wait, and the group is then unusable.
+//   NCCL: the ranks are processes; rank 0 makes the clique id with
+//   ddlaNcclUniqueId and every rank passes the same 128 bytes.
+struct DdlaLocalGroup;
+ddlaStatus_t ddlaLocalGroupCreate(DdlaLocalGroup** group, int nranks, double timeout_s = 120.0);
+ddlaStatus_t ddlaLocalGroupDestroy(DdlaLocalGroup* group);
+ddlaStatus_t ddlaSetLocalGroup(DdlaHandle_t handle, DdlaLocalGroup* group, int rank, int nprows, int npcols,
+                               char major = 'R');
+bool ddlaNcclAvailable();
+ddlaStatus_t ddlaNcclUniqueId(void* id128);
+ddlaStatus_t ddlaSetNccl(DdlaHandle_t handle, const void* id128, int nranks, int rank, int nprows, int npcols,
+                         char major = 'R');
 
 bool ddlaBackendAvailable(DdlaBackend backend);
 DdlaBackend ddlaGetBackend(const DdlaHandle_t& handle);
@@ -85,7 +107,8 @@ const char* ddlaGetErrorString(ddlaStatus_t status);
 ddlaStatus_t ddlaSetStream(const DdlaHandle_t& handle, void* stream);
 void* ddlaGetStream(const DdlaHandle_t& handle);
 
-// Grid accessors (always the 1x1 grid of rank 0).
+// Grid accessors.  The communicators are the single-rank stand-in of this build;
+// the grid itself is the handle's (1x1 after ddlaSet).
 MPI_Comm ddlaGetCommunicator(const DdlaHandle_t& handle);
 MPI_Comm ddlaGetRowCommunicator(const DdlaHandle_t& handle);
 MPI_Comm ddlaGetColCommunicator(const DdlaHandle_t& handle);

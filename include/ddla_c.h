@@ -27,6 +27,17 @@ const char* ddla_c_error_string(int status);                                  /*
 int ddla_c_init_backend(void** handle, int backend);                          /* ddla_c_api.cpp:100 */
 int ddla_c_set(void* handle, int f_comm, int nprows, int npcols, char major); /* ddla_c_api.cpp:115 */
 int ddla_c_set_communication(void* handle, int communication);                /* ddla_c_api.cpp:134 */
+/* Process grids of more than one rank (the reference forms them from an MPI
+ * communicator, ddla_c_api.cpp:115 / src/ddla_handle_t.cpp:94-201; MPI is not
+ * part of this build).  A local group joins ranks that are threads of this
+ * process, one handle per rank; NCCL joins ranks that are processes (rank 0
+ * makes the 128-byte clique id, every rank passes it).  Additive entry points. */
+int ddla_c_local_group_create(void** group, int nranks, double timeout_s);
+int ddla_c_local_group_destroy(void* group);
+int ddla_c_set_local_group(void* handle, void* group, int rank, int nprows, int npcols, char major);
+int ddla_c_nccl_available(void);
+int ddla_c_nccl_unique_id(void* id128);
+int ddla_c_set_nccl(void* handle, const void* id128, int nranks, int rank, int nprows, int npcols, char major);
 int ddla_c_get_communication(void* handle, int* communication);               /* ddla_c_api.cpp:144 */
 int ddla_c_communication_available(void* handle, int communication);          /* ddla_c_api.cpp:156 */
 int ddla_c_destroy(void** handle);                                            /* ddla_c_api.cpp:165 */

@@ -319,6 +319,39 @@ long long ddlak_get_wait_budget(void);
 void ddlak_profile_enable(int on);
 int ddlak_profile_read(int kind, double* ms, long long* launches, double* flops, double* bytes, int reset);
 
+
+/* ---- distributed (P x Q grid) Cholesky and solve: local steps -------------
+ * Index map of a block-cyclically distributed dimension: local index l goes to
+ * ((L / nb) * nprocs + (coord - src) mod nprocs) * nb + L mod nb - base with
+ * L = first + l (ScaLAPACK's local-to-global map, offset); nprocs == 0 is the
+ * identity l -> l.  A NULL map is the identity. */
+typedef struct {
+    int first, coord, src, nprocs, nb;
+    long long base;
+} ddlak_gmap;
+
+/* C(i,j) = beta C(i,j) + alpha sum_p opA(i,p) opB(p,j) on an m x n C, contraction k,
+ * opA(i,p) = A[ma(i) + p lda] ('N') or conj(A[ma(p) + i lda]) ('C'),
+ * opB(p,j) = B[mb(p) + j ldb] ('N') or conj(B[mb(j) + p ldb]) ('C'),
+ * mask 0: all of C; 1: only where mi(i) >= mj(j); 2: only where mi(i) <= mj(j).
+ * alpha, beta: {re, im}; beta NULL writes C without reading it.  The trailing
+ * update (herk / gemm / gemmBatched on stored tiles) of src/Cholesky/ppotrf.cpp:196-317
+ * and the block updates of src/PBLAS/ptrtrs.cpp:209-224 on a grid. */
+int ddlak_grid_gemm(char type, char opA, char opB, int mask, int m, int n, int k, const double* alpha, const void* A,
+                    long long lda, const ddlak_gmap* ma, const void* B, long long ldb, const ddlak_gmap* mb,
+                    const double* beta, void* C, long long ldc, const ddlak_gmap* mi, const ddlak_gmap* mj,
+                    void* stream);
+/* dst(i,j) = src(i,j), or conj(src(j,i)) when conj_trans, for i < rows, j < cols. */
+int ddlak_grid_pack(char type, int conj_trans, int rows, int cols, const void* src, long long lds, void* dst,
+                    long long ldd, void* stream);
+/* dst(map(l), c) = src(l, c) for l < rows, c < cols. */
+int ddlak_grid_unscatter(char type, int rows, int cols, const void* src, long long lds, void* dst, long long ldd,
+                         const ddlak_gmap* map, void* stream);
+/* W = I (n x n). */
+int ddlak_grid_identity(char type, int n, void* W, long long ldw, void* stream);
+/* dst[e] += src[e], e < count reals ('s' float, 'd' double). */
+int ddlak_grid_accumulate(char real_type, unsigned long long count, const void* src, void* dst, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -75,6 +75,8 @@ int gather_impl(void* handle, int m, int n, const void* A, int ia, int ja, const
         ddla::detail::check_desc(descA, h);
         if (m < 0 || n < 0 || ia < 1 || ja < 1 || ia - 1 + m > descA[ddla::DDLA_M_] || ja - 1 + n > descA[ddla::DDLA_N_])
             throw std::invalid_argument("gather: invalid extents or offsets");
+        if (h->nprocs > 1)
+            throw std::invalid_argument("gather: served on a 1x1 grid only (on a grid every rank copies its local piece)");
         if (root != 0) throw std::invalid_argument("gather: root outside the 1x1 grid");
         if (m == 0 || n == 0) return ST_SUCCESS;
         if (!A || !dst || lddst < m) throw std::invalid_argument("gather: null pointer or short leading dimension");
@@ -95,6 +97,8 @@ int scatter_impl(void* handle, int m, int n, void* A, int ia, int ja, const int*
         ddla::detail::check_desc(descA, h);
         if (m < 0 || n < 0 || ia < 1 || ja < 1 || ia - 1 + m > descA[ddla::DDLA_M_] || ja - 1 + n > descA[ddla::DDLA_N_])
             throw std::invalid_argument("scatter: invalid extents or offsets");
+        if (h->nprocs > 1)
+            throw std::invalid_argument("scatter: served on a 1x1 grid only (on a grid every rank copies its local piece)");
         if (root != 0) throw std::invalid_argument("scatter: root outside the 1x1 grid");
         if (m == 0 || n == 0) return ST_SUCCESS;
         if (!A || !src || ldsrc < m) throw std::invalid_argument("scatter: null pointer or short leading dimension");
@@ -313,6 +317,48 @@ int ddla_c_set(void* handle, int f_comm, int nprows, int npcols, char major)
         if (nprows > 0 && npcols > 0) st = ddla::ddlaSet(H(handle), comm, nprows, npcols, major);
         else st = ddla::ddlaSet(H(handle), comm, major);
         return static_cast<int>(st);
+    });
+}
+
+int ddla_c_local_group_create(void** group, int nranks, double timeout_s)
+{
+    return guarded("ddla_c_local_group_create", [&]() -> int {
+        if (group == nullptr) return ST_INVALID_VALUE;
+        ddla::DdlaLocalGroup* g = nullptr;
+        const ddla::ddlaStatus_t st = ddla::ddlaLocalGroupCreate(&g, nranks, timeout_s);
+        *group = g;
+        return static_cast<int>(st);
+    });
+}
+
+int ddla_c_local_group_destroy(void* group)
+{
+    return guarded("ddla_c_local_group_destroy", [&]() -> int {
+        return static_cast<int>(ddla::ddlaLocalGroupDestroy(static_cast<ddla::DdlaLocalGroup*>(group)));
+    });
+}
+
+int ddla_c_set_local_group(void* handle, void* group, int rank, int nprows, int npcols, char major)
+{
+    return guarded("ddla_c_set_local_group", [&]() -> int {
+        if (handle == nullptr) return ST_INVALID_HANDLE;
+        return static_cast<int>(ddla::ddlaSetLocalGroup(H(handle), static_cast<ddla::DdlaLocalGroup*>(group), rank,
+                                                        nprows, npcols, major));
+    });
+}
+
+int ddla_c_nccl_available(void) { return ddla::ddlaNcclAvailable() ? 1 : 0; }
+
+int ddla_c_nccl_unique_id(void* id128)
+{
+    return guarded("ddla_c_nccl_unique_id", [&]() -> int { return static_cast<int>(ddla::ddlaNcclUniqueId(id128)); });
+}
+
+int ddla_c_set_nccl(void* handle, const void* id128, int nranks, int rank, int nprows, int npcols, char major)
+{
+    return guarded("ddla_c_set_nccl", [&]() -> int {
+        if (handle == nullptr) return ST_INVALID_HANDLE;
+        return static_cast<int>(ddla::ddlaSetNccl(H(handle), id128, nranks, rank, nprows, npcols, major));
     });
 }
 

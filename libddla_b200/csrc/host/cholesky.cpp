@@ -22,6 +22,7 @@
 #include <ddla_kernels.h>
 
 #include "ddla_stream.h"
+#include "grid.h"
 
 namespace ddla {
 
@@ -86,7 +87,7 @@ void ppotrf_bottom_right_check(const DdlaHandle_t& h, char uplo, int n, const vo
     detail::check_desc(d, h);
     detail::require_gpu(h, "ppotrf_bottom_right");
     if ((uplo != 'L' && uplo != 'U') || n < 0 || n > d[DDLA_M_] || n > d[DDLA_N_] || d[DDLA_MB_] != d[DDLA_NB_] ||
-        h->nprows_ != h->npcols_)
+        h->nprows_ != h->npcols_ || h->nprocs > 1)
         throw std::invalid_argument("ppotrf_bottom_right: invalid triangle, dimensions, blocks or grid");
     if (n && !A) throw std::invalid_argument("ppotrf_bottom_right: null local matrix");
 }
@@ -119,6 +120,10 @@ void ppotrf_run(const DdlaHandle_t& h, char uplo, int n, T* A, int, int, const i
         info = 0;
         return;
     }
+    if (h->nprocs > 1) {  // a grid of several ranks: the distributed factorization (its own scratch)
+        grid::ppotrf_grid<T>(h, uplo, n, A, descA, info);
+        return;
+    }
     if (backend_bytes < detail::padded_bytes<int>(1) || backend_work == nullptr)
         throw std::invalid_argument("ppotrf: workspace smaller than ppotrf_workspace_size");
     char* w = static_cast<char*>(backend_work);
@@ -141,6 +146,10 @@ void ppotrs_run(const DdlaHandle_t& h, char side, char uplo, char, int n, int nr
                 T* B, const int* descB, void* backend_work, std::size_t backend_bytes, void*, std::size_t)
 {
     if (n == 0 || nrhs == 0) return;
+    if (h->nprocs > 1) {  // a grid of several ranks: the distributed solve (its own scratch)
+        grid::ppotrs_grid<T>(h, side, uplo, n, nrhs, A, descA, B, descB);
+        return;
+    }
     const unsigned long long need = ddlak_potrs_workspace(n, nrhs);
     if (backend_bytes < need || backend_work == nullptr)
         throw std::invalid_argument("ppotrs: workspace smaller than ppotrs_workspace_size");
@@ -351,9 +360,10 @@ void diag_logdet(const DdlaHandle_t& h, int n, const T* a, int lda, std::complex
     logdet_core<T>(h, n, a, lda, result, "diag_logdet");
 }
 
-// The descriptor form (src/PBLAS/pdiag_logdet.cpp:11-48) on a 1x1 grid: the local
+// The descriptor form (src/PBLAS/pdiag_logdet.cpp:11-48).  On a 1x1 grid the local
 // block is the whole matrix and the all-reduce of the four partial sums is the
-// identity, so the result is diag_logdet's with LLD_ as the leading dimension.
+// identity, so the result is diag_logdet's with LLD_ as the leading dimension; on a
+// grid of several ranks every rank's state is summed over the grid (grid.cpp).
 template <typename T>
 void pdiag_logdet(const DdlaHandle_t& h, int n, const T* a, const int* desc, std::complex<real_type_t<T>>& result)
 {
@@ -361,6 +371,13 @@ void pdiag_logdet(const DdlaHandle_t& h, int n, const T* a, const int* desc, std
     detail::check_desc(desc, h);
     if (n < 0 || n > desc[DDLA_M_] || n > desc[DDLA_N_])
         throw std::invalid_argument("pdiag_logdet: order exceeds descriptor");
+    if (h->nprocs > 1) {  // every rank's local state, summed over the grid, finished on every rank
+        double total[5], re = 0, im = 0;
+        grid::pdiag_logdet_grid<T>(h, n, a, desc, total);
+        pdiag_logdet_finish(total, re, im);
+        result = std::complex<real_type_t<T>>(static_cast<real_type_t<T>>(re), static_cast<real_type_t<T>>(im));
+        return;
+    }
     if (n > 0 && !a) throw std::invalid_argument("pdiag_logdet: null local matrix");
     logdet_core<T>(h, n, a, desc[DDLA_LLD_], result, "pdiag_logdet");
 }

@@ -11,6 +11,10 @@
 
 #include <ddla/ddla_handle_t.h>
 
+#include <memory>
+
+#include "grid_comm.h"
+
 namespace ddla {
 
 class DdlaStream {
@@ -26,6 +30,8 @@ public:
     int nprows_ = 1, npcols_ = 1, myprow_ = 0, mypcol_ = 0, rank = 0, nprocs = 1;
     char major = 'R';
     int host_threads = 1;
+    // collectives of a grid of more than one rank (null on a 1x1 grid)
+    std::shared_ptr<detail::GridComm> grid;
 };
 
 namespace detail {

@@ -2,6 +2,9 @@
 // src/ddla_stream.cpp, restricted to a GPU handle on a 1x1 grid).
 #include <cuda_runtime.h>
 
+#include <functional>
+#include <memory>
+
 #include <atomic>
 #include <cstring>
 #include <mutex>
@@ -128,16 +131,9 @@ ddlaStatus_t ddlaInit(DdlaHandle_t& handle, DdlaBackend requested_backend)
     return ddlaStatus_t::DDLA_STATUS_SUCCESS;
 }
 
-static ddlaStatus_t set_impl(DdlaHandle_t handle, const MPI_Comm& comm, int nprows, int npcols, char major)
+// The handle's stream and pinned word, created once (the first ddlaSet*).
+static ddlaStatus_t ensure_resources(DdlaHandle_t handle)
 {
-    if (handle == nullptr) return ddlaStatus_t::DDLA_STATUS_INVALID_HANDLE;
-    if (major != 'R' && major != 'C') return ddlaStatus_t::DDLA_STATUS_INVALID_VALUE;
-#ifndef DDLA_SINGLE_RANK_MPI
-    int size = 1;
-    MPI_Comm_size(comm, &size);
-    if (size != 1) return ddlaStatus_t::DDLA_STATUS_BACKEND_UNAVAILABLE;
-#endif
-    if (nprows * npcols != 1) return ddlaStatus_t::DDLA_STATUS_BACKEND_UNAVAILABLE;
     if (!handle->initialized) {
         const cudaError_t e1 = cudaSetDevice(handle->device);
         if (e1 != cudaSuccess) return from_cuda(e1);
@@ -164,6 +160,21 @@ static ddlaStatus_t set_impl(DdlaHandle_t handle, const MPI_Comm& comm, int npro
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
         }
     }
+    return ddlaStatus_t::DDLA_STATUS_SUCCESS;
+}
+
+static ddlaStatus_t set_impl(DdlaHandle_t handle, const MPI_Comm& comm, int nprows, int npcols, char major)
+{
+    if (handle == nullptr) return ddlaStatus_t::DDLA_STATUS_INVALID_HANDLE;
+    if (major != 'R' && major != 'C') return ddlaStatus_t::DDLA_STATUS_INVALID_VALUE;
+#ifndef DDLA_SINGLE_RANK_MPI
+    int size = 1;
+    MPI_Comm_size(comm, &size);
+    if (size != 1) return ddlaStatus_t::DDLA_STATUS_BACKEND_UNAVAILABLE;
+#endif
+    if (nprows * npcols != 1) return ddlaStatus_t::DDLA_STATUS_BACKEND_UNAVAILABLE;
+    if (const ddlaStatus_t e = ensure_resources(handle); e != ddlaStatus_t::DDLA_STATUS_SUCCESS) return e;
+    handle->grid.reset();
     handle->comm = comm;
     handle->nprows_ = handle->npcols_ = 1;
     handle->myprow_ = handle->mypcol_ = 0;
@@ -181,6 +192,84 @@ ddlaStatus_t ddlaSet(DdlaHandle_t handle, const MPI_Comm& comm, int nprows, int 
     return set_impl(handle, comm, nprows, npcols, major);
 }
 
+// ---- grids of more than one rank -------------------------------------------
+struct DdlaLocalGroup {
+    std::shared_ptr<detail::LocalGroup> g;
+};
+
+ddlaStatus_t ddlaLocalGroupCreate(DdlaLocalGroup** group, int nranks, double timeout_s)
+{
+    if (group == nullptr || nranks < 1) return ddlaStatus_t::DDLA_STATUS_INVALID_VALUE;
+    *group = new DdlaLocalGroup{detail::make_local_group(nranks, timeout_s)};
+    return ddlaStatus_t::DDLA_STATUS_SUCCESS;
+}
+
+ddlaStatus_t ddlaLocalGroupDestroy(DdlaLocalGroup* group)
+{
+    delete group;  // the members' handles keep the group alive until they are destroyed
+    return ddlaStatus_t::DDLA_STATUS_SUCCESS;
+}
+
+static ddlaStatus_t set_grid(DdlaHandle_t handle, int rank, int nprows, int npcols, char major,
+                             const std::function<std::unique_ptr<detail::GridComm>()>& make)
+{
+    if (handle == nullptr) return ddlaStatus_t::DDLA_STATUS_INVALID_HANDLE;
+    if ((major != 'R' && major != 'C') || nprows <= 0 || npcols <= 0 || rank < 0 || rank >= nprows * npcols)
+        return ddlaStatus_t::DDLA_STATUS_INVALID_VALUE;
+    const cudaError_t e = cudaSetDevice(handle->device);
+    if (e != cudaSuccess) return from_cuda(e);
+    if (const ddlaStatus_t s = ensure_resources(handle); s != ddlaStatus_t::DDLA_STATUS_SUCCESS) return s;
+    std::shared_ptr<detail::GridComm> comm;
+    if (nprows * npcols > 1) comm = make();
+    handle->grid = std::move(comm);
+    handle->comm = MPI_COMM_WORLD;
+    handle->nprows_ = nprows;
+    handle->npcols_ = npcols;
+    handle->major = major;
+    handle->rank = rank;
+    handle->nprocs = nprows * npcols;
+    if (major == 'C') {
+        handle->myprow_ = rank % nprows;
+        handle->mypcol_ = rank / nprows;
+    } else {
+        handle->myprow_ = rank / npcols;
+        handle->mypcol_ = rank % npcols;
+    }
+    handle->initialized = true;
+    return ddlaStatus_t::DDLA_STATUS_SUCCESS;
+}
+
+ddlaStatus_t ddlaSetLocalGroup(DdlaHandle_t handle, DdlaLocalGroup* group, int rank, int nprows, int npcols,
+                               char major)
+{
+    if (group == nullptr || nprows * npcols != detail::local_group_size(*group->g)) return ddlaStatus_t::DDLA_STATUS_INVALID_VALUE;
+    if (handle == nullptr) return ddlaStatus_t::DDLA_STATUS_INVALID_HANDLE;
+    const int dev = handle->device;
+    return set_grid(handle, rank, nprows, npcols, major,
+                    [&] { return detail::make_local_comm(group->g, rank, nprows, npcols, major, dev); });
+}
+
+bool ddlaNcclAvailable() { return detail::nccl_available(); }
+
+ddlaStatus_t ddlaNcclUniqueId(void* id128)
+{
+    if (id128 == nullptr) return ddlaStatus_t::DDLA_STATUS_INVALID_VALUE;
+    if (!detail::nccl_available()) return ddlaStatus_t::DDLA_STATUS_BACKEND_UNAVAILABLE;
+    detail::nccl_unique_id(id128);
+    return ddlaStatus_t::DDLA_STATUS_SUCCESS;
+}
+
+ddlaStatus_t ddlaSetNccl(DdlaHandle_t handle, const void* id128, int nranks, int rank, int nprows, int npcols,
+                         char major)
+{
+    if (id128 == nullptr || nprows * npcols != nranks) return ddlaStatus_t::DDLA_STATUS_INVALID_VALUE;
+    if (nranks > 1 && !detail::nccl_available()) return ddlaStatus_t::DDLA_STATUS_BACKEND_UNAVAILABLE;
+    if (handle == nullptr) return ddlaStatus_t::DDLA_STATUS_INVALID_HANDLE;
+    const int dev = handle->device;
+    return set_grid(handle, rank, nprows, npcols, major,
+                    [&] { return detail::make_nccl_comm(id128, nranks, rank, nprows, npcols, major, dev); });
+}
+
 ddlaStatus_t ddlaDestroy(DdlaHandle_t& handle)
 {
     if (handle == nullptr) return ddlaStatus_t::DDLA_STATUS_SUCCESS;
@@ -188,6 +277,7 @@ ddlaStatus_t ddlaDestroy(DdlaHandle_t& handle)
     if (s->initialized || s->stream || s->host_word) {
         cudaSetDevice(s->device);
         if (s->stream) cudaStreamSynchronize(s->stream);
+        s->grid.reset();
         if (s->owns_stream && s->stream) cudaStreamDestroy(s->stream);
         if (s->host_word) cudaFreeHost(s->host_word);
     }
@@ -403,16 +493,26 @@ void ddlaGetGridDims(const DdlaHandle_t& handle, int& nprows, int& npcols)
     nprows = handle && handle->initialized ? handle->nprows_ : 0;
     npcols = handle && handle->initialized ? handle->npcols_ : 0;
 }
+// rank <-> (row, col), row-major for 'R' and column-major for 'C' (src/ddla_stream.h:114-125);
+// -1 outside the grid
 void ddlaRankToRc(const DdlaHandle_t& handle, int rank, int& row, int& col)
 {
-    (void)handle;
-    row = rank == 0 ? 0 : -1;
-    col = rank == 0 ? 0 : -1;
+    row = col = -1;
+    if (handle == nullptr || !handle->initialized || rank < 0 || rank >= handle->nprocs) return;
+    if (handle->major == 'C') {
+        row = rank % handle->nprows_;
+        col = rank / handle->nprows_;
+    } else {
+        row = rank / handle->npcols_;
+        col = rank % handle->npcols_;
+    }
 }
 int ddlaRcToRank(const DdlaHandle_t& handle, int row, int col)
 {
-    (void)handle;
-    return row == 0 && col == 0 ? 0 : -1;
+    if (handle == nullptr || !handle->initialized || row < 0 || col < 0 || row >= handle->nprows_ ||
+        col >= handle->npcols_)
+        return -1;
+    return handle->major == 'C' ? col * handle->nprows_ + row : row * handle->npcols_ + col;
 }
 
 }  // namespace ddla

@@ -50,6 +50,7 @@ void phegst(const DdlaHandle_t& handle, char uplo, int n, T* A, const int* descA
 {
     if (handle == nullptr) throw std::runtime_error("phegst: null handle");
     detail::require_gpu(handle, "phegst");
+    if (handle->nprocs > 1) throw std::invalid_argument("phegst: served on a 1x1 grid only");
     const char up = static_cast<char>(std::toupper(static_cast<unsigned char>(uplo)));
     if (n < 0 || n > INT_MAX / 8 || (up != 'L' && up != 'U'))
         throw std::invalid_argument("phegst: invalid order or triangle");

@@ -56,6 +56,7 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
     detail::check_desc(descB, h);
     detail::check_desc(descX, h);
     detail::require_gpu(h, "pposv_mixed");
+    if (h->nprocs > 1) throw std::invalid_argument("pposv_mixed: served on a 1x1 grid only");
     if (uplo != 'L' || (precision != 'B' && precision != 'T' && precision != 'D') || n < 0 || nrhs < 0 ||
         n > descA[DDLA_M_] || n > descA[DDLA_N_] || n > descB[DDLA_M_] || nrhs > descB[DDLA_N_] ||
         n > descX[DDLA_M_] || nrhs > descX[DDLA_N_])

@@ -16,7 +16,7 @@ from ._c_api import (  # noqa: F401
 from .backend import Backend, Communication, Handle  # noqa: F401
 from .layout import ProcessorLayout  # noqa: F401
 from .matrix import DistributedMatrix  # noqa: F401
-from . import autograd, batched  # noqa: F401
+from . import autograd, batched, grid  # noqa: F401
 from .ops import (diag_logdet, gather, pdiag_logdet, pdiag_logdet_finish, pdiag_logdet_grid,  # noqa: F401
                   pdiag_logdet_local, phegst, potrf, potrf_bottom_right, pposv, pposv_mixed, ppotrf,
                   ppotrf_bottom_right, ppotrs, scatter)

@@ -111,6 +111,12 @@ _SIGS = {
     "ddla_c_error_string": (ctypes.c_char_p, [_i]),
     "ddla_c_init_backend": (_i, [ctypes.POINTER(_vp), _i]),
     "ddla_c_set": (_i, [_vp, _i, _i, _i, _c]),
+    "ddla_c_local_group_create": (_i, [ctypes.POINTER(_vp), _i, ctypes.c_double]),
+    "ddla_c_local_group_destroy": (_i, [_vp]),
+    "ddla_c_set_local_group": (_i, [_vp, _vp, _i, _i, _i, _c]),
+    "ddla_c_nccl_available": (_i, []),
+    "ddla_c_nccl_unique_id": (_i, [_vp]),
+    "ddla_c_set_nccl": (_i, [_vp, _vp, _i, _i, _i, _i, _c]),
     "ddla_c_set_communication": (_i, [_vp, _i]),
     "ddla_c_get_communication": (_i, [_vp, _ip]),
     "ddla_c_communication_available": (_i, [_vp, _i]),

@@ -23,14 +23,39 @@ class Communication(enum.IntEnum):
 
 
 class Handle:
-    """Owns one ddla handle: backend, 1x1 process grid and the CUDA stream."""
+    """Owns one ddla handle: backend, process grid and the CUDA stream.
+
+    The grid is 1x1 by default.  A grid of several ranks (one rank per GPU, this
+    handle's current device) is joined with `local_group` (a grid.LocalGroup: the
+    ranks are threads of this process) or `nccl_id` (the 128-byte clique id from
+    grid.nccl_unique_id on rank 0: the ranks are processes), with `rank` and
+    `nprows` x `npcols`."""
 
     def __init__(self, backend: Backend, layout: Optional[ProcessorLayout] = None, comm=None,
-                 nprows: Optional[int] = None, npcols: Optional[int] = None, major: str = "R"):
+                 nprows: Optional[int] = None, npcols: Optional[int] = None, major: str = "R",
+                 local_group=None, nccl_id: Optional[bytes] = None, rank: int = 0):
         self._handle = ctypes.c_void_p()
         if backend is None:
             raise TypeError("backend must explicitly select CPU or GPU")
         C.check_status(C.ddla_c_init_backend(ctypes.byref(self._handle), int(backend)), "ddla_c_init_backend")
+        if local_group is not None or nccl_id is not None:
+            if nprows is None or npcols is None:
+                self.destroy()
+                raise ValueError("a grid of several ranks needs nprows and npcols")
+            self.layout = None
+            if local_group is not None:
+                st = C.ddla_c_set_local_group(self._handle, local_group.ptr, int(rank), int(nprows), int(npcols),
+                                              major.encode())
+                what = "ddla_c_set_local_group"
+            else:
+                idbuf = ctypes.create_string_buffer(bytes(nccl_id), 128)
+                st = C.ddla_c_set_nccl(self._handle, idbuf, int(nprows) * int(npcols), int(rank), int(nprows),
+                                       int(npcols), major.encode())
+                what = "ddla_c_set_nccl"
+            if st != C.STATUS_SUCCESS:
+                self.destroy()
+            C.check_status(st, what)
+            return
         if layout is None:
             layout = ProcessorLayout(comm=comm, np_rows=nprows, np_cols=npcols, major=major)
         self.layout = layout
