@@ -3,11 +3,12 @@
 // This is the work the reference hands to cuSOLVER inside ?potrf
 // (src/Cholesky/potrf.cpp:111) and, on multi-rank grids, to herk/gemm
 // (src/Cholesky/ppotrf.cpp:212-238).  For double it runs on the FP64 tensor
-// cores: mma.sync m8n8k4 f64 (DMMA).  Each CTA owns one 128x128 lower tile of
-// the region, streams the two 128 x nbk panel slices through a cp.async
-// 3-stage ring in 16-wide k chunks, and keeps its accumulators in registers
-// (8 warps, each a 64x32 sub-tile = 8x4 DMMA fragments).  Diagonal tiles store
-// only i >= j.  Other types use the SIMT kernel in potrf.cu.
+// cores: mma.sync m16n8k4 f64 (DMMA).  Each CTA owns one 128x128 lower tile of
+// the region, streams the two 128 x nbk panel slices through a 3-stage ring in
+// k chunks (cp.async, or TMA boxes), and keeps its accumulators in registers
+// (8 warps, each a 64x32 sub-tile = 4x4 DMMA fragments of 16x8).  Diagonal tiles
+// store only i >= j.  Complex double runs as two real DMMA products per
+// fragment; float and complex float use the SIMT kernel in potrf.cu.
 #include <cuda.h>
 
 #include "common.cuh"
@@ -36,11 +37,16 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int byt
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
+// D += A B over k = 4 on the FP64 tensor cores, for two 8-row blocks at once
+// (mma.sync m16n8k4 f64): lane (g = lane / 4, q = lane % 4) supplies A(g, q) and
+// A(g + 8, q) -- the rows of its upper and lower 8-row block -- and B(q, g), and
+// holds D(g, 2q + e) in u[e] and D(g + 8, 2q + e) in v[e].  The same fragments as
+// two m8n8k4 products on the two blocks, in half the instructions.
+__device__ __forceinline__ void dmma2(double (&u)[2], double (&v)[2], double a_up, double a_lo, double b)
 {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
-                 : "+d"(d0), "+d"(d1)
-                 : "d"(a), "d"(b));
+    asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+                 : "+d"(u[0]), "+d"(u[1]), "+d"(v[0]), "+d"(v[1])
+                 : "d"(a_up), "d"(a_lo), "d"(b));
 }
 
 // One k chunk (16 columns of the panel) of the A rows [ri, ri+128) and the B
@@ -139,9 +145,9 @@ __global__ void __launch_bounds__(256, 1) k_syrk_dmma(double* __restrict__ A, lo
 #pragma unroll
             for (int b = 0; b < 4; ++b) bf[b] = Bs[(kk + q) * DM_LDS + wn * 32 + b * 8 + g];
 #pragma unroll
-            for (int a = 0; a < 8; ++a)
+            for (int a = 0; a < 8; a += 2)
 #pragma unroll
-                for (int b = 0; b < 4; ++b) dmma(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+                for (int b = 0; b < 4; ++b) dmma2(acc[a][b], acc[a + 1][b], af[a], af[a + 1], bf[b]);
         }
         __syncthreads();
     }
@@ -261,9 +267,9 @@ __global__ void __launch_bounds__(256, 1) k_syrk_dmma_tma(const __grid_constant_
 #pragma unroll
             for (int b = 0; b < 4; ++b) bf[b] = Bs[(kk + q) * DT_LDS + wn * 32 + b * 8 + g];
 #pragma unroll
-            for (int a = 0; a < 8; ++a)
+            for (int a = 0; a < 8; a += 2)
 #pragma unroll
-                for (int b = 0; b < 4; ++b) dmma(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+                for (int b = 0; b < 4; ++b) dmma2(acc[a][b], acc[a + 1][b], af[a], af[a + 1], bf[b]);
         }
         __syncthreads();  // stage s is free again
         if (threadIdx.x == 0 && c + DT_NS < nchunks) issue(c + DT_NS);
@@ -421,11 +427,11 @@ __global__ void __launch_bounds__(128) k_herk_zmma_tma(const __grid_constant__ C
                 bf[b] = part ? v.y : v.x;
             }
 #pragma unroll
-            for (int a = 0; a < 4; ++a)
+            for (int a = 0; a < 4; a += 2)
 #pragma unroll
                 for (int b = 0; b < 4; ++b) {
-                    dmma(re[a][b][0], re[a][b][1], a1[a], bf[b]);
-                    dmma(im[a][b][0], im[a][b][1], a2[a], bf[b]);
+                    dmma2(re[a][b], re[a + 1][b], a1[a], a1[a + 1], bf[b]);
+                    dmma2(im[a][b], im[a + 1][b], a2[a], a2[a + 1], bf[b]);
                 }
         }
         __syncthreads();
