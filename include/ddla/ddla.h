@@ -240,6 +240,20 @@ void pposv_mixed(const DdlaHandle_t& handle, char uplo, char precision, int n, i
                  const int* descA, const double* B, const int* descB, double* X, const int* descX, int& info,
                  MixedReport* report = nullptr);
 
+// pposv_mixed with A, B and X in HOST memory (column-major, leading dimensions
+// lda, ldb, ldx; only A's lower triangle is read).  The lower part of A goes to
+// the device in column panels while the panels that have arrived are already
+// factored (left-looking), so the host-to-device copy overlaps the tensor-core
+// factorization; X comes back to host memory and the handle's stream is
+// synchronised on return.  Pass pinned host memory (ddlaMallocHost /
+// cudaHostAlloc) for the overlap: pageable memory is copied synchronously.
+// Device scratch for A (n x n FP64), W and the factor's low-precision copy is
+// taken per call from the handle's stream-ordered pool.  Same results and
+// report as pposv_mixed on the device copies.
+void pposv_mixed_host(const DdlaHandle_t& handle, char uplo, char precision, int n, int nrhs, const double* A,
+                      int lda, const double* B, int ldb, double* X, int ldx, int& info,
+                      MixedReport* report = nullptr);
+
 }  // namespace ddla
 
 #endif

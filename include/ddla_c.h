@@ -263,6 +263,11 @@ int ddla_d_ppotrs_noalloc(void* handle, char side, char uplo, char trans, int n,
  * {double iter, double gmres, double shift, double backward_error}. */
 int ddla_d_pposv_mixed(void* handle, char uplo, char precision, int n, int nrhs, void* A, const int* descA,
                        const void* B, const int* descB, void* X, const int* descX, int* info, double* report);
+/* The same with A, B and X in host memory (pinned for the overlap; see
+ * ddla::pposv_mixed_host): A's lower part streams to the device by column
+ * panels while the arrived panels are factored.  No reference counterpart. */
+int ddla_d_pposv_mixed_host(void* handle, char uplo, char precision, int n, int nrhs, const void* A, int lda,
+                            const void* B, int ldb, void* X, int ldx, int* info, double* report);
 
 /* Batched uneven Cholesky factor + solve + log-determinant in one persistent
  * launch (no reference counterpart; ddla::posvVbatched, VbatchedPlan and

@@ -181,6 +181,19 @@ int ddlak_potrf_mixed_grouped(char precision, int group, int n, void* W, long lo
 
 /* Inverses (FP64) of the 64 x 64 diagonal blocks of an FP32 factor (lower):
  * ddlak_inv_diag_bytes(n) bytes, one column-major block per block row. */
+/* Left-looking mixed factorization fed from host memory: the lower part of A
+ * (A_host, leading dimension lda_host) goes to A (device, lda) in column panels
+ * of 128 * group columns on copy_stream, and on stream each panel is converted
+ * to W (FP32), updated from every earlier column at once, factored and appended
+ * to Lk, the K-contiguous low-precision copy of L (ldk elements per row, from
+ * ddlak_mixed_lk_bytes; TF32 in FP32 words, or BF16).  colsum (n doubles) and
+ * anrm receive ||A||_inf as ddlak_convert_lower's do; dinfo / status as
+ * ddlak_potrf_mixed's.  Pinned host memory gives the overlap. */
+unsigned long long ddlak_mixed_lk_bytes(char precision, int n, long long* ldk);
+int ddlak_potrf_mixed_stream(char precision, int group, int n, const void* A_host, long long lda_host, void* A,
+                             long long lda, void* W, long long ldw, void* Lk, long long ldk, void* colsum, void* anrm,
+                             int* dinfo, int* status, void* copy_stream, void* stream);
+
 unsigned long long ddlak_inv_diag_bytes(int n);
 int ddlak_inv_diag_blocks(int n, const void* L32, long long ldl, void* Dinv, void* stream);
 

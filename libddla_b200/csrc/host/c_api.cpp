@@ -692,6 +692,24 @@ int ddla_c_profile_read(int kind, double* ms, long long* launches, double* flops
     return e == 0 ? ST_SUCCESS : ST_INTERNAL_ERROR;
 }
 
+int ddla_d_pposv_mixed_host(void* handle, char uplo, char precision, int n, int nrhs, const void* A, int lda,
+                            const void* B, int ldb, void* X, int ldx, int* info, double* report)
+{
+    return run(handle, [&](ddla::DdlaHandle_t h) -> int {
+        if (!info) return ST_INVALID_VALUE;
+        ddla::MixedReport rep;
+        ddla::pposv_mixed_host(h, uplo, precision, n, nrhs, static_cast<const double*>(A), lda,
+                               static_cast<const double*>(B), ldb, static_cast<double*>(X), ldx, *info, &rep);
+        if (report) {
+            report[0] = rep.iter;
+            report[1] = rep.gmres;
+            report[2] = rep.shift;
+            report[3] = rep.backward_error;
+        }
+        return ST_SUCCESS;
+    });
+}
+
 int ddla_d_pposv_mixed(void* handle, char uplo, char precision, int n, int nrhs, void* A, const int* descA,
                        const void* B, const int* descB, void* X, const int* descX, int* info, double* report)
 {

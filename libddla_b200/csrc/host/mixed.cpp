@@ -27,6 +27,7 @@
 #include <vector>
 
 #include <ddla/ddla.h>
+#include <ddla/ddla_desc.h>
 #include <ddla_kernels.h>
 
 #include "ddla_stream.h"
@@ -49,25 +50,29 @@ struct Scalars {
 
 }  // namespace
 
-void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nrhs, double* A, const int* descA,
-                 const double* B, const int* descB, double* X, const int* descX, int& info, MixedReport* report)
+namespace {
+
+// Where the first factorization takes A from when A is still in host memory:
+// the lower part arrives by column panels on copy_stream while the panels that
+// have arrived are factored (ddlak_potrf_mixed_stream).
+struct HostSource {
+    const double* A;
+    long long lda;
+    cudaStream_t copy_stream;
+};
+
+void mixed_core(const DdlaHandle_t& h, char precision, int n, int nrhs, double* A, long long lda, const double* B,
+                long long ldb, double* X, long long ldx, int& info, MixedReport* report, const HostSource* src)
 {
-    detail::check_desc(descA, h);
-    detail::check_desc(descB, h);
-    detail::check_desc(descX, h);
-    detail::require_gpu(h, "pposv_mixed");
-    if (h->nprocs > 1) throw std::invalid_argument("pposv_mixed: served on a 1x1 grid only");
-    if (uplo != 'L' || (precision != 'B' && precision != 'T' && precision != 'D') || n < 0 || nrhs < 0 ||
-        n > descA[DDLA_M_] || n > descA[DDLA_N_] || n > descB[DDLA_M_] || nrhs > descB[DDLA_N_] ||
-        n > descX[DDLA_M_] || nrhs > descX[DDLA_N_])
-        throw std::invalid_argument("pposv_mixed: invalid triangle, precision or dimensions");
-    if (n && (!A || (nrhs && (!B || !X)))) throw std::invalid_argument("pposv_mixed: null matrix");
     MixedReport rep;
     info = 0;
     if (report) *report = rep;
     if (n == 0) return;
     cudaStream_t st = h->stream;
-    const long long lda = descA[DDLA_LLD_], ldb = descB[DDLA_LLD_], ldx = descX[DDLA_LLD_];
+    // descriptors of the device-resident operands for the FP64 path (1x1 grid)
+    const int nbd = 256;
+    const int descA[9] = {DDLA_BLOCK_CYCLIC_2D, 0, n, n, nbd, nbd, 0, 0, (int)lda};
+    const int descX[9] = {DDLA_BLOCK_CYCLIC_2D, 0, n, std::max(1, nrhs), nbd, nbd, 0, 0, (int)ldx};
     auto copy_b_to_x = [&] {
         if (nrhs)
             detail::cuda_check(cudaMemcpy2DAsync(X, ldx * sizeof(double), B, ldb * sizeof(double),
@@ -97,7 +102,10 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
     const std::size_t dinv_bytes = blocked ? ddlak_bis_inverse_bytes(n) : ddlak_inv_diag_bytes(n);
     const std::size_t dinv32_bytes = blocked ? detail::padded_bytes<float>(ddlak_bis_inverse_bytes(n) / 8) : 0;
     const int kry = GmresIR::kRestart;
+    long long ldk = 0;
+    const std::size_t lk_bytes = src ? (std::size_t)ddlak_mixed_lk_bytes(precision, n, &ldk) : 0;
     const std::size_t bytes = detail::padded_bytes<float>((std::size_t)ldw * n) + 2 * pbytes +
+                              (lk_bytes ? (lk_bytes + 255) / 256 * 256 : 0) +
                               3 * detail::padded_bytes<double>((std::size_t)n * std::max(1, nrhs)) +
                               detail::padded_bytes<double>(n) + detail::padded_bytes<Scalars>(1) +
                               2 * detail::padded_bytes<double>(std::max(1, nrhs)) + sbytes +
@@ -105,6 +113,8 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
     detail::DeviceScratch ws(h, bytes);
     char* w = ws.data();
     float* W = detail::take<float>(w, (std::size_t)ldw * n);
+    void* Lk = w;
+    w += lk_bytes ? (lk_bytes + 255) / 256 * 256 : 0;
     void* P0 = w;
     w += pbytes;
     void* P1 = w;
@@ -135,8 +145,16 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
     double shift = 0.0;
     bool factored = false;
     for (int attempt = 0; attempt < kMaxShiftTries && !factored; ++attempt) {
-        ck(ddlak_convert_lower(n, A, lda, W, ldw, 1.0 + shift, colsum, &sc->anrm, st), "convert to FP32");
-        ck(ddlak_potrf_mixed(precision, n, W, ldw, P0, P1, &sc->info, &sc->status, st), "mixed factorization");
+        if (attempt == 0 && src) {
+            // A arrives from host memory while it is factored; every later attempt
+            // (a shifted diagonal) starts from the device copy it leaves behind
+            ck(ddlak_potrf_mixed_stream(precision, DDLAK_MIXED_GROUP, n, src->A, src->lda, A, lda, W, ldw, Lk, ldk,
+                                        colsum, &sc->anrm, &sc->info, &sc->status, src->copy_stream, st),
+               "streamed mixed factorization");
+        } else {
+            ck(ddlak_convert_lower(n, A, lda, W, ldw, 1.0 + shift, colsum, &sc->anrm, st), "convert to FP32");
+            ck(ddlak_potrf_mixed(precision, n, W, ldw, P0, P1, &sc->info, &sc->status, st), "mixed factorization");
+        }
         read_scalars();
         if (hs.status != 0) throw std::runtime_error("pposv_mixed: a tensor-core update wait timed out");
         if (hs.info == 0) factored = true;
@@ -229,6 +247,91 @@ void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nr
     rep.gmres = use_gmres ? 1 : 0;
     // ---- 5: FP64 fallback ---------------------------------------------------------------
     fp64_path(sweeps);
+}
+
+}  // namespace
+
+void pposv_mixed(const DdlaHandle_t& h, char uplo, char precision, int n, int nrhs, double* A, const int* descA,
+                 const double* B, const int* descB, double* X, const int* descX, int& info, MixedReport* report)
+{
+    detail::check_desc(descA, h);
+    detail::check_desc(descB, h);
+    detail::check_desc(descX, h);
+    detail::require_gpu(h, "pposv_mixed");
+    if (h->nprocs > 1) throw std::invalid_argument("pposv_mixed: served on a 1x1 grid only");
+    if (uplo != 'L' || (precision != 'B' && precision != 'T' && precision != 'D') || n < 0 || nrhs < 0 ||
+        n > descA[DDLA_M_] || n > descA[DDLA_N_] || n > descB[DDLA_M_] || nrhs > descB[DDLA_N_] ||
+        n > descX[DDLA_M_] || nrhs > descX[DDLA_N_])
+        throw std::invalid_argument("pposv_mixed: invalid triangle, precision or dimensions");
+    if (n && (!A || (nrhs && (!B || !X)))) throw std::invalid_argument("pposv_mixed: null matrix");
+    mixed_core(h, precision, n, nrhs, A, descA[DDLA_LLD_], B, descB[DDLA_LLD_], X, descX[DDLA_LLD_], info, report,
+               nullptr);
+}
+
+void pposv_mixed_host(const DdlaHandle_t& h, char uplo, char precision, int n, int nrhs, const double* A, int lda,
+                      const double* B, int ldb, double* X, int ldx, int& info, MixedReport* report)
+{
+    detail::require_gpu(h, "pposv_mixed_host");
+    if (h->nprocs > 1) throw std::invalid_argument("pposv_mixed_host: served on a 1x1 grid only");
+    if (uplo != 'L' || (precision != 'B' && precision != 'T' && precision != 'D') || n < 0 || nrhs < 0 ||
+        lda < std::max(1, n) || ldb < std::max(1, n) || ldx < std::max(1, n))
+        throw std::invalid_argument("pposv_mixed_host: invalid triangle, precision, dimensions or leading dimensions");
+    if (n && (!A || (nrhs && (!B || !X)))) throw std::invalid_argument("pposv_mixed_host: null matrix");
+    info = 0;
+    if (report) *report = MixedReport{};
+    if (n == 0) return;
+    cudaStream_t st = h->stream;
+    // device copies: A (lower part only is ever written or read; even leading
+    // dimension for the FP64 tile maps of the residual), B and X
+    const long long ldad = n + (n & 1);
+    const std::size_t rhs_bytes = detail::padded_bytes<double>((std::size_t)n * std::max(1, nrhs));
+    detail::DeviceScratch dev(h, detail::padded_bytes<double>((std::size_t)ldad * n) + 2 * rhs_bytes);
+    double* dA = reinterpret_cast<double*>(dev.data());
+    double* dB = reinterpret_cast<double*>(dev.data() + detail::padded_bytes<double>((std::size_t)ldad * n));
+    double* dX = reinterpret_cast<double*>(reinterpret_cast<char*>(dB) + rhs_bytes);
+    if (nrhs)
+        detail::cuda_check(cudaMemcpy2DAsync(dB, sizeof(double) * n, B, sizeof(double) * ldb, sizeof(double) * n,
+                                             nrhs, cudaMemcpyHostToDevice, st),
+                           "copy B to the device");
+    // the copy stream starts after the allocations on the handle stream
+    struct CopyStream {
+        cudaStream_t s = nullptr;
+        cudaEvent_t ready = nullptr;
+        ~CopyStream()
+        {
+            if (ready) cudaEventDestroy(ready);
+            if (s) cudaStreamDestroy(s);
+        }
+    } cs;
+    detail::cuda_check(cudaStreamCreateWithFlags(&cs.s, cudaStreamNonBlocking), "copy stream");
+    detail::cuda_check(cudaEventCreateWithFlags(&cs.ready, cudaEventDisableTiming), "copy stream event");
+    detail::cuda_check(cudaEventRecord(cs.ready, st), "copy stream event");
+    detail::cuda_check(cudaStreamWaitEvent(cs.s, cs.ready, 0), "copy stream event");
+    try {
+        if (precision == 'D' || nrhs == 0) {
+            // no tensor-core factor to overlap: the lower part of A in column panels, then the device routine
+            const long long pw = 1024;
+            for (long long c0 = 0; c0 < n; c0 += pw)
+                detail::cuda_check(cudaMemcpy2DAsync(dA + c0 + c0 * ldad, sizeof(double) * ldad, A + c0 + c0 * lda,
+                                                     sizeof(double) * lda, sizeof(double) * (n - c0),
+                                                     (size_t)std::min(pw, n - c0), cudaMemcpyHostToDevice, st),
+                                   "copy A to the device");
+            mixed_core(h, precision, n, nrhs, dA, ldad, dB, n, dX, n, info, report, nullptr);
+        } else {
+            const HostSource src{A, lda, cs.s};
+            mixed_core(h, precision, n, nrhs, dA, ldad, dB, n, dX, n, info, report, &src);
+        }
+        if (nrhs)
+            detail::cuda_check(cudaMemcpy2DAsync(X, sizeof(double) * ldx, dX, sizeof(double) * n,
+                                                 sizeof(double) * n, nrhs, cudaMemcpyDeviceToHost, st),
+                               "copy X to the host");
+        detail::cuda_check(cudaStreamSynchronize(st), "stream synchronisation");
+        detail::cuda_check(cudaStreamSynchronize(cs.s), "stream synchronisation");
+    } catch (...) {
+        cudaStreamSynchronize(cs.s);
+        cudaStreamSynchronize(st);
+        throw;
+    }
 }
 
 }  // namespace ddla

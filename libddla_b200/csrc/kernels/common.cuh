@@ -202,12 +202,22 @@ template <class T, bool UP>
 __device__ __forceinline__ void load_lview_block(T* s, int ld, const T* A, long long lda, long long r0, long long c0,
                                                  int rows, int cols, int brows, int bcols, bool lower)
 {
-    for (int idx = threadIdx.x; idx < brows * bcols; idx += blockDim.x) {
-        int i, j;
-        if (UP) { j = idx % bcols; i = idx / bcols; } else { i = idx % brows; j = idx / brows; }
+    auto elem = [&](int i, int j) {
         const bool valid = i < rows && j < cols && (!lower || i >= j);
         const T* src = UP ? A + (c0 + j) + (r0 + i) * lda : A + (r0 + i) + (c0 + j) * lda;
         cp_async_elem<sizeof(T)>(&s[i + j * ld], valid ? src : A, valid);
+    };
+    if (brows == 128 && bcols == 128) {
+        // the full block: index arithmetic by shifts (consecutive threads on the contiguous index)
+        for (int idx = threadIdx.x; idx < 128 * 128; idx += blockDim.x) {
+            if (UP) elem(idx >> 7, idx & 127);
+            else elem(idx & 127, idx >> 7);
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < brows * bcols; idx += blockDim.x) {
+            if (UP) elem(idx / bcols, idx % bcols);
+            else elem(idx % brows, idx / brows);
+        }
     }
     cp_async_commit_wait_all();
     __syncthreads();

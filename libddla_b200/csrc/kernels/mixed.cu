@@ -16,6 +16,7 @@
 #include <cuda_bf16.h>
 
 #include <mutex>
+#include <vector>
 #include <type_traits>
 
 #include <ddla_kernels.h>
@@ -39,10 +40,18 @@ constexpr int MX_NB = 128;  // block width of the mixed factorization (= UMMA ti
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_convert_lower(const double* __restrict__ A, long long lda,
                                                        float* __restrict__ W, long long ldw, int n, double diag_scale,
-                                                       double* __restrict__ colsum)
+                                                       double* __restrict__ colsum, int jt0)
 {
+    // jt0 < 0: every lower 64 x 64 tile, one per block (triangle order); jt0 >= 0: the
+    // tiles of tile columns jt0 + blockIdx.y, tile row J + blockIdx.x (a column panel)
     int I, J;
-    tile_of_tri(blockIdx.x, I, J);
+    if (jt0 < 0) {
+        tile_of_tri(blockIdx.x, I, J);
+    } else {
+        J = jt0 + (int)blockIdx.y;
+        I = J + (int)blockIdx.x;
+        if ((long long)I * 64 >= n) return;
+    }
     const long long ri = (long long)I * 64, rj = (long long)J * 64;
     __shared__ double csw[8][16];   // per warp: column sums of its 32 rows
     __shared__ double rsum[4][64];
@@ -100,36 +109,71 @@ __global__ void __launch_bounds__(256) k_potrf_diag_mixed(float* __restrict__ W,
     const int ld = nbk + 1;
     if (*(volatile int*)info != 0) return;
     const int total = nbk * nbk;
-    for (int base = 0; base < total; base += 16 * 256) {
-        float v[16];
-#pragma unroll
-        for (int u = 0; u < 16; ++u) {
-            const int idx = base + u * 256 + threadIdx.x;
-            const int i = idx % nbk, j = idx / nbk;
-            v[u] = (idx < total && i >= j) ? W[(k0 + i) + (long long)(k0 + j) * ldw] : 0.f;
+    const float* Wb = W + k0 + (long long)k0 * ldw;
+    if (nbk == 128) {
+        // the full block by float4 columns (ldw and k0 are multiples of 4): 32 per column,
+        // consecutive threads down a column; groups wholly above the diagonal are skipped
+#pragma unroll 4
+        for (int idx = threadIdx.x; idx < 128 * 32; idx += 256) {
+            const int q = idx & 31, j = idx >> 5;
+            if (4 * q + 3 < j) continue;
+            const float4 v = *reinterpret_cast<const float4*>(Wb + 4 * q + (long long)j * ldw);
+            double* d = s + 4 * q + j * ld;
+            d[0] = v.x;
+            d[1] = v.y;
+            d[2] = v.z;
+            d[3] = v.w;
         }
+    } else {
+        for (int base = 0; base < total; base += 16 * 256) {
+            float v[16];
 #pragma unroll
-        for (int u = 0; u < 16; ++u) {
-            const int idx = base + u * 256 + threadIdx.x;
-            if (idx < total) s[(idx % nbk) + (idx / nbk) * ld] = (double)v[u];
+            for (int u = 0; u < 16; ++u) {
+                const int idx = base + u * 256 + threadIdx.x;
+                const int i = idx % nbk, j = idx / nbk;
+                v[u] = (idx < total && i >= j) ? Wb[i + (long long)j * ldw] : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+                const int idx = base + u * 256 + threadIdx.x;
+                if (idx < total) s[(idx % nbk) + (idx / nbk) * ld] = (double)v[u];
+            }
         }
     }
     __syncthreads();
     const int fail = factor_block_smem<double>(s, ld, nbk);
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const int i = idx % nbk, j = idx / nbk;
-        if (i >= j) W[(k0 + i) + (long long)(k0 + j) * ldw] = (float)s[i + j * ld];
+    if (nbk == 128) {
+        // float4 stores of the lower part; a group crossing the diagonal keeps its upper entries
+        for (int idx = threadIdx.x; idx < 128 * 32; idx += 256) {
+            const int q = idx & 31, j = idx >> 5;
+            if (4 * q + 3 < j) continue;
+            float* dst = W + k0 + 4 * q + (long long)(k0 + j) * ldw;
+            const double* src = s + 4 * q + j * ld;
+            if (4 * q >= j) {
+                *reinterpret_cast<float4*>(dst) = make_float4((float)src[0], (float)src[1], (float)src[2], (float)src[3]);
+            } else {
+                for (int e = 0; e < 4; ++e)
+                    if (4 * q + e >= j) dst[e] = (float)src[e];
+            }
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+            const int i = idx % nbk, j = idx / nbk;
+            if (i >= j) W[(k0 + i) + (long long)(k0 + j) * ldw] = (float)s[i + j * ld];
+        }
     }
     if (fail && threadIdx.x == 0) *info = k0 + fail;
 }
 
 // ---------------------------------------------------------------------------
-// panel rows [pr0, n) x columns [k0, k0+nbk) of W -> P, K-contiguous:
-// P[r*nbk + k] = round(W[(pr0+r) + (k0+k)*ldw]) (BF16, or FP32 rounded to TF32)
+// panel rows [pr0, n) x columns [k0, k0+nbk) of W -> P, K-contiguous with row
+// stride ldp: P[r*ldp + k] = round(W[(pr0+r) + (k0+k)*ldw]) (BF16, or FP32
+// rounded to TF32)
 // ---------------------------------------------------------------------------
 template <bool TF32>
 __global__ void __launch_bounds__(256) k_pack_panel(const float* __restrict__ W, long long ldw, int n, long long pr0,
-                                                    int k0, int nbk, void* __restrict__ P, const int* __restrict__ info)
+                                                    int k0, int nbk, void* __restrict__ P, long long ldp,
+                                                    const int* __restrict__ info)
 {
     __shared__ float t[32][33];
     if (*(volatile int*)info != 0) return;
@@ -144,7 +188,7 @@ __global__ void __launch_bounds__(256) k_pack_panel(const float* __restrict__ W,
         const long long r = r0 + y;
         if (pr0 + r >= n) continue;
         const float x = t[threadIdx.x][y];
-        const long long off = r * nbk + kk0 + threadIdx.x;
+        const long long off = r * ldp + kk0 + threadIdx.x;
         if (TF32) {
             uint32_t b;
             asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(b) : "f"(x));
@@ -746,14 +790,15 @@ EncodeFn encode_fn()
     return fn;
 }
 
-// P: rows x kp elements, K contiguous; box = 128 rows x 128 bytes, 128-byte swizzle
-bool encode_panel_map(CUtensorMap* map, const void* P, long long rows, int kp, bool tf32)
+// P: rows x kp elements, K contiguous, row stride ldp elements; box = 128 rows x
+// 128 bytes, 128-byte swizzle
+bool encode_panel_map(CUtensorMap* map, const void* P, long long rows, int kp, long long ldp, bool tf32)
 {
     EncodeFn fn = encode_fn();
     if (!fn) return false;
     const cuuint64_t esize = tf32 ? 4 : 2;
     const cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)rows};
-    const cuuint64_t strides[1] = {(cuuint64_t)kp * esize};
+    const cuuint64_t strides[1] = {(cuuint64_t)ldp * esize};
     const cuuint32_t box[2] = {(cuuint32_t)(128 / esize), 128u};
     const cuuint32_t estr[2] = {1u, 1u};
     const CUresult r = fn(map, tf32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
@@ -818,13 +863,13 @@ MixedStreams& mixed_streams()
 
 template <bool TF32>
 cudaError_t mixed_update(float* W, long long ldw, int n, long long t0, long long pr0, int cols, const void* P,
-                         int nbk, const int* dinfo, int* status, cudaStream_t st)
+                         long long ldp, int nbk, const int* dinfo, int* status, cudaStream_t st)
 {
     const long long m = (long long)n - t0;
-    if (m <= 0) return cudaSuccess;
+    if (m <= 0 || nbk <= 0) return cudaSuccess;
     if (cudaError_t e = smem_optin(k_mixed_update<TF32>, MU_SMEM); e != cudaSuccess) return e;
     CUtensorMap map;
-    if (!encode_panel_map(&map, P, (long long)n - pr0, nbk, TF32)) return cudaErrorInvalidValue;
+    if (!encode_panel_map(&map, P, (long long)n - pr0, nbk, ldp, TF32)) return cudaErrorInvalidValue;
     CUtensorMap wmap;
     if (!encode_w_map(&wmap, W, n, ldw)) return cudaErrorInvalidValue;
     const long long t = ceil_div(m, 128);
@@ -881,7 +926,7 @@ cudaError_t potrf_mixed_enqueue(float* W, long long ldw, int n, int G, void* P0,
         dim3 grid((unsigned)ceil_div(m, 32), kw / 32);
         {
             ProfScope ps(PK_MIXED_OTHER, s, 0.0, (double)m * kw * (4.0 + (TF32 ? 4.0 : 2.0)));
-            k_pack_panel<TF32><<<grid, dim3(32, 8), 0, s>>>(W, ldw, n, pr0, k0, kw, Pbuf, dinfo);
+            k_pack_panel<TF32><<<grid, dim3(32, 8), 0, s>>>(W, ldw, n, pr0, k0, kw, Pbuf, kw, dinfo);
         }
         note_launches(1);
         return cudaGetLastError();
@@ -904,7 +949,7 @@ cudaError_t potrf_mixed_enqueue(float* W, long long ldw, int n, int G, void* P0,
             if (g > 0) {
                 if ((e = pack(kg, (int)k0, g * NB, Pleft, hi)) != cudaSuccess) return e;
                 const int cols = (long long)n - kg < NB ? (int)(n - kg) : NB;
-                if ((e = mixed_update<TF32>(W, ldw, n, kg, kg, cols, Pleft, g * NB, dinfo, status, hi)) !=
+                if ((e = mixed_update<TF32>(W, ldw, n, kg, kg, cols, Pleft, g * NB, g * NB, dinfo, status, hi)) !=
                     cudaSuccess)
                     return e;
             }
@@ -920,13 +965,13 @@ cudaError_t potrf_mixed_enqueue(float* W, long long ldw, int n, int G, void* P0,
         // super-step's trailing update has reached them
         if (have_rest) cudaStreamWaitEvent(hi, L.rest, 0);
         const int la_cols = (long long)n - t0 < SW ? (int)(n - t0) : (int)SW;
-        if ((e = mixed_update<TF32>(W, ldw, n, t0, t0, la_cols, Ppanel, (int)SW, dinfo, status, hi)) != cudaSuccess)
+        if ((e = mixed_update<TF32>(W, ldw, n, t0, t0, la_cols, Ppanel, SW, (int)SW, dinfo, status, hi)) != cudaSuccess)
             return e;
         // the rest of the trailing matrix on the caller's stream
         have_rest = false;
         if (t0 + SW < n) {
             cudaStreamWaitEvent(st, L.panel, 0);
-            if ((e = mixed_update<TF32>(W, ldw, n, t0 + SW, t0, 0, Ppanel, (int)SW, dinfo, status, st)) !=
+            if ((e = mixed_update<TF32>(W, ldw, n, t0 + SW, t0, 0, Ppanel, SW, (int)SW, dinfo, status, st)) !=
                 cudaSuccess)
                 return e;
             cudaEventRecord(L.rest, st);
@@ -937,6 +982,104 @@ cudaError_t potrf_mixed_enqueue(float* W, long long ldw, int n, int G, void* P0,
     cudaEventRecord(L.panel, hi);
     cudaStreamWaitEvent(st, L.panel, 0);
     return cudaGetLastError();
+}
+
+// Left-looking factorization fed from host memory, one super-step panel at a
+// time (the end-to-end form of pposv_mixed).  The copy stream cs brings the
+// lower part of A in column panels of SW = 128 G columns (rows [c0, n) of
+// columns [c0, c0 + SW), the part uplo 'L' references) into Ad; on the
+// compute stream st, panel c waits only for its own arrival, so the copies of
+// the later panels overlap the factorization of the earlier ones:
+//   1. W(panel) = fl32(A(panel)), column / row sums for ||A||_inf;
+//   2. the panel takes the update from every earlier column in ONE launch,
+//      W(i, j) -= sum_{k < c0} Lk(i, k) Lk(j, k), from Lk, the K-contiguous
+//      low-precision copy of L the factorization appends to (row stride ldk);
+//   3. its G block columns are factored one after the other, block g after the
+//      update from blocks 0..g-1 of the panel (from Lk as well), with the FP64
+//      diagonal block and the panel solve of the right-looking form, and each
+//      finished block column is rounded into Lk.
+// No part of W to the right of the panel is touched before it arrives.  The
+// trailing updates of the right-looking form read and write the FP32 trailing
+// matrix once per super-step; here each panel is written once and the factor
+// is read (in TF32/BF16) once per later panel.
+template <bool TF32>
+cudaError_t potrf_mixed_stream_enqueue(int n, int G, const double* Ah, long long ldah, double* Ad, long long ldad,
+                                       float* W, long long ldw, void* Lk, long long ldk, double* colsum,
+                                       double* anrm, int* dinfo, int* status, cudaStream_t cs, cudaStream_t st)
+{
+    constexpr int NB = MX_NB;
+    const size_t diag_smem = (size_t)NB * (NB + 1) * sizeof(double);
+    if (cudaError_t e = smem_optin(k_potrf_diag_mixed, diag_smem); e != cudaSuccess) return e;
+    const long long SW = (long long)G * NB;
+    const size_t esz = TF32 ? 4 : 2;
+    const int S = (int)ceil_div(n, SW);
+    auto lk_at = [&](long long row, long long k) -> void* {
+        return static_cast<unsigned char*>(Lk) + (size_t)(row * ldk + k) * esz;
+    };
+    std::vector<cudaEvent_t> arrive((size_t)S, nullptr);
+    cudaError_t e = cudaSuccess;
+    for (int c = 0; c < S && e == cudaSuccess; ++c) e = cudaEventCreateWithFlags(&arrive[c], cudaEventDisableTiming);
+    auto release = [&] {
+        for (cudaEvent_t ev : arrive)
+            if (ev) cudaEventDestroy(ev);  // resources go once the recorded work is done
+    };
+    if (e != cudaSuccess) {
+        release();
+        return e;
+    }
+    for (int c = 0; c < S && e == cudaSuccess; ++c) {
+        const long long c0 = (long long)c * SW, w = std::min<long long>(SW, n - c0);
+        e = cudaMemcpy2DAsync(Ad + c0 + c0 * ldad, (size_t)ldad * 8, Ah + c0 + c0 * ldah, (size_t)ldah * 8,
+                              (size_t)(n - c0) * 8, (size_t)w, cudaMemcpyHostToDevice, cs);
+        if (e == cudaSuccess) e = cudaEventRecord(arrive[c], cs);
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(colsum, 0, sizeof(double) * n, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(anrm, 0, sizeof(double), st);
+    for (int c = 0; c < S && e == cudaSuccess; ++c) {
+        const long long c0 = (long long)c * SW, w = std::min<long long>(SW, n - c0);
+        if ((e = cudaStreamWaitEvent(st, arrive[c], 0)) != cudaSuccess) break;
+        {
+            const long long jt = c0 / 64, jts = ceil_div(c0 + w, 64) - jt, its = ceil_div(n - c0, 64);
+            ProfScope ps(PK_MIXED_OTHER, st, 0.0, 6.0 * (double)(n - c0) * w);
+            k_convert_lower<<<dim3((unsigned)its, (unsigned)jts), 256, 0, st>>>(Ad, ldad, W, ldw, n, 1.0, colsum,
+                                                                                (int)jt);
+        }
+        note_launches(1);
+        if (c0 > 0 &&
+            (e = mixed_update<TF32>(W, ldw, n, c0, 0, (int)w, Lk, ldk, (int)c0, dinfo, status, st)) != cudaSuccess)
+            break;
+        for (int g = 0; g < G && e == cudaSuccess; ++g) {
+            const long long kg = c0 + (long long)g * NB;
+            if (kg >= n) break;
+            const int nbk = (long long)n - kg < NB ? (int)(n - kg) : NB;
+            if (g > 0 && (e = mixed_update<TF32>(W, ldw, n, kg, 0, nbk, lk_at(0, c0), ldk, g * NB, dinfo, status,
+                                                 st)) != cudaSuccess)
+                break;
+            {
+                ProfScope ps(PK_MIXED_OTHER, st, (double)nbk * nbk * nbk / 3.0, 4.0 * nbk * (nbk + 1));
+                k_potrf_diag_mixed<<<1, 256, (size_t)nbk * (nbk + 1) * sizeof(double), st>>>(W, ldw, (int)kg, nbk,
+                                                                                             dinfo);
+            }
+            note_launches(1);
+            if (kg + nbk >= n) break;  // the last block column: nothing to its right
+            if ((e = launch_trsm_panel<float, false>(W, ldw, (int)kg, nbk, n, dinfo, st)) != cudaSuccess) break;
+            {
+                const long long m = (long long)n - kg;
+                ProfScope ps(PK_MIXED_OTHER, st, 0.0, (double)m * NB * (4.0 + (TF32 ? 4.0 : 2.0)));
+                k_pack_panel<TF32><<<dim3((unsigned)ceil_div(m, 32), NB / 32), dim3(32, 8), 0, st>>>(
+                    W, ldw, n, kg, (int)kg, NB, lk_at(kg, kg), ldk, dinfo);
+            }
+            note_launches(1);
+            e = cudaGetLastError();
+        }
+    }
+    if (e == cudaSuccess) {
+        k_max_nonneg<<<148, 256, 0, st>>>(colsum, n, anrm);
+        note_launches(1);
+        e = cudaGetLastError();
+    }
+    release();
+    return e;
 }
 
 }  // namespace
@@ -966,7 +1109,7 @@ extern "C" int ddlak_convert_lower(int n, const void* A, long long lda, void* W,
         ProfScope ps(PK_MIXED_OTHER, st, 0.0, 6.0 * (double)n * n);
         k_convert_lower<<<(unsigned)(t * (t + 1) / 2), 256, 0, st>>>(static_cast<const double*>(A), lda,
                                                                      static_cast<float*>(W), ldw, n, diag_scale,
-                                                                     static_cast<double*>(colsum));
+                                                                     static_cast<double*>(colsum), -1);
         k_max_nonneg<<<148, 256, 0, st>>>(static_cast<const double*>(colsum), n, static_cast<double*>(anrm));
     }
     note_launches(2);
@@ -1112,4 +1255,42 @@ extern "C" int ddlak_axpy(int n, int ncol, double alpha, const void* X, long lon
                                                                          static_cast<double*>(Y), ldy);
     note_launches(1);
     return (int)cudaGetLastError();
+}
+
+extern "C" unsigned long long ddlak_mixed_lk_bytes(char precision, int n, long long* ldk)
+{
+    // the K-contiguous copy of L: n rows of ldk elements, ldk a multiple of 64 (TMA row strides
+    // and the 128-byte boxes stay aligned)
+    const long long ld = ((long long)(n > 0 ? n : 1) + 63) / 64 * 64;
+    if (ldk) *ldk = ld;
+    return (unsigned long long)ld * (unsigned long long)(n > 0 ? n : 0) * (precision == 'B' ? 2u : 4u);
+}
+
+extern "C" int ddlak_potrf_mixed_stream(char precision, int group, int n, const void* A_host, long long lda_host,
+                                        void* A, long long lda, void* W, long long ldw, void* Lk, long long ldk,
+                                        void* colsum, void* anrm, int* dinfo, int* status, void* copy_stream,
+                                        void* stream)
+{
+    using namespace ddlak;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(dinfo, 0, sizeof(int), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, sizeof(int), st);
+    if (e != cudaSuccess) return (int)e;
+    if (n <= 0) return 0;
+    if (ldw % 4 != 0 || ldk % 64 != 0 || ldk < n || lda < n || lda_host < n || group < 1 ||
+        group > DDLAK_MIXED_MAX_GROUP || (reinterpret_cast<uintptr_t>(Lk) & 255))
+        return (int)cudaErrorInvalidValue;
+    const double* ah = static_cast<const double*>(A_host);
+    double* ad = static_cast<double*>(A);
+    float* w = static_cast<float*>(W);
+    cudaStream_t cs = static_cast<cudaStream_t>(copy_stream);
+    double* cols = static_cast<double*>(colsum);
+    double* an = static_cast<double*>(anrm);
+    if (precision == 'T')
+        return (int)potrf_mixed_stream_enqueue<true>(n, group, ah, lda_host, ad, lda, w, ldw, Lk, ldk, cols, an, dinfo,
+                                                     status, cs, st);
+    if (precision == 'B')
+        return (int)potrf_mixed_stream_enqueue<false>(n, group, ah, lda_host, ad, lda, w, ldw, Lk, ldk, cols, an,
+                                                      dinfo, status, cs, st);
+    return (int)cudaErrorInvalidValue;
 }

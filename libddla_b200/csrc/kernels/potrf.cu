@@ -41,9 +41,16 @@ __global__ void __launch_bounds__(256) k_potrf_diag(T* __restrict__ A, long long
     if (*(volatile int*)info != 0) return;
     load_lview_block<T, UP>(s, ld, A, lda, k0, k0, nbk, nbk, nbk, nbk, true);
     const int fail = factor_block_smem<T>(s, ld, nbk);
-    for (int idx = threadIdx.x; idx < nbk * nbk; idx += blockDim.x) {
-        const int i = idx % nbk, j = idx / nbk;
-        if (i >= j) lview_st<T, UP>(A, lda, k0 + i, k0 + j, s[i + j * ld]);
+    if (nbk == 128) {  // the full block: index arithmetic by shifts
+        for (int idx = threadIdx.x; idx < 128 * 128; idx += blockDim.x) {
+            const int i = UP ? idx >> 7 : idx & 127, j = UP ? idx & 127 : idx >> 7;
+            if (i >= j) lview_st<T, UP>(A, lda, k0 + i, k0 + j, s[i + j * ld]);
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < nbk * nbk; idx += blockDim.x) {
+            const int i = idx % nbk, j = idx / nbk;
+            if (i >= j) lview_st<T, UP>(A, lda, k0 + i, k0 + j, s[i + j * ld]);
+        }
     }
     if (fail && threadIdx.x == 0) *info = k0 + fail;
 }

@@ -18,7 +18,7 @@ from .layout import ProcessorLayout  # noqa: F401
 from .matrix import DistributedMatrix  # noqa: F401
 from . import autograd, batched, grid  # noqa: F401
 from .ops import (diag_logdet, gather, pdiag_logdet, pdiag_logdet_finish, pdiag_logdet_grid,  # noqa: F401
-                  pdiag_logdet_local, phegst, potrf, potrf_bottom_right, pposv, pposv_mixed, ppotrf,
+                  pdiag_logdet_local, phegst, potrf, potrf_bottom_right, pposv, pposv_mixed, pposv_mixed_host, ppotrf,
                   ppotrf_bottom_right, ppotrs, scatter)
 
 

@@ -141,6 +141,7 @@ _SIGS = {
     "ddla_c_finalize": (None, []),
     "ddla_c_bcast_dims": (_i, [_i, _ip, _ip, _ip, _i]),
     "ddla_d_pposv_mixed": (_i, [_vp, _c, _c, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _ip, _dp]),
+    "ddla_d_pposv_mixed_host": (_i, [_vp, _c, _c, _i, _i, _vp, _i, _vp, _i, _vp, _i, _ip, _dp]),
     "ddla_c_get_stream": (_i, [_vp, ctypes.POINTER(_vp)]),
     "ddla_c_launch_count": (_ll, []),
     "ddla_c_pdiag_logdet_finish": (_i, [_vp, _i, _vp]),

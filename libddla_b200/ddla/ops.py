@@ -166,6 +166,33 @@ def pposv_mixed(A: DistributedMatrix, B: DistributedMatrix, X: DistributedMatrix
     return X, info.value, report
 
 
+def pposv_mixed_host(handle, A, B, precision: str = "T", uplo: str = "L", X=None):
+    """pposv_mixed on host arrays (ddla_d_pposv_mixed_host): A (n x n) and B (n x nrhs) float64 in
+    host memory, column-major; only A's lower triangle is read.  A streams to the device by column
+    panels while the arrived panels are factored; with pinned arrays (for instance the .numpy() view
+    of a torch tensor made with pin_memory=True) the copy overlaps the factorization.  Returns
+    (X, info, report); X is a new Fortran-ordered array unless one is given."""
+    import numpy as np
+
+    A = np.asarray(A)
+    B = np.asarray(B)
+    if A.dtype != np.float64 or B.dtype != np.float64:
+        raise TypeError("pposv_mixed_host takes float64 arrays")
+    A = np.asfortranarray(A)
+    B = np.asfortranarray(B if B.ndim == 2 else B[:, None])
+    n, nrhs = A.shape[0], B.shape[1]
+    if X is None:
+        X = np.empty((n, nrhs), dtype=np.float64, order="F")
+    info = ctypes.c_int(0)
+    rep = (ctypes.c_double * 4)()
+    C.check_status(C.ddla_d_pposv_mixed_host(handle.ptr, _ch(uplo), _ch(precision), n, nrhs, A.ctypes.data,
+                                             max(1, A.shape[0]), B.ctypes.data, max(1, B.shape[0]), X.ctypes.data,
+                                             max(1, X.shape[0]), ctypes.byref(info), rep),
+                   "ddla_d_pposv_mixed_host")
+    report = {"iter": int(rep[0]), "gmres": int(rep[1]), "shift": float(rep[2]), "backward_error": float(rep[3])}
+    return X, info.value, report
+
+
 def gather(A: DistributedMatrix, root: int = 0):
     return A.to_global_matrix(root)
 
