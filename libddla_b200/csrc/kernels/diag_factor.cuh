@@ -22,6 +22,7 @@
 // row of the block) and the failed pivot keeps its value.
 // Must be called by all 256 threads of the CTA.
 #pragma once
+#include <type_traits>
 #include "common.cuh"
 
 namespace ddlak {
@@ -185,6 +186,53 @@ __device__ __forceinline__ void trailing(T* s, int ld, int c0, int c1, int nbk, 
         }
 }
 
+// (C) for double on the FP64 tensor cores: the trailing lower triangle in 16 x 8
+// tiles (mma.sync m16n8k4 f64), tile (I, K) covering rows c1 + 16 I .. + 15 and
+// columns c1 + 8 K .. + 7, handed out to the warps round-robin; lane (g, q) feeds
+// L(row g / g + 8, c0 + kk + q) and L(col g, c0 + kk + q) and receives the
+// products for rows g and g + 8, columns 2q and 2q + 1.  Only k <= i is written.
+__device__ __forceinline__ void mma16x8x4(double (&u)[2], double (&v)[2], double a_up, double a_lo, double b)
+{
+    asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+                 : "+d"(u[0]), "+d"(u[1]), "+d"(v[0]), "+d"(v[1])
+                 : "d"(a_up), "d"(a_lo), "d"(b));
+}
+
+__device__ __forceinline__ void trailing_dmma(double* s, int ld, int c0, int c1, int nbk, int t)
+{
+    const int warp = t >> 5, lane = t & 31, g = lane >> 2, q = lane & 3;
+    const int m2 = nbk - c1;
+    const int ti = (m2 + 15) / 16;
+    // tiles of the lower triangle, row by row: row I holds column tiles 0 .. min(2I + 1, last)
+    const int tk_all = (m2 + 7) / 8;
+    int ntiles = 0;
+    for (int I = 0; I < ti; ++I) ntiles += min(2 * I + 2, tk_all);
+    for (int tile = warp; tile < ntiles; tile += 8) {
+        int I = 0, rem = tile;
+        while (rem >= min(2 * I + 2, tk_all)) {
+            rem -= min(2 * I + 2, tk_all);
+            ++I;
+        }
+        const int K = rem;
+        const int r_up = 16 * I + g, r_lo = r_up + 8, col = 8 * K + g;
+        double u[2] = {0.0, 0.0}, v[2] = {0.0, 0.0};
+#pragma unroll
+        for (int kk = 0; kk < PW; kk += 4) {
+            const double* cj0 = s + (c0 + kk + q) * ld + c1;
+            const double a_up = r_up < m2 ? cj0[r_up] : 0.0;
+            const double a_lo = r_lo < m2 ? cj0[r_lo] : 0.0;
+            const double b = col < m2 ? cj0[col] : 0.0;
+            mma16x8x4(u, v, a_up, a_lo, b);
+        }
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int k = 8 * K + 2 * q + e;
+            if (r_up < m2 && k <= r_up) s[(c1 + r_up) + (c1 + k) * ld] -= u[e];
+            if (r_lo < m2 && k <= r_lo) s[(c1 + r_lo) + (c1 + k) * ld] -= v[e];
+        }
+    }
+}
+
 }  // namespace diagf
 
 template <class T>
@@ -210,7 +258,8 @@ __device__ int factor_block_smem(T* s, int ld, int nbk)
         __syncthreads();
         if (fail) break;
         if (c1 < nbk) {
-            trailing<T>(s, ld, c0, c1, nbk, t);
+            if constexpr (std::is_same<T, double>::value) trailing_dmma(s, ld, c0, c1, nbk, t);
+            else trailing<T>(s, ld, c0, c1, nbk, t);
             __syncthreads();
         }
     }
