@@ -948,7 +948,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     hbm = peaks.get("hbm_gbs") or 6650.0
     roof = {"bound": "hbm", "kernel": "k_mixed_update (tcgen05 trailing update, FP32 W read-modify-write)",
             "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm if gbs else None,
-            "traffic": traffic.get("k_mixed_update", {}).get("bytes_per_launch_at_bench"),
+            # DRAM bytes per launch: the measured bytes per 128 x 128 tile times the tiles an average launch updates
+            "traffic": (traffic["k_mixed_update"]["bytes_per_tile"] * (dom["bytes"] / dom["launches"]) /
+                        traffic["k_mixed_update"]["algorithmic_bytes_per_tile"])
+            if dom.get("launches") and "bytes_per_tile" in traffic.get("k_mixed_update", {}) else None,
+            "traffic_source": "profiles/dram_traffic.json (one-launch capture at n=8192, per tile, scaled)",
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks.get("hbm_gbs") else "fallback 6650 GB/s",
             "launches": dom.get("launches"), "avg_launch_ms": (dom["ms"] / dom["launches"]) if dom.get("launches") else None}
     line = {
