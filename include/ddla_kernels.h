@@ -154,7 +154,7 @@ int ddlak_diag_logsum_grid(char type, int n, const void* A, long long lld, int l
  * (ddlak_potrf_mixed uses DDLAK_MIXED_GROUP; ddlak_potrf_mixed_grouped takes
  * 1 .. DDLAK_MIXED_MAX_GROUP). */
 #define DDLAK_MIXED_GROUP 4
-#define DDLAK_MIXED_MAX_GROUP 4
+#define DDLAK_MIXED_MAX_GROUP 8
 
 /* Bytes of one of the two panel-operand slots of an order-n factorization
  * (enough for any group up to DDLAK_MIXED_MAX_GROUP). */

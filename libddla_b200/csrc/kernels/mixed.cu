@@ -991,9 +991,13 @@ cudaError_t potrf_mixed_enqueue(float* W, long long ldw, int n, int G, void* P0,
 // compute stream st, panel c waits only for its own arrival, so the copies of
 // the later panels overlap the factorization of the earlier ones:
 //   1. W(panel) = fl32(A(panel)), column / row sums for ||A||_inf;
-//   2. the panel takes the update from every earlier column in ONE launch,
+//   2. the panel takes the update from every earlier column,
 //      W(i, j) -= sum_{k < c0} Lk(i, k) Lk(j, k), from Lk, the K-contiguous
-//      low-precision copy of L the factorization appends to (row stride ldk);
+//      low-precision copy of L the factorization appends to (row stride ldk),
+//      in launches of 1024 columns of K (each subtracts its partial sum in FP32):
+//      the columns of panels 0 .. c-2 on the compute stream while the previous
+//      panel's chain still runs on a high-priority stream (look-ahead), those
+//      of panel c-1 on that stream once its chain is done;
 //   3. its G block columns are factored one after the other, block g after the
 //      update from blocks 0..g-1 of the panel (from Lk as well), with the FP64
 //      diagonal block and the panel solve of the right-looking form, and each
@@ -1016,17 +1020,25 @@ cudaError_t potrf_mixed_stream_enqueue(int n, int G, const double* Ah, long long
     auto lk_at = [&](long long row, long long k) -> void* {
         return static_cast<unsigned char*>(Lk) + (size_t)(row * ldk + k) * esz;
     };
-    std::vector<cudaEvent_t> arrive((size_t)S, nullptr);
+    // events: each panel's arrival, the end of its update from the earlier panels (on st)
+    // and the end of its chain (on the high-priority stream)
+    std::vector<cudaEvent_t> ev((size_t)3 * S, nullptr);
     cudaError_t e = cudaSuccess;
-    for (int c = 0; c < S && e == cudaSuccess; ++c) e = cudaEventCreateWithFlags(&arrive[c], cudaEventDisableTiming);
+    for (size_t i = 0; i < ev.size() && e == cudaSuccess; ++i)
+        e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
     auto release = [&] {
-        for (cudaEvent_t ev : arrive)
-            if (ev) cudaEventDestroy(ev);  // resources go once the recorded work is done
+        for (cudaEvent_t x : ev)
+            if (x) cudaEventDestroy(x);  // resources go once the recorded work is done
     };
     if (e != cudaSuccess) {
         release();
         return e;
     }
+    cudaEvent_t* arrive = ev.data();
+    cudaEvent_t* big = ev.data() + S;
+    cudaEvent_t* chained = ev.data() + 2 * S;
+    MixedStreams& MS = mixed_streams();
+    cudaStream_t hs = MS.hi;
     for (int c = 0; c < S && e == cudaSuccess; ++c) {
         const long long c0 = (long long)c * SW, w = std::min<long long>(SW, n - c0);
         e = cudaMemcpy2DAsync(Ad + c0 + c0 * ldad, (size_t)ldad * 8, Ah + c0 + c0 * ldah, (size_t)ldah * 8,
@@ -1035,6 +1047,14 @@ cudaError_t potrf_mixed_stream_enqueue(int n, int G, const double* Ah, long long
     }
     if (e == cudaSuccess) e = cudaMemsetAsync(colsum, 0, sizeof(double) * n, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(anrm, 0, sizeof(double), st);
+    if (e == cudaSuccess) e = cudaEventRecord(MS.start, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(hs, MS.start, 0);
+    // Look-ahead: on st, panel c is converted and takes the update from the panels
+    // 0 .. c-2 (whose chains are done) while the high-priority stream still runs the
+    // chain of panel c-1; then, on that stream, panel c takes the update from panel
+    // c-1 and its own chain runs.  The two streams write disjoint panels of W and
+    // disjoint columns of Lk.
+    constexpr long long KL = 1024;
     for (int c = 0; c < S && e == cudaSuccess; ++c) {
         const long long c0 = (long long)c * SW, w = std::min<long long>(SW, n - c0);
         if ((e = cudaStreamWaitEvent(st, arrive[c], 0)) != cudaSuccess) break;
@@ -1045,34 +1065,49 @@ cudaError_t potrf_mixed_stream_enqueue(int n, int G, const double* Ah, long long
                                                                                 (int)jt);
         }
         note_launches(1);
-        if (c0 > 0 &&
-            (e = mixed_update<TF32>(W, ldw, n, c0, 0, (int)w, Lk, ldk, (int)c0, dinfo, status, st)) != cudaSuccess)
+        // the update from the columns of panels 0 .. c-2, in launches of at most KL columns:
+        // each launch's partial sum is subtracted from W in FP32 by the epilogue, as the
+        // right-looking form does per super-step (one tensor-core accumulation over the
+        // whole of K, up to n, measured a less accurate factor: more refinement sweeps)
+        const long long kfar = c0 - SW;
+        if (kfar > 0 && (e = cudaStreamWaitEvent(st, chained[c - 2], 0)) != cudaSuccess) break;
+        for (long long k0 = 0; k0 < kfar && e == cudaSuccess; k0 += KL)
+            e = mixed_update<TF32>(W, ldw, n, c0, 0, (int)w, lk_at(0, k0), ldk, (int)std::min(KL, kfar - k0), dinfo,
+                                   status, st);
+        if (e == cudaSuccess) e = cudaEventRecord(big[c], st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(hs, big[c], 0);
+        if (e != cudaSuccess) break;
+        // on the chain's stream: the update from panel c-1, then the panel's block columns
+        if (c0 > 0 && (e = mixed_update<TF32>(W, ldw, n, c0, 0, (int)w, lk_at(0, c0 - SW), ldk, (int)SW, dinfo,
+                                              status, hs)) != cudaSuccess)
             break;
         for (int g = 0; g < G && e == cudaSuccess; ++g) {
             const long long kg = c0 + (long long)g * NB;
             if (kg >= n) break;
             const int nbk = (long long)n - kg < NB ? (int)(n - kg) : NB;
             if (g > 0 && (e = mixed_update<TF32>(W, ldw, n, kg, 0, nbk, lk_at(0, c0), ldk, g * NB, dinfo, status,
-                                                 st)) != cudaSuccess)
+                                                 hs)) != cudaSuccess)
                 break;
             {
-                ProfScope ps(PK_MIXED_OTHER, st, (double)nbk * nbk * nbk / 3.0, 4.0 * nbk * (nbk + 1));
-                k_potrf_diag_mixed<<<1, 256, (size_t)nbk * (nbk + 1) * sizeof(double), st>>>(W, ldw, (int)kg, nbk,
+                ProfScope ps(PK_MIXED_OTHER, hs, (double)nbk * nbk * nbk / 3.0, 4.0 * nbk * (nbk + 1));
+                k_potrf_diag_mixed<<<1, 256, (size_t)nbk * (nbk + 1) * sizeof(double), hs>>>(W, ldw, (int)kg, nbk,
                                                                                              dinfo);
             }
             note_launches(1);
             if (kg + nbk >= n) break;  // the last block column: nothing to its right
-            if ((e = launch_trsm_panel<float, false>(W, ldw, (int)kg, nbk, n, dinfo, st)) != cudaSuccess) break;
+            if ((e = launch_trsm_panel<float, false>(W, ldw, (int)kg, nbk, n, dinfo, hs)) != cudaSuccess) break;
             {
                 const long long m = (long long)n - kg;
-                ProfScope ps(PK_MIXED_OTHER, st, 0.0, (double)m * NB * (4.0 + (TF32 ? 4.0 : 2.0)));
-                k_pack_panel<TF32><<<dim3((unsigned)ceil_div(m, 32), NB / 32), dim3(32, 8), 0, st>>>(
+                ProfScope ps(PK_MIXED_OTHER, hs, 0.0, (double)m * NB * (4.0 + (TF32 ? 4.0 : 2.0)));
+                k_pack_panel<TF32><<<dim3((unsigned)ceil_div(m, 32), NB / 32), dim3(32, 8), 0, hs>>>(
                     W, ldw, n, kg, (int)kg, NB, lk_at(kg, kg), ldk, dinfo);
             }
             note_launches(1);
             e = cudaGetLastError();
         }
+        if (e == cudaSuccess) e = cudaEventRecord(chained[c], hs);
     }
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, chained[S - 1], 0);
     if (e == cudaSuccess) {
         k_max_nonneg<<<148, 256, 0, st>>>(colsum, n, anrm);
         note_launches(1);

@@ -166,3 +166,37 @@ def test_not_positive_definite_raises():
     A[1, 10, 10] = -5.0
     with pytest.raises(RuntimeError, match="matrix 1"):
         _ag().chol_nll(A, y)
+
+
+@pytest.mark.parametrize("n,batch", [(1, 3), (15, 2), (17, 5), (33, 1), (100, 4), (255, 2), (512, 1), (1000, 3),
+                                     (1024, 2)])
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_trtri_batched_inverse(n, batch, dtype):
+    """ddlak_trtri_batched (W = L^-1, the lower triangle) against the inverse
+    of the same factor, at orders that do and do not fill the 16-column block columns and
+    32-row blocks, with batches small enough that each matrix is split over several CTAs."""
+    import ctypes
+
+    torch = _t()
+    from libddla_b200.ddla import _c_api as C
+
+    dt = getattr(torch, dtype)
+    A, _ = spd(batch, n, torch.float64, 500 + n)
+    Lf = torch.linalg.cholesky(A)
+    L = Lf.to(dt).transpose(1, 2).contiguous().transpose(1, 2)  # column-major per matrix
+    L = L.permute(0, 2, 1).contiguous()  # row-major storage of L^T = column-major L
+    W = torch.full_like(L, float("nan"))
+    f = C.lib.ddlak_trtri_batched
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_char, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong, ctypes.c_longlong,
+                  ctypes.c_void_p, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_void_p]
+    torch.cuda.synchronize()
+    assert f(b"d" if dtype == "float64" else b"s", batch, n, L.data_ptr(), n, n * n, W.data_ptr(), n, n * n,
+             None) == 0
+    torch.cuda.synchronize()
+    Wc = W.permute(0, 2, 1).double()  # back to (row, col) indexing
+    ref = torch.linalg.inv(L.permute(0, 2, 1).double())
+    low = torch.tril(torch.ones(n, n, dtype=torch.bool, device=W.device))
+    assert bool(torch.isfinite(Wc[:, low]).all())
+    err = (Wc[:, low] - ref[:, low]).abs().max() / ref.abs().max()
+    assert err < (1e-12 if dtype == "float64" else 1e-4), err

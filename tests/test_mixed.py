@@ -167,3 +167,34 @@ def test_pposv_mixed_not_positive_definite_falls_back(handle):
     _, info, rep = ddla.pposv_mixed(dA, dB, dX, precision="B")
     assert info == 201
     assert rep["iter"] < 0
+
+
+@pytest.mark.parametrize("group", [1, 3, 5, 8])
+def test_grouped_tensor_core_factorization(handle, group):
+    """ddlak_potrf_mixed_grouped: every super-step width up to the maximum gives a factor
+    at the TF32 rounding level, on an order that fills no super-step exactly."""
+    n = 1500
+    rng = np.random.default_rng(40 + group)
+    A = _spd(rng, n)
+    ldw = (n + 3) // 4 * 4
+    W = np.zeros((ldw, n), dtype=np.float32, order="F")
+    W[:n, :n] = np.tril(A).astype(np.float32)
+    vp, i, ll, c = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_char
+    pb = _k("ddlak_mixed_panel_bytes", i)
+    pb.restype = ctypes.c_ulonglong
+    f = _k("ddlak_potrf_mixed_grouped", c, i, i, vp, ll, vp, vp, vp, vp, vp)
+    dW = _dev(handle, W)
+    P0, P1 = handle.malloc(pb(n)), handle.malloc(pb(n))
+    dI = handle.malloc(256)
+    try:
+        assert f(b"T", group, n, dW, ldw, P0, P1, dI, dI + 4, _stream(handle)) == 0
+        out = np.zeros(2, dtype=np.int32)
+        handle.memcpy(out.ctypes.data, dI, 8)
+        handle.memcpy(W.ctypes.data, dW, W.nbytes)
+        handle.synchronize()
+        assert out[1] == 0 and out[0] == 0, out
+        L = np.tril(W[:n, :n]).astype(np.float64)
+        assert np.linalg.norm(A - L @ L.T) / np.linalg.norm(A) < 4e-3
+    finally:
+        for p in (dW, P0, P1, dI):
+            handle.free(p)
