@@ -241,9 +241,133 @@ DDLAK_INST_SIMT(cf64, true)
 // ---------------------------------------------------------------------------
 template <class T> constexpr int potrf_nb() { return sizeof(T) == 16 ? 64 : 128; }
 
+// ---------------------------------------------------------------------------
+// The FP32 panel of the mixed factorization (lower storage, nbk <= 128): one
+// thread per row.  X L11^T = A21 along the row, in two halves of 64 columns so
+// that at most 64 of the row's values are live in registers:
+//   1. x1 = row[0:64] solved against L11[0:64, 0:64] (x_j *= 1 / l_jj,
+//      x_k -= x_j l_kj for k > j), written back and staged in shared memory;
+//   2. x2 = row[64:128] - x1 L11[64:128, 0:64]^T, then solved against
+//      L11[64:128, 64:128], written back.
+// Columns of L11 are read from shared memory as float4 broadcasts (every thread
+// of the warp reads the same address); the row loads and stores are coalesced
+// (consecutive threads, consecutive rows of the column-major panel), and no
+// shuffle sits on the per-column chain.
+// ---------------------------------------------------------------------------
+constexpr int TRR_NT = 128;
+constexpr size_t TRR_SMEM = (128 * 128 + 64 * TRR_NT) * sizeof(float);
+
+// a shared-memory float4 load kept in program order (the unrolled substitution would
+// otherwise hoist hundreds of them ahead of their use and run out of registers)
+__device__ __forceinline__ float4 ld_shared_f4(const float4* p)
+{
+    float4 v;
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+    return v;
+}
+
+// x (64 values at column offset c0) against the 64 x 64 diagonal part of L11 at (c0, c0)
+__device__ __forceinline__ void trr_solve64(float (&x)[64], const float* l11, const float* rinv, int c0)
+{
+#pragma unroll
+    for (int j = 0; j < 64; ++j) {
+        x[j] *= rinv[c0 + j];
+        const float4* col = reinterpret_cast<const float4*>(&l11[(c0 + j) * 128 + c0]);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            if (4 * q + 3 > j) {
+                const float4 l = ld_shared_f4(col + q);
+                if (4 * q + 0 > j) x[4 * q + 0] = fmaf(-x[j], l.x, x[4 * q + 0]);
+                if (4 * q + 1 > j) x[4 * q + 1] = fmaf(-x[j], l.y, x[4 * q + 1]);
+                if (4 * q + 2 > j) x[4 * q + 2] = fmaf(-x[j], l.z, x[4 * q + 2]);
+                if (4 * q + 3 > j) x[4 * q + 3] = fmaf(-x[j], l.w, x[4 * q + 3]);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(TRR_NT) k_trsm_panel_rows(float* __restrict__ A, long long lda, int k0, int nbk,
+                                                            int n, const int* __restrict__ info)
+{
+    extern __shared__ __align__(16) float trr_smem[];
+    float* l11 = trr_smem;               // l11[j * 128 + k] = L(k0 + k, k0 + j), zero for k < j or k >= nbk
+    float* xs = trr_smem + 128 * 128;    // xs[j * TRR_NT + t]: thread t's solved first half
+    __shared__ float rinv[128];
+    if (*(volatile const int*)info != 0) return;
+    const float* Ad = A + k0 + (long long)k0 * lda;
+    for (int idx = threadIdx.x; idx < 128 * 32; idx += TRR_NT) {
+        const int j = idx >> 5, k4 = (idx & 31) * 4;
+        float v[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int k = k4 + e;
+            v[e] = (j < nbk && k < nbk && k >= j) ? Ad[k + (long long)j * lda] : 0.f;
+        }
+        *reinterpret_cast<float4*>(&l11[j * 128 + k4]) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+    __syncthreads();
+    rinv[threadIdx.x] = threadIdx.x < nbk ? 1.f / l11[threadIdx.x * 129] : 0.f;
+    __syncthreads();
+    const int t = threadIdx.x;
+    const long long row = (long long)k0 + nbk + (long long)blockIdx.x * TRR_NT + t;
+    const bool live = row < n;
+    float* Ar = A + (live ? row : (long long)k0) + (long long)k0 * lda;
+    float x[64];
+#pragma unroll
+    for (int c = 0; c < 64; ++c) x[c] = (live && c < nbk) ? Ar[(long long)c * lda] : 0.f;
+    trr_solve64(x, l11, rinv, 0);
+    {
+        // the row's addresses are recomputed here rather than kept live through the solve
+        float* p = Ar;
+        long long ld = lda;
+        asm volatile("" : "+l"(p), "+l"(ld));
+#pragma unroll
+        for (int c = 0; c < 64; ++c) {
+            if (live && c < nbk) p[(long long)c * ld] = x[c];
+            xs[c * TRR_NT + t] = x[c];
+        }
+    }
+    if (nbk <= 64) return;  // uniform: no barrier follows
+#pragma unroll
+    for (int c = 0; c < 64; ++c) x[c] = (live && 64 + c < nbk) ? Ar[(long long)(64 + c) * lda] : 0.f;
+#pragma unroll 4
+    for (int j = 0; j < 64; ++j) {
+        const float xj = xs[j * TRR_NT + t];
+        const float4* col = reinterpret_cast<const float4*>(&l11[j * 128 + 64]);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const float4 l = ld_shared_f4(col + q);
+            x[4 * q + 0] = fmaf(-xj, l.x, x[4 * q + 0]);
+            x[4 * q + 1] = fmaf(-xj, l.y, x[4 * q + 1]);
+            x[4 * q + 2] = fmaf(-xj, l.z, x[4 * q + 2]);
+            x[4 * q + 3] = fmaf(-xj, l.w, x[4 * q + 3]);
+        }
+    }
+    trr_solve64(x, l11, rinv, 64);
+    {
+        float* p = Ar;
+        long long ld = lda;
+        asm volatile("" : "+l"(p), "+l"(ld));
+#pragma unroll
+        for (int c = 0; c < 64; ++c)
+            if (live && 64 + c < nbk) p[(long long)(64 + c) * ld] = x[c];
+    }
+}
+
 template <class T, bool UP>
 cudaError_t launch_trsm_panel(T* A, long long lda, int k0, int nbk, int n, const int* dinfo, cudaStream_t s)
 {
+    if constexpr (std::is_same<T, float>::value && !UP) {
+        const long long m = (long long)n - k0 - nbk;
+        if (m <= 0) return cudaSuccess;
+        if (cudaError_t e = smem_optin(k_trsm_panel_rows, TRR_SMEM); e != cudaSuccess) return e;
+        const double md = (double)m, b = nbk;
+        ProfScope ps(PK_TRSM_PANEL, s, md * b * b, sizeof(T) * (2.0 * md * b + b * (b + 1) / 2));
+        k_trsm_panel_rows<<<(unsigned)ceil_div(m, TRR_NT), TRR_NT, TRR_SMEM, s>>>(A, lda, k0, nbk, n, dinfo);
+        note_launches(1);
+        return cudaGetLastError();
+    }
     constexpr int NQ = potrf_nb<T>() / 32;
     constexpr int PR = sizeof(T) >= 16 ? 4 : 8;
     const size_t panel_smem = (size_t)(NQ * 32) * (NQ * 32 + 1) * sizeof(T);
