@@ -599,10 +599,20 @@ def gp_leg(args, torch, device):
     y = torch.randn(B, n, generator=g, device=device, dtype=torch.float64)
     th = torch.tensor([0.3, 1.0, 1e-2], dtype=torch.float64, device=device, requires_grad=True)
 
+    dist = torch.distributed
+    world = dist.get_world_size() if dist.is_available() and dist.is_initialized() else 1
+    red = torch.zeros(4, dtype=torch.float64, device=device)
+
     def ours():
         th.grad = None
         loss = ag.gp_nll(X, y, th).sum()
         loss.backward()
+        if world > 1:
+            # data-parallel fit: every rank holds its own problems; the summed likelihood and its
+            # theta-gradient (4 doubles) are all-reduced once per step
+            red[0] = loss.detach()
+            red[1:] = th.grad
+            dist.all_reduce(red)
         return loss
 
     def se(Xb, t):
@@ -679,8 +689,10 @@ def gp_leg(args, torch, device):
     big_err = None
     if not args.no_gp_large:
         big_err = gp_large_gradient_check(torch, device, X2, y2, th2.grad.detach().clone())
-    return {"metric": "GP marginal likelihood logdet+grad evaluations/s", "value": rate, "unit": "1/s",
-            "ms_per_step": ms, "dtype": "f64",
+    return {"metric": "GP marginal likelihood logdet+grad evaluations/s", "value": rate * world, "unit": "1/s",
+            "ms_per_step": ms, "dtype": "f64", "ranks": world,
+            "exchange": "all-reduce (sum) of the likelihood and dloss/dtheta, 4 doubles per step" if world > 1
+            else "none (one rank)",
             "config": {"workload": f"{B} x n={n} SE-kernel GPs, points U[0,1]^2, l=0.3 sigma_f^2=1 sigma^2=1e-2, "
                                    "loss = 1/2 (y^T A^-1 y + logdet A), dloss/dtheta by the adjoint kernels",
                        "loop": f"torch.linalg.cholesky/cholesky_solve + autograd one matrix at a time "
