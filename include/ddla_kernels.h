@@ -220,9 +220,16 @@ int ddlak_bis_block(void);
 unsigned long long ddlak_bis_inverse_bytes(int n);
 int ddlak_bis_inverse(int n, const void* L32, long long ldl, void* Dinv, void* tmp, void* stream);
 int ddlak_bis_inverse_narrow(int n, const void* Dinv, void* Dinv32, void* stream);
+/* The same inverse blocks from an FP64 factor (lower, even ldl), read in place. */
+int ddlak_bis_inverse_f64(int n, const void* L, long long ldl, void* Dinv, void* stream);
 unsigned long long ddlak_bis_solve_workspace(int n, int nrhs);
 int ddlak_bis_solve(int n, int nrhs, const void* L32, long long ldl, const void* Dinv, void* B, long long ldb,
                     void* work, unsigned long long work_bytes, void* stream);
+/* L L^T X = B with an FP64 factor (lower, even ldl, 16-byte aligned), FP64 vectors and the
+ * FP64 inverse blocks of ddlak_bis_inverse_f64: the FP64 form of the same persistent solve
+ * (the plain ppotrs for nrhs <= 16 at large orders). */
+int ddlak_bis_solve_f64(int n, int nrhs, const void* L, long long ldl, const void* Dinv, void* B, long long ldb,
+                        void* work, unsigned long long work_bytes, void* stream);
 int ddlak_bis_solve_f32(int n, int nrhs, const void* L32, long long ldl, const void* Dinv32, void* B, long long ldb,
                         void* work, unsigned long long work_bytes, void* stream);
 /* Host-side view of that solve's unit queue (no device work): the number of

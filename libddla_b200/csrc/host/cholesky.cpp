@@ -132,13 +132,32 @@ void ppotrf_run(const DdlaHandle_t& h, char uplo, int n, T* A, int, int, const i
     info = read_device_int(h, dinfo);
 }
 
+// The plain FP64 solve at large orders with few right-hand sides (uplo 'L', side 'L',
+// nrhs <= 16) runs as the persistent solve by inverted 1024-row diagonal blocks
+// (ddlak_bis_inverse_f64 + ddlak_bis_solve_f64): a few dozen diagonal blocks instead
+// of a chain of n / 64 block rows per direction.  Below kBisMinOrder the fused
+// 64-row solve is faster (the inverses cost O(n * 1024^2)).
+constexpr int kBisMinOrder = 4096;
+
+template <typename T>
+bool bis_candidate(char side, int n, int nrhs)
+{
+    return std::is_same<T, double>::value && side == 'L' && n >= kBisMinOrder && nrhs >= 1 && nrhs <= 16;
+}
+
+std::size_t bis_bytes(int n, int nrhs)
+{
+    return detail::padded_bytes<char>(static_cast<std::size_t>(ddlak_bis_inverse_bytes(n))) +
+           static_cast<std::size_t>(ddlak_bis_solve_workspace(n, nrhs));
+}
+
 template <typename T>
 void ppotrs_workspace_size(const DdlaHandle_t&, char side, int n, int nrhs, const int*, const int*,
                            std::size_t* backend_bytes, std::size_t* host_bytes)
 {
-    (void)side;
     *host_bytes = 0;
     *backend_bytes = (n > 0 && nrhs > 0) ? static_cast<std::size_t>(ddlak_potrs_workspace(n, nrhs)) : 0;
+    if (bis_candidate<T>(side, n, nrhs)) *backend_bytes = std::max(*backend_bytes, bis_bytes(n, nrhs));
 }
 
 template <typename T>
@@ -148,6 +167,20 @@ void ppotrs_run(const DdlaHandle_t& h, char side, char uplo, char, int n, int nr
     if (n == 0 || nrhs == 0) return;
     if (h->nprocs > 1) {  // a grid of several ranks: the distributed solve (its own scratch)
         grid::ppotrs_grid<T>(h, side, uplo, n, nrhs, A, descA, B, descB);
+        return;
+    }
+    const long long lda = descA[DDLA_LLD_];
+    if (bis_candidate<T>(side, n, nrhs) && uplo == 'L' && !(lda & 1) &&
+        !(reinterpret_cast<std::uintptr_t>(A) & 15) && backend_work != nullptr && backend_bytes >= bis_bytes(n, nrhs)) {
+        char* w = static_cast<char*>(backend_work);
+        void* Dinv = w;
+        void* swork = w + detail::padded_bytes<char>(static_cast<std::size_t>(ddlak_bis_inverse_bytes(n)));
+        const std::size_t sbytes = backend_bytes - static_cast<std::size_t>(static_cast<char*>(swork) - w);
+        detail::kernel_check(ddlak_bis_inverse_f64(n, A, lda, Dinv, h->stream), "diagonal block inverses");
+        detail::kernel_check(ddlak_bis_solve_f64(n, nrhs, A, lda, Dinv, B, descB[DDLA_LLD_], swork, sbytes, h->stream),
+                             "persistent solve");
+        if (read_device_int(h, static_cast<const int*>(swork)) != 0)
+            throw std::runtime_error("ppotrs: a device wait in the persistent solve timed out");
         return;
     }
     const unsigned long long need = ddlak_potrs_workspace(n, nrhs);

@@ -57,7 +57,8 @@ constexpr int CQ = 8;     // right-hand sides per pass
 constexpr int CH_NT = 512;
 
 // tmp[s] (BS x BS, ld BS) = FP64 copy of the lower triangle of the diagonal block s of L32
-__global__ void k_bis_widen(int n, const float* __restrict__ L, long long ldl, double* __restrict__ tmp)
+template <class LT>
+__global__ void k_bis_widen(int n, const LT* __restrict__ L, long long ldl, double* __restrict__ tmp)
 {
     const int s = blockIdx.z;
     const long long s0 = (long long)s * BS;
@@ -95,7 +96,6 @@ __global__ void k_bis_narrow(long long count, const double* __restrict__ src, fl
 struct Chain {
     int n, S, Tt;
     long long nf, total;
-    const float* L;
     long long ldl;
     int* ctl;  // [0] status, [1] fdone, [2..3] queue head (64-bit)
     int* cnt_f;
@@ -271,14 +271,14 @@ template <> struct VecIO<double> {
 
 // Every unit streams its matrix through shared memory in 64 KB chunks, one
 // TMA box each: a 64-row x KC-column box of L or of the inverse blocks for the
-// row units (KC = 256 for FP32, 128 for FP64), a 256-row x 64-column box of L
-// for the column units.  A TMA box costs a CTA about half a microsecond however
+// row units (KC = 256 for FP32, 128 for FP64), a PR-row x 64-column box of L
+// for the column units (PR = 256 for an FP32 factor, 128 for FP64).  A TMA box costs a CTA about half a microsecond however
 // large it is, so the boxes are as large as two stages of shared memory allow;
 // a sliced unit is one box, prefetched in full while the unit waits.
 constexpr int CHUNK = 65536;
 constexpr int NSTAGE = 2;
 template <class MT> constexpr int chunk_cols() { return CHUNK / (CT * (int)sizeof(MT)); }
-constexpr int PT_ROWS = CHUNK / (CT * 4);  // rows of a column-unit chunk (256)
+template <class LT> constexpr int pt_rows() { return CHUNK / (CT * (int)sizeof(LT)); }  // rows of a column-unit chunk
 
 // Row unit, one chunk: acc(4g+u, q) += sum over this thread's columns of the
 // chunk (k-slice ks of 32) of M(4g+u, k) V(k, q), M(r, k) at tile[k*64 + r]
@@ -312,28 +312,30 @@ __device__ __forceinline__ void row_chunk(const MT* tile, const T* vs, int j, in
     }
 }
 
-// Column unit, one chunk (rows j*256 .. j*256+255 of the unit, 64 columns,
-// tile[c*256 + r]): warp w owns columns 4w..4w+3, lane l the rows 4l..4l+3 and
-// 128+4l..128+4l+3, so the 32 lanes read 512 contiguous bytes of a column.
-// xq holds the vector q-major (xq[q*XQ + row]), read the same way.  The sum
-// over the lanes is taken once per unit (col_reduce).
-constexpr int XQ = BS + PT_ROWS;  // rows of the q-major vector
-template <class T>
-__device__ __forceinline__ void col_chunk(const float* tile, const T* xq, int j, T (&acc)[4][CQ])
+// Column unit, one chunk (rows j*PR .. j*PR+PR-1 of the unit, 64 columns,
+// tile[c*PR + r]): warp w owns columns 4w..4w+3, lane l the rows 4l..4l+3 of
+// each 128-row step, so the 32 lanes read 512 (FP32) or 1024 (FP64) contiguous
+// bytes of a column.  xq holds the vector q-major (xq[q*XQ + row]), read the
+// same way.  The sum over the lanes is taken once per unit (col_reduce).
+template <class LT> constexpr int xq_rows() { return BS + pt_rows<LT>(); }  // rows of the q-major vector
+template <class T, class LT>
+__device__ __forceinline__ void col_chunk(const LT* tile, const T* xq, int j, T (&acc)[4][CQ])
 {
+    constexpr int PR = pt_rows<LT>(), XQ = xq_rows<LT>();
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
-    for (int step = 0; step < 2; ++step) {
+    for (int step = 0; step < PR / 128; ++step) {
         const int r = step * 128 + 4 * lane;
         T x[CQ][4];
 #pragma unroll
-        for (int q = 0; q < CQ; ++q) VecIO<T>::ld4(xq + q * XQ + j * PT_ROWS + r, x[q]);
+        for (int q = 0; q < CQ; ++q) VecIO<T>::ld4(xq + q * XQ + j * PR + r, x[q]);
 #pragma unroll
         for (int cc = 0; cc < 4; ++cc) {
-            const float4 l = *reinterpret_cast<const float4*>(tile + (4 * w + cc) * PT_ROWS + r);
+            LT l[4];
+            VecIO<LT>::ld4(tile + (4 * w + cc) * PR + r, l);
 #pragma unroll
             for (int q = 0; q < CQ; ++q)
-                acc[cc][q] = fma((T)l.w, x[q][3], fma((T)l.z, x[q][2], fma((T)l.y, x[q][1], fma((T)l.x, x[q][0], acc[cc][q]))));
+                acc[cc][q] = fma((T)l[3], x[q][3], fma((T)l[2], x[q][2], fma((T)l[1], x[q][1], fma((T)l[0], x[q][0], acc[cc][q]))));
         }
     }
 }
@@ -369,7 +371,7 @@ template <class T>
 constexpr size_t chain_smem()
 {
     static_assert((size_t)NSTAGE * CHUNK >= sizeof(T) * (CH_NT / 32) * CT * CQ, "reduction does not fit the stages");
-    static_assert(VS_ROWS * CQ >= XQ * CQ, "vector staging");
+    static_assert(VS_ROWS >= xq_rows<float>() && VS_ROWS >= xq_rows<double>(), "vector staging");
     return 1024 + (size_t)NSTAGE * CHUNK + sizeof(T) * (size_t)VS_ROWS * CQ;
 }
 
@@ -391,7 +393,7 @@ __device__ __forceinline__ bool wait_inputs(const Chain& c, int kind, int s, int
     return __all_sync(0xffffffffu, ok);
 }
 
-template <class T>
+template <class T, class LT>
 __global__ void __launch_bounds__(CH_NT, 1) k_bis_chain(const __grid_constant__ CUtensorMap mapL,
                                                         const __grid_constant__ CUtensorMap mapLt,
                                                         const __grid_constant__ CUtensorMap mapD, Chain c,
@@ -410,7 +412,9 @@ __global__ void __launch_bounds__(CH_NT, 1) k_bis_chain(const __grid_constant__ 
     unsigned long long* head = reinterpret_cast<unsigned long long*>(c.ctl + 2);
     const int tid = threadIdx.x;
     constexpr int KCD = chunk_cols<T>();      // inverse-block columns per chunk
-    constexpr int KCL = chunk_cols<float>();  // factor columns per chunk (row units)
+    constexpr int KCL = chunk_cols<LT>();  // factor columns per chunk (row units)
+    constexpr int PR = pt_rows<LT>();      // factor rows per chunk (column units)
+    constexpr int XQ = xq_rows<LT>();
     if (tid == 0) {
         for (int s = 0; s < NS; ++s) tc::mbar_init(&full[s], 1);
         tc::mbar_fence_init();
@@ -455,7 +459,7 @@ __global__ void __launch_bounds__(CH_NT, 1) k_bis_chain(const __grid_constant__ 
             vsrc = Y + (s0 + kb) * CQ;
         } else {
             ke = bulk ? bsz : min(kb + KS, bsz);
-            nch = (ke - kb + PT_ROWS - 1) / PT_ROWS;
+            nch = (ke - kb + PR - 1) / PR;
             vsrc = X + (s0 + kb) * CQ;
         }
         auto issue = [&](int j) {
@@ -467,7 +471,7 @@ __global__ void __launch_bounds__(CH_NT, 1) k_bis_chain(const __grid_constant__ 
             else if (kind == 1)
                 tc::tma_load_2d(dst, &mapL, &full[st], idx * CT, (int)(s0 + kb + j * KCL));
             else
-                tc::tma_load_2d(dst, &mapLt, &full[st], (int)(s0 + kb + j * PT_ROWS), idx * CT);
+                tc::tma_load_2d(dst, &mapLt, &full[st], (int)(s0 + kb + j * PR), idx * CT);
         };
         auto prefetch = [&](int j) {
             if (kind == 0 || kind == 2)
@@ -475,7 +479,7 @@ __global__ void __launch_bounds__(CH_NT, 1) k_bis_chain(const __grid_constant__ 
             else if (kind == 1)
                 tc::tma_prefetch_l2_2d(&mapL, idx * CT, (int)(s0 + kb + j * KCL));
             else
-                tc::tma_prefetch_l2_2d(&mapLt, (int)(s0 + kb + j * PT_ROWS), idx * CT);
+                tc::tma_prefetch_l2_2d(&mapLt, (int)(s0 + kb + j * PR), idx * CT);
         };
         const int npro = nch < NS ? nch : NS;
         if (tid == 0) {
@@ -508,7 +512,7 @@ __global__ void __launch_bounds__(CH_NT, 1) k_bis_chain(const __grid_constant__ 
                 dst[e] = (e / PER) < vavail ? __ldcg(src + e) : make_float4(0.f, 0.f, 0.f, 0.f);
         } else {
             constexpr int QP = 16 / (int)sizeof(T);  // right-hand sides per 16-byte piece
-            const int vlen = nch * PT_ROWS;
+            const int vlen = nch * PR;
             const float4* src = reinterpret_cast<const float4*>(vsrc);
             for (int e = tid; e < vlen * (CQ / QP); e += CH_NT) {
                 const int row = e / (CQ / QP), q0 = (e % (CQ / QP)) * QP;
@@ -536,11 +540,11 @@ __global__ void __launch_bounds__(CH_NT, 1) k_bis_chain(const __grid_constant__ 
             if (kind == 0)
                 row_chunk<T, T, 1>(reinterpret_cast<const T*>(tile), vs, j, kb, ke, rloc, g, ks, acc);
             else if (kind == 1)
-                row_chunk<T, float, 0>(reinterpret_cast<const float*>(tile), vs, j, kb, ke, rloc, g, ks, acc);
+                row_chunk<T, LT, 0>(reinterpret_cast<const LT*>(tile), vs, j, kb, ke, rloc, g, ks, acc);
             else if (kind == 2)
                 row_chunk<T, T, 2>(reinterpret_cast<const T*>(tile), vs, j, kb, ke, rloc, g, ks, acc);
             else
-                col_chunk<T>(reinterpret_cast<const float*>(tile), vs, j, acc);
+                col_chunk<T, LT>(reinterpret_cast<const LT*>(tile), vs, j, acc);
             __syncthreads();  // stage consumed by every thread
             if (tid == 0 && j + NS < nch) issue(j + NS);
         }
@@ -647,8 +651,8 @@ ChainLayout chain_layout(int n, size_t elem)
 }
 
 // workspace: [flags][Y][X][Bv]; the flags, Y and X start at zero
-template <class T>
-cudaError_t bis_chain_solve(int n, int nrhs, const float* L, long long ldl, const T* Dinv, double* B, long long ldb,
+template <class T, class LT>
+cudaError_t bis_chain_solve(int n, int nrhs, const LT* L, long long ldl, const T* Dinv, double* B, long long ldb,
                             void* work, cudaStream_t st)
 {
     if (n > (1 << 30) / 2) return cudaErrorInvalidValue;  // TMA coordinates are 32-bit
@@ -664,7 +668,6 @@ cudaError_t bis_chain_solve(int n, int nrhs, const float* L, long long ldl, cons
     c.Tt = lay.Tt;
     c.nf = lay.nf;
     c.total = lay.nf + lay.nb;
-    c.L = L;
     c.ldl = ldl;
     c.ctl = ctl;
     c.cnt_f = ctl + 64;
@@ -674,21 +677,22 @@ cudaError_t bis_chain_solve(int n, int nrhs, const float* L, long long ldl, cons
     const size_t smem = chain_smem<T>();
     CUtensorMap mapL, mapLt, mapD;
     const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
-    if (!tc::encode_colmajor_2d(&mapL, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, L, n, n, ldl, CT, chunk_cols<float>(),
+    const CUtensorMapDataType lt = sizeof(LT) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    if (!tc::encode_colmajor_2d(&mapL, lt, (int)sizeof(LT), L, n, n, ldl, CT, chunk_cols<LT>(),
                                 CU_TENSOR_MAP_SWIZZLE_NONE) ||
-        !tc::encode_colmajor_2d(&mapLt, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, L, n, n, ldl, PT_ROWS, CT,
+        !tc::encode_colmajor_2d(&mapLt, lt, (int)sizeof(LT), L, n, n, ldl, pt_rows<LT>(), CT,
                                 CU_TENSOR_MAP_SWIZZLE_NONE) ||
         !tc::encode_colmajor_2d(&mapD, dt, (int)sizeof(T), Dinv, BS, (long long)lay.S * BS, BS, CT, chunk_cols<T>(),
                                 CU_TENSOR_MAP_SWIZZLE_NONE))
         return cudaErrorInvalidValue;
-    if (cudaError_t e = smem_optin(k_bis_chain<T>, smem); e != cudaSuccess) return e;
+    if (cudaError_t e = smem_optin(k_bis_chain<T, LT>, smem); e != cudaSuccess) return e;
     // every CTA of the queue resident at once: SMs of this device x CTAs per SM
     int grid = 0;
     {
         int dev = 0, sms = 148, per = 1;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bis_chain<T>, CH_NT, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bis_chain<T, LT>, CH_NT, smem);
         grid = sms * (per > 0 ? per : 1);
     }
     const unsigned g = (unsigned)std::min<long long>(grid, c.total);
@@ -699,7 +703,7 @@ cudaError_t bis_chain_solve(int n, int nrhs, const float* L, long long ldl, cons
         cudaError_t e = cudaMemsetAsync(ctl, 0, lay.flag_bytes + 2 * lay.vec_bytes, st);
         if (e != cudaSuccess) return e;
         k_bis_pack<T><<<gv, 256, 0, st>>>(n, nr, B + r0 * ldb, ldb, Bv);
-        k_bis_chain<T><<<g, CH_NT, smem, st>>>(mapL, mapLt, mapD, c, Bv, Yv, Xv);
+        k_bis_chain<T, LT><<<g, CH_NT, smem, st>>>(mapL, mapLt, mapD, c, Bv, Yv, Xv);
         k_bis_unpack<T><<<gv, 256, 0, st>>>(n, nr, Xv, B + r0 * ldb, ldb, ctl);
         launches += 3;
     }
@@ -728,7 +732,7 @@ extern "C" int ddlak_bis_inverse(int n, const void* L32, long long ldl, void* Di
     {
         ProfScope ps(PK_MIXED_OTHER, st, (double)S * BS * BS * BS / 3.0, 16.0 * S * BS * BS);
         dim3 grid(BS / 32, BS / 32, S), block(32, 32);
-        k_bis_widen<<<grid, block, 0, st>>>(n, static_cast<const float*>(L32), ldl, static_cast<double*>(tmp));
+        k_bis_widen<float><<<grid, block, 0, st>>>(n, static_cast<const float*>(L32), ldl, static_cast<double*>(tmp));
         note_launches(1);
     }
     cudaError_t e = cudaGetLastError();
@@ -744,6 +748,31 @@ extern "C" int ddlak_bis_inverse(int n, const void* L32, long long ldl, void* Di
     if (r != 0) return r;
     dim3 grid(BS / 32, BS / 32, S), block(32, 32);
     k_bis_mirror<<<grid, block, 0, st>>>(static_cast<double*>(Dinv));
+    note_launches(1);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int ddlak_bis_inverse_f64(int n, const void* L, long long ldl, void* Dinv, void* stream)
+{
+    using namespace ddlak;
+    if (n <= 0) return 0;
+    if (!L || !Dinv || ldl < n) return (int)cudaErrorInvalidValue;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // the inverses straight from the factor's diagonal blocks (the batched inversion reads only
+    // their lower triangles): block s starts at L + s BS (ldl + 1)
+    const double* Ld = static_cast<const double*>(L);
+    double* D = static_cast<double*>(Dinv);
+    const long long bb = (long long)BS * BS, lstride = (long long)BS * (ldl + 1);
+    const int full = n / BS, last = n - full * BS;
+    int r = 0;
+    if (full > 0) r = ddlak_trtri_batched('d', full, BS, Ld, ldl, lstride, D, BS, bb, stream);
+    if (r == 0 && last > 0)
+        r = ddlak_trtri_batched('d', 1, last, Ld + (long long)full * lstride, ldl, lstride, D + full * bb, BS, bb,
+                                stream);
+    if (r != 0) return r;
+    const int S = (int)ceil_div(n, BS);
+    dim3 grid(BS / 32, BS / 32, S), block(32, 32);
+    k_bis_mirror<<<grid, block, 0, st>>>(D);
     note_launches(1);
     return (int)cudaGetLastError();
 }
@@ -818,8 +847,24 @@ extern "C" int ddlak_bis_solve(int n, int nrhs, const void* L32, long long ldl, 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const double nd = n, rd = nrhs;
     ProfScope ps(PK_POTRS_FUSED, st, 2.0 * nd * nd * rd, 4.0 * nd * (nd + 1));
-    return (int)bis_chain_solve<double>(n, nrhs, static_cast<const float*>(L32), ldl, static_cast<const double*>(Dinv),
+    return (int)bis_chain_solve<double, float>(n, nrhs, static_cast<const float*>(L32), ldl, static_cast<const double*>(Dinv),
                                         static_cast<double*>(B), ldb, work, st);
+}
+
+extern "C" int ddlak_bis_solve_f64(int n, int nrhs, const void* L, long long ldl, const void* Dinv, void* B,
+                                   long long ldb, void* work, unsigned long long work_bytes, void* stream)
+{
+    using namespace ddlak;
+    if (n <= 0 || nrhs <= 0) return 0;
+    if (nrhs > 16 || !L || !Dinv || !B || ldb < n || ldl < n || (ldl & 1) || (reinterpret_cast<uintptr_t>(L) & 15) ||
+        (reinterpret_cast<uintptr_t>(Dinv) & 15) || work_bytes < ddlak_bis_solve_workspace(n, nrhs))
+        return (int)cudaErrorInvalidValue;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const double nd = n, rd = nrhs;
+    ProfScope ps(PK_POTRS_FUSED, st, 2.0 * nd * nd * rd, 8.0 * nd * (nd + 1));
+    return (int)bis_chain_solve<double, double>(n, nrhs, static_cast<const double*>(L), ldl,
+                                                static_cast<const double*>(Dinv), static_cast<double*>(B), ldb, work,
+                                                st);
 }
 
 extern "C" int ddlak_bis_solve_f32(int n, int nrhs, const void* L32, long long ldl, const void* Dinv32, void* B,
@@ -831,6 +876,6 @@ extern "C" int ddlak_bis_solve_f32(int n, int nrhs, const void* L32, long long l
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const double nd = n, rd = nrhs;
     ProfScope ps(PK_POTRS_FUSED, st, 2.0 * nd * nd * rd, 4.0 * nd * (nd + 1));
-    return (int)bis_chain_solve<float>(n, nrhs, static_cast<const float*>(L32), ldl, static_cast<const float*>(Dinv32),
+    return (int)bis_chain_solve<float, float>(n, nrhs, static_cast<const float*>(L32), ldl, static_cast<const float*>(Dinv32),
                                        static_cast<double*>(B), ldb, work, st);
 }

@@ -83,3 +83,45 @@ def test_bis_solve_argument_errors(handle):
     assert solve(100, 8, 256, 102, 256, 256, 100, 256, 1 << 30, None) != 0
     assert solve(100, 8, 256, 100, 256, 256, 100, 256, 16, None) != 0
     assert solve(0, 8, None, 0, None, None, 0, None, 0, None) == 0
+
+
+@pytest.mark.parametrize("n,nrhs", [(1, 1), (63, 3), (1000, 8), (1024, 16), (1025, 8), (2111, 1), (3000, 9),
+                                    (4100, 8)])
+def test_bis_solve_fp64_factor_matches_numpy(handle, n, nrhs):
+    """The same persistent solve with an FP64 factor (the plain ppotrs at large orders): the
+    inverse blocks read in place from L (ddlak_bis_inverse_f64), FP64 boxes of 128 columns
+    for the row units and 128 rows for the column units; the upper triangle of L's storage
+    and its padding rows are NaN (never read)."""
+    rng = np.random.default_rng(77 * n + nrhs)
+    G = rng.standard_normal((n, n))
+    L = np.linalg.cholesky(G @ G.T / n + np.eye(n))
+    ldl = n + (n & 1) + 2  # even, with padding rows
+    Lp = np.full((ldl, n), np.nan, order="F")
+    Lp[:n, :n] = np.tril(L) + np.triu(np.full((n, n), np.nan), 1)
+    B = np.asfortranarray(rng.standard_normal((n, nrhs)))
+    vp, i, ll, ull = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_ulonglong
+    inv_bytes = _k("ddlak_bis_inverse_bytes", ull, i)(n)
+    ws = _k("ddlak_bis_solve_workspace", ull, i, i)(n, nrhs)
+    inverse = _k("ddlak_bis_inverse_f64", i, i, vp, ll, vp, vp)
+    solve = _k("ddlak_bis_solve_f64", i, i, i, vp, ll, vp, vp, ll, vp, ull, vp)
+    st = ctypes.c_void_p()
+    _C().check_status(_C().ddla_c_get_stream(handle.ptr, ctypes.byref(st)), "stream")
+    ptrs = []
+    try:
+        dL, dD, dW, dB = handle.malloc(Lp.nbytes), handle.malloc(inv_bytes), handle.malloc(ws), handle.malloc(B.nbytes)
+        ptrs += [dL, dD, dW, dB]
+        handle.memcpy(dL, Lp.ctypes.data, Lp.nbytes)
+        handle.memcpy(dB, B.ctypes.data, B.nbytes)
+        assert inverse(n, dL, ldl, dD, st) == 0
+        assert solve(n, nrhs, dL, ldl, dD, dB, n, dW, ws, st) == 0
+        X = np.empty_like(B)
+        status = np.zeros(1, dtype=np.int32)
+        handle.memcpy(X.ctypes.data, dB, X.nbytes)
+        handle.memcpy(status.ctypes.data, dW, 4)
+        handle.synchronize()
+    finally:
+        for p in ptrs:
+            handle.free(p)
+    assert status[0] == 0
+    Xref = np.linalg.solve(L @ L.T, B)
+    assert np.max(np.abs(X - Xref)) / np.max(np.abs(Xref)) < 1e-11
