@@ -36,6 +36,20 @@ int ddlak_potrf(char type, char uplo, int n, void* A, long long lda, int* dinfo,
 #define DDLAK_POTRF_MAX_GROUP 8
 int ddlak_potrf_grouped(char type, char uplo, int group, int n, void* A, long long lda, int* dinfo, void* stream);
 
+/* A batch of equal-order FP64 matrices (lower), matrix m at A + m*astride, its
+ * info at dinfo[m] (zeroed here): the blocked factorization of ddlak_potrf
+ * (block columns of 128, no look-ahead), one launch per kernel and block column
+ * over the whole batch.  Needs even lda and astride, a 16-byte aligned A and
+ * batch <= 65535 (cudaErrorInvalidValue otherwise). */
+int ddlak_potrf_batched_f64(int batch, int n, void* A, long long lda, long long astride, int* dinfo, void* stream);
+
+/* L L^T x = b in place for a batch of FP64 factors from ddlak_potrf_batched_f64
+ * (order <= 1024, one right-hand side at B + m*bstride); logdet[m] = 2 sum log
+ * l_ii when logdet is not null.  A matrix with dinfo[m] != 0 keeps b and gets
+ * logdet NaN. */
+int ddlak_potrs_batched_f64(int batch, int n, const void* L, long long lda, long long astride, void* B,
+                            long long bstride, const int* dinfo, double* logdet, void* stream);
+
 /* In place A <- J A J on the leading n x n (element (i, j) trades places with
  * (n-1-i, n-1-j); J the order-reversing permutation).  With it the bottom-right
  * factorization of src/Cholesky/potrf_bottom_right.cpp:208-256 (A = U U^H or
@@ -290,7 +304,9 @@ int ddlak_fill_spd_vbatched(char type, int batch, const int* d_n, void* const* d
 int ddlak_gp_build(char type, int batch, int n, int d, const void* X, long long xstride, const double* theta,
                    int tstride, void* A, long long lda, long long astride, void* stream);
 
-/* W = L^-1 (lower triangle written) for n <= 1024, one CTA per matrix. */
+/* W = L^-1 (lower triangle written) for n <= 1024.  FP64 with W apart from L and
+ * n > 64: recursive inversion on the FP64 tensor cores, which overwrites W's
+ * strictly upper triangle as scratch; otherwise one CTA per matrix (W may be L). */
 int ddlak_trtri_batched(char type, int batch, int n, const void* L, long long ldl, long long lstride, void* W,
                         long long ldw, long long wstride, void* stream);
 

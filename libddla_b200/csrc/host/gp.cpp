@@ -3,14 +3,18 @@
 // loss = 1/2 (y^T A^-1 y + log det A) and its adjoint (no reference counterpart).
 //
 // Orders up to 1024: the forward is one persistent batched factor + solve +
-// log-determinant launch (posvVbatched), the backward a batched W = L^-1 and
+// log-determinant launch (posvVbatched) or, for FP64 batches of one even order
+// from 512, the blocked factorization batched over the matrices and a batched
+// substitution; the backward a batched W = L^-1 and
 // the tiled (W^T W) contraction with the adjoint epilogue.  Larger orders
 // (batch 1): the blocked factorization (ddlak_potrf), the fused solve, and for
 // the backward W = L^-1 from the fused forward substitution on the identity.
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdint>
 #include <limits>
+#include <type_traits>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -47,6 +51,15 @@ void check_theta(const char* routine, int d, const double* theta, int tstride, c
     if (!theta || !X) throw std::invalid_argument(std::string(routine) + ": null points or theta");
 }
 
+// FP64 batches of one even order in [512, 1024] with a 16-byte aligned base take
+// the batched blocked factorization; the rest the persistent posvVbatched launch.
+template <class T>
+bool uniform_blocked(int batch, int n, const T* A)
+{
+    return std::is_same<T, double>::value && n >= 512 && n <= kBatchedMaxOrder && n % 2 == 0 && batch <= 65535 &&
+           (reinterpret_cast<uintptr_t>(A) & 15) == 0;
+}
+
 template <class T>
 void factor_solve(const DdlaHandle_t& h, int batch, int n, T* A, const T* y, T* alpha, double* logdet, double* quad,
                   int* info)
@@ -55,7 +68,13 @@ void factor_solve(const DdlaHandle_t& h, int batch, int n, T* A, const T* y, T* 
     const long long nn = (long long)n * n;
     detail::cuda_check(cudaMemcpyAsync(alpha, y, sizeof(T) * (size_t)batch * n, cudaMemcpyDeviceToDevice, st),
                        "copy y");
-    if (n <= kBatchedMaxOrder) {
+    if (uniform_blocked<T>(batch, n, A)) {
+        // equal orders from 512: the blocked factorization batched over the matrices (diagonal
+        // blocks, panels and DMMA trailing updates, one launch each per block column), then one
+        // substitution launch that also forms log det
+        ck(ddlak_potrf_batched_f64(batch, n, A, n, nn, info, st), "factorization");
+        ck(ddlak_potrs_batched_f64(batch, n, A, n, nn, alpha, n, info, logdet, st), "solve");
+    } else if (n <= kBatchedMaxOrder) {
         // device arrays for the batched launch: orders, leading dimensions, pointers
         const size_t bytes = detail::padded_bytes<int>(batch) * 2 + detail::padded_bytes<T*>(batch) * 2;
         detail::DeviceScratch ws(h, bytes);

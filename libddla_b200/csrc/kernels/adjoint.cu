@@ -10,7 +10,9 @@
 //                     partial results are staged in shared memory, all warps solve
 //                     them against the 32 x 32 diagonal block of L (a few columns
 //                     each, shuffles), and every thread updates the rows it owns
-//                     below from registers;
+//                     below from registers.  For FP64 it inverts only the 64 x 64
+//                     diagonal blocks, which k_trtri_level joins pairwise on the
+//                     FP64 tensor cores (recursive inversion, bottom-up);
 //   k_adjoint_contract  (W^T W) tile by tile (128 x 128 lower tiles, k from the tile's
 //                     first row: W is lower triangular) with a fused epilogue that
 //                     either contracts Abar with dA/dtheta (recomputed from the
@@ -75,7 +77,7 @@ template <> struct TrWidth<float> { static constexpr int B = 32; };
 template <class T>
 __global__ void __launch_bounds__(TR_NT, 1)
     k_trtri_batched(int n, const T* __restrict__ Lg, long long ldl, long long lstride, T* __restrict__ Wg,
-                    long long ldw, long long wstride)
+                    long long ldw, long long wstride, int nsub, long long lsub, long long wsub)
 {
     constexpr int B = TrWidth<T>::B;
     constexpr int RPT = TR_NMAX / TR_NT;
@@ -84,8 +86,10 @@ __global__ void __launch_bounds__(TR_NT, 1)
     __shared__ __align__(16) T Xr[2][32][B];        // the solved block, row-major for 128-bit broadcast reads
     __shared__ T Ls[2][32][33];
     __shared__ T Ri[2][32];  // reciprocal pivots of the staged diagonal block
-    const T* L = Lg + blockIdx.x * lstride;
-    T* W = Wg + blockIdx.x * wstride;
+    // blockIdx.x = matrix * nsub + sub-block (the diagonal blocks of a recursive inversion)
+    const long long mm = blockIdx.x / nsub, sub = blockIdx.x % nsub;
+    const T* L = Lg + mm * lstride + sub * lsub;
+    T* W = Wg + mm * wstride + sub * wsub;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     // block columns of W are independent: part p of gridDim.y takes the range
     // [jb, je) holding about 1/P of the work ((n - J)^3 / 3 beyond column J)
@@ -431,17 +435,182 @@ int gp_build_t(int batch, int n, int d, const void* X, long long xstride, const 
     return (int)cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Recursive FP64 inversion, bottom-up: the 64 x 64 diagonal blocks by
+// k_trtri_batched, then for h = 64, 128, ... each pair of inverted h-blocks
+// (o = 2 p h) is joined by
+//   W21 = -W22 (L21 W11),  L21 = L(o+h.., o..), W11 = W(o.., o..), W22 = W(o+h.., o+h..),
+// two batched products on the FP64 tensor cores (mma.sync m16n8k4):
+//   step 1: T = L21 W11 (W11 lower: k >= j), kept transposed in W's strictly
+//           upper block W(o.., o+h..), which the result does not use;
+//   step 2: W21 = -W22 T (W22 lower: k <= i), written to W(o+h.., o..).
+// 64 x 64 tiles, 4 warps of 32 x 32, k in chunks of 32 staged by cp.async
+// (3 stages); shared rows padded to 68 / 36 doubles so that the fragment reads
+// are conflict free.  The strictly upper triangles of W are read nowhere
+// (masked) and are overwritten as scratch.
+// ---------------------------------------------------------------------------
+constexpr int TL_BK = 32, TL_NS = 3, TL_LDK = 68, TL_LDJ = 36;
+constexpr int TL_ASZ = TL_BK * TL_LDK;  // A slice [k][i]
+constexpr int TL_BSZ = 64 * TL_LDJ;     // B slice [j][k] (step 1) or [k][j] (step 2, 32 x 68 fits)
+constexpr size_t TL_SMEM = (size_t)TL_NS * (TL_ASZ + TL_BSZ) * sizeof(double);
+
+__device__ __forceinline__ void tl_mma(double (&u)[2], double (&v)[2], double a_up, double a_lo, double b)
+{
+    asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+                 : "+d"(u[0]), "+d"(u[1]), "+d"(v[0]), "+d"(v[1])
+                 : "d"(a_up), "d"(a_lo), "d"(b));
+}
+
+template <int STEP>
+__global__ void __launch_bounds__(128) k_trtri_level(int n, int h, const double* __restrict__ Lg, long long ldl,
+                                                     long long lstride, double* __restrict__ Wg, long long ldw,
+                                                     long long wstride)
+{
+    extern __shared__ __align__(16) double tl_smem[];
+    const int p = blockIdx.y;
+    const long long m = blockIdx.z;
+    const int o = 2 * p * h, r2 = min(h, n - o - h);  // rows of the lower block (> 0 by the grid)
+    const int ntn = h / 64;
+    const int i0 = (blockIdx.x / ntn) * 64, j0 = (blockIdx.x % ntn) * 64;
+    if (i0 >= r2) return;
+    const double* L = Lg + m * lstride;
+    double* W = Wg + m * wstride;
+    const int kbeg = STEP == 1 ? j0 : 0;
+    const int kend = STEP == 1 ? h : min(i0 + 64, r2);
+    const int nch = (kend - kbeg + TL_BK - 1) / TL_BK;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, q = lane & 3;
+
+    auto stage = [&](int c, int sidx) {
+        double* As = tl_smem + (size_t)sidx * (TL_ASZ + TL_BSZ);
+        double* Bs = As + TL_ASZ;
+        const int k0 = kbeg + c * TL_BK;
+        for (int e = t; e < TL_BK * 64; e += 128) {
+            const int i = e & 63, kk = e >> 6, k = k0 + kk, gi = i0 + i;
+            bool v;
+            const double* src;
+            if (STEP == 1) {
+                v = gi < r2 && k < kend;
+                src = L + (o + h + gi) + (long long)(o + k) * ldl;
+            } else {
+                v = gi < r2 && k < kend && k <= gi;
+                src = W + (o + h + gi) + (long long)(o + h + k) * ldw;
+            }
+            cp_async_elem<8>(&As[kk * TL_LDK + i], v ? src : W, v);
+        }
+        for (int e = t; e < TL_BK * 64; e += 128) {
+            if (STEP == 1) {
+                const int kk = e & 31, j = e >> 5, k = k0 + kk, gj = j0 + j;
+                const bool v = k < kend && k >= gj;
+                cp_async_elem<8>(&Bs[j * TL_LDJ + kk], v ? W + (o + k) + (long long)(o + gj) * ldw : W, v);
+            } else {
+                const int j = e & 63, kk = e >> 6, k = k0 + kk, gj = j0 + j;
+                const bool v = k < kend;
+                cp_async_elem<8>(&Bs[kk * TL_LDK + j], v ? W + (o + gj) + (long long)(o + h + k) * ldw : W, v);
+            }
+        }
+    };
+
+    double u[2][4][2], v[2][4][2];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) u[a][b][0] = u[a][b][1] = v[a][b][0] = v[a][b][1] = 0.0;
+#pragma unroll
+    for (int c = 0; c < TL_NS - 1; ++c) {
+        if (c < nch) stage(c, c);
+        cp_group_commit();
+    }
+    for (int c = 0; c < nch; ++c) {
+        cp_group_wait<TL_NS - 2>();
+        __syncthreads();
+        if (c + TL_NS - 1 < nch) stage(c + TL_NS - 1, (c + TL_NS - 1) % TL_NS);
+        cp_group_commit();
+        const double* As = tl_smem + (size_t)(c % TL_NS) * (TL_ASZ + TL_BSZ);
+        const double* Bs = As + TL_ASZ;
+#pragma unroll
+        for (int kk = 0; kk < TL_BK; kk += 4) {
+            double a[2][2], b[4];
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+                a[mt][0] = As[(kk + q) * TL_LDK + wm * 32 + mt * 16 + g];
+                a[mt][1] = As[(kk + q) * TL_LDK + wm * 32 + mt * 16 + 8 + g];
+            }
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                const int jb = wn * 32 + nt * 8 + g;
+                b[nt] = STEP == 1 ? Bs[jb * TL_LDJ + kk + q] : Bs[(kk + q) * TL_LDK + jb];
+            }
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+                for (int nt = 0; nt < 4; ++nt) tl_mma(u[mt][nt], v[mt][nt], a[mt][0], a[mt][1], b[nt]);
+        }
+    }
+    cp_group_wait<0>();
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int j = j0 + wn * 32 + nt * 8 + 2 * q + e;
+#pragma unroll
+                for (int hh = 0; hh < 2; ++hh) {
+                    const int i = i0 + wm * 32 + mt * 16 + g + 8 * hh;
+                    if (i >= r2) continue;
+                    const double val = hh ? v[mt][nt][e] : u[mt][nt][e];
+                    if (STEP == 1) W[(o + j) + (long long)(o + h + i) * ldw] = val;
+                    else W[(o + h + i) + (long long)(o + j) * ldw] = -val;
+                }
+            }
+}
+
+int trtri_recursive_f64(int batch, int n, const double* L, long long ldl, long long lstride, double* W, long long ldw,
+                        long long wstride, cudaStream_t st)
+{
+    constexpr int LEAF = 64;
+    const int full = n / LEAF, last = n - full * LEAF;
+    if (full > 0) {
+        k_trtri_batched<double><<<dim3((unsigned)((long long)batch * full), 1), TR_NT, 0, st>>>(
+            LEAF, L, ldl, lstride, W, ldw, wstride, full, LEAF * (ldl + 1), LEAF * (ldw + 1));
+        note_launches(1);
+    }
+    if (last > 0) {
+        const long long off_l = (long long)full * LEAF * (ldl + 1), off_w = (long long)full * LEAF * (ldw + 1);
+        k_trtri_batched<double><<<dim3((unsigned)batch, 1), TR_NT, 0, st>>>(last, L + off_l, ldl, lstride, W + off_w,
+                                                                            ldw, wstride, 1, 0, 0);
+        note_launches(1);
+    }
+    if (cudaError_t e = cudaGetLastError(); e != cudaSuccess) return (int)e;
+    if (cudaError_t e = smem_optin(k_trtri_level<1>, TL_SMEM); e != cudaSuccess) return (int)e;
+    if (cudaError_t e = smem_optin(k_trtri_level<2>, TL_SMEM); e != cudaSuccess) return (int)e;
+    for (int h = LEAF; h < n; h *= 2) {
+        const int npairs = (n - h + 2 * h - 1) / (2 * h);  // pairs whose lower block exists
+        const dim3 grid((unsigned)((h / 64) * (h / 64)), (unsigned)npairs, (unsigned)batch);
+        k_trtri_level<1><<<grid, 128, TL_SMEM, st>>>(n, h, L, ldl, lstride, W, ldw, wstride);
+        k_trtri_level<2><<<grid, 128, TL_SMEM, st>>>(n, h, L, ldl, lstride, W, ldw, wstride);
+        note_launches(2);
+    }
+    return (int)cudaGetLastError();
+}
+
 template <class T>
 int trtri_t(int batch, int n, const void* L, long long ldl, long long lstride, void* W, long long ldw,
             long long wstride, cudaStream_t st)
 {
+    // FP64 above one leaf, W apart from L: the recursive inversion on the tensor cores
+    if constexpr (std::is_same<T, double>::value)
+        if (n > 64 && L != W && batch <= 65535)
+            return trtri_recursive_f64(batch, n, static_cast<const double*>(L), ldl, lstride, static_cast<double*>(W),
+                                       ldw, wstride, st);
     // split each matrix over block-column ranges until the launch covers the SMs twice
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     int parts = 1;
     while (parts < 8 && (long long)batch * parts < 2LL * sms && n / TrWidth<T>::B >= 4 * parts) parts *= 2;
     k_trtri_batched<T><<<dim3(batch, parts), TR_NT, 0, st>>>(n, static_cast<const T*>(L), ldl, lstride,
-                                                             static_cast<T*>(W), ldw, wstride);
+                                                             static_cast<T*>(W), ldw, wstride, 1, 0, 0);
     note_launches(1);
     return (int)cudaGetLastError();
 }

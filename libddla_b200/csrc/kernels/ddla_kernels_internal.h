@@ -16,6 +16,13 @@ cudaError_t trailing_update(T* A, long long lda, int k0, int nbk, int n, long lo
 template <class T, bool UP>
 cudaError_t launch_trsm_panel(T* A, long long lda, int k0, int nbk, int n, const int* dinfo, cudaStream_t s);
 
+// The FP64 lower update of the region from row / column t0 over a batch of
+// equal-order matrices (astride elements apart, info per matrix) by the TMA
+// DMMA tile kernel (syrk.cu); false (nothing launched) when its conditions
+// (even lda and astride, 16-byte aligned A, nbk a multiple of 32) do not hold.
+bool launch_dmma_tma_batched(double* A, long long lda, long long astride, int batch, int k0, int nbk, int n,
+                             long long t0, const int* dinfo, cudaStream_t st, cudaError_t* err);
+
 template <class T, bool UP>
 cudaError_t trailing_update_simt(T* A, long long lda, int k0, int nbk, int n, long long t0, int cols,
                                  const int* dinfo, cudaStream_t st);

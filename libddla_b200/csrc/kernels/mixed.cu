@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(256) k_potrf_diag_mixed(float* __restrict__ W,
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* s = reinterpret_cast<double*>(smem_raw);
-    const int ld = nbk + 1;
+    const int ld = diag_block_ld<double>(nbk);
     if (*(volatile int*)info != 0) return;
     const int total = nbk * nbk;
     const float* Wb = W + k0 + (long long)k0 * ldw;
@@ -903,7 +903,7 @@ cudaError_t potrf_mixed_enqueue(float* W, long long ldw, int n, int G, void* P0,
                                 cudaStream_t st)
 {
     constexpr int NB = MX_NB;
-    const size_t diag_smem = (size_t)NB * (NB + 1) * sizeof(double);
+    const size_t diag_smem = (size_t)NB * diag_block_ld<double>(NB) * sizeof(double);
     if (cudaError_t e = smem_optin(k_potrf_diag_mixed, diag_smem); e != cudaSuccess) return e;
     MixedStreams& L = mixed_streams();
     cudaStream_t hi = L.hi;
@@ -914,7 +914,7 @@ cudaError_t potrf_mixed_enqueue(float* W, long long ldw, int n, int G, void* P0,
         const int nbk = n - k0 < NB ? n - k0 : NB;
         {
             ProfScope ps(PK_MIXED_OTHER, s, (double)nbk * nbk * nbk / 3.0, 4.0 * nbk * (nbk + 1));
-            k_potrf_diag_mixed<<<1, 256, (size_t)nbk * (nbk + 1) * sizeof(double), s>>>(W, ldw, k0, nbk, dinfo);
+            k_potrf_diag_mixed<<<1, 256, (size_t)nbk * diag_block_ld<double>(nbk) * sizeof(double), s>>>(W, ldw, k0, nbk, dinfo);
         }
         note_launches(1);
         if ((long long)n - k0 - nbk <= 0) return cudaGetLastError();
@@ -1012,7 +1012,7 @@ cudaError_t potrf_mixed_stream_enqueue(int n, int G, const double* Ah, long long
                                        double* anrm, int* dinfo, int* status, cudaStream_t cs, cudaStream_t st)
 {
     constexpr int NB = MX_NB;
-    const size_t diag_smem = (size_t)NB * (NB + 1) * sizeof(double);
+    const size_t diag_smem = (size_t)NB * diag_block_ld<double>(NB) * sizeof(double);
     if (cudaError_t e = smem_optin(k_potrf_diag_mixed, diag_smem); e != cudaSuccess) return e;
     const long long SW = (long long)G * NB;
     const size_t esz = TF32 ? 4 : 2;
@@ -1090,7 +1090,7 @@ cudaError_t potrf_mixed_stream_enqueue(int n, int G, const double* Ah, long long
                 break;
             {
                 ProfScope ps(PK_MIXED_OTHER, hs, (double)nbk * nbk * nbk / 3.0, 4.0 * nbk * (nbk + 1));
-                k_potrf_diag_mixed<<<1, 256, (size_t)nbk * (nbk + 1) * sizeof(double), hs>>>(W, ldw, (int)kg, nbk,
+                k_potrf_diag_mixed<<<1, 256, (size_t)nbk * diag_block_ld<double>(nbk) * sizeof(double), hs>>>(W, ldw, (int)kg, nbk,
                                                                                              dinfo);
             }
             note_launches(1);

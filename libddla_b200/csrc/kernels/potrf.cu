@@ -32,12 +32,14 @@ namespace ddlak {
 // 1. diagonal block
 // ---------------------------------------------------------------------------
 template <class T, bool UP>
-__global__ void __launch_bounds__(256) k_potrf_diag(T* __restrict__ A, long long lda, int k0, int nbk,
-                                                    int* __restrict__ info)
+__global__ void __launch_bounds__(256) k_potrf_diag(T* __restrict__ A, long long lda, long long astride, int k0,
+                                                    int nbk, int* __restrict__ info)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* s = reinterpret_cast<T*>(smem_raw);
-    const int ld = nbk + 1;
+    const int ld = diag_block_ld<T>(nbk);
+    A += (long long)blockIdx.x * astride;  // blockIdx.x: the matrix of a batch (grid 1 for one matrix)
+    info += blockIdx.x;
     if (*(volatile int*)info != 0) return;
     load_lview_block<T, UP>(s, ld, A, lda, k0, k0, nbk, nbk, nbk, nbk, true);
     const int fail = factor_block_smem<T>(s, ld, nbk);
@@ -355,6 +357,97 @@ __global__ void __launch_bounds__(TRR_NT) k_trsm_panel_rows(float* __restrict__ 
     }
 }
 
+// ---------------------------------------------------------------------------
+// The FP64 panel (lower storage, nbk <= 128): one thread per row, in four
+// chunks of 32 columns so that 32 of the row's values are live in registers.
+// Chunk C: x = row[32C : 32C + 32]; x -= x_J L11[32C.., 32J..]^T for the
+// chunks J < C (their solved values re-read from the row this thread already
+// wrote); then x is solved against the diagonal block (x_j *= 1 / l_jj,
+// x_k -= x_j l_kj for k > j) and written back.  Every entry receives the
+// updates of its columns in increasing order, as in the column-by-column
+// substitution.  L11's lower part is held as ten 32 x 32 blocks (80 KB, two
+// CTAs per SM) read as 16-byte broadcasts; the row loads and stores are
+// coalesced (consecutive threads, consecutive rows).
+// ---------------------------------------------------------------------------
+constexpr int TRD_NT = 128;
+constexpr size_t TRD_SMEM = 10 * 32 * 32 * sizeof(double);
+
+__device__ __forceinline__ double2 ld_shared_d2(const double2* p)
+{
+    double2 v;
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(a));
+    return v;
+}
+
+__global__ void __launch_bounds__(TRD_NT) k_trsm_panel_rows_f64(double* __restrict__ A, long long lda,
+                                                                long long astride, int k0, int nbk, int n,
+                                                                const int* __restrict__ info)
+{
+    // block (C, J), J <= C, at trd_smem + (C (C + 1) / 2 + J) * 1024, element [j * 32 + i]
+    // = L(k0 + 32 C + i, k0 + 32 J + j), zero above the diagonal and past nbk
+    extern __shared__ __align__(16) double trd_smem[];
+    __shared__ double rinv[128];
+    A += (long long)blockIdx.y * astride;  // blockIdx.y: the matrix of a batch
+    info += blockIdx.y;
+    if (*(volatile const int*)info != 0) return;
+    const double* Ad = A + k0 + (long long)k0 * lda;
+    for (int idx = threadIdx.x; idx < 10 * 1024; idx += TRD_NT) {
+        const int b = idx >> 10, e = idx & 1023, j = e >> 5, i = e & 31;
+        const int C = b >= 6 ? 3 : b >= 3 ? 2 : b >= 1 ? 1 : 0;
+        const int J = b - C * (C + 1) / 2;
+        const int r = 32 * C + i, c = 32 * J + j;
+        trd_smem[idx] = (r < nbk && c < nbk && r >= c) ? Ad[r + (long long)c * lda] : 0.0;
+    }
+    __syncthreads();
+    {
+        const int t = threadIdx.x, C = t >> 5, i = t & 31;
+        rinv[t] = t < nbk ? 1.0 / trd_smem[(C * (C + 1) / 2 + C) * 1024 + i * 32 + i] : 0.0;
+    }
+    __syncthreads();
+    const long long row = (long long)k0 + nbk + (long long)blockIdx.x * TRD_NT + threadIdx.x;
+    const bool live = row < n;
+    double* Ar = A + (live ? row : (long long)k0) + (long long)k0 * lda;
+    const int nch = (nbk + 31) >> 5;
+    for (int C = 0; C < nch; ++C) {
+        double x[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) x[i] = (live && 32 * C + i < nbk) ? Ar[(long long)(32 * C + i) * lda] : 0.0;
+        for (int J = 0; J < C; ++J) {
+            const double* blk = trd_smem + (C * (C + 1) / 2 + J) * 1024;
+            const double* xs = Ar + (long long)(32 * J) * lda;
+#pragma unroll 4
+            for (int j = 0; j < 32; ++j) {
+                const double xj = live ? xs[(long long)j * lda] : 0.0;
+                const double2* col = reinterpret_cast<const double2*>(blk + j * 32);
+#pragma unroll
+                for (int h = 0; h < 16; ++h) {
+                    const double2 l = ld_shared_d2(col + h);
+                    x[2 * h] = fma(-xj, l.x, x[2 * h]);
+                    x[2 * h + 1] = fma(-xj, l.y, x[2 * h + 1]);
+                }
+            }
+        }
+        const double* dblk = trd_smem + (C * (C + 1) / 2 + C) * 1024;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            x[j] *= rinv[32 * C + j];
+            const double2* col = reinterpret_cast<const double2*>(dblk + j * 32);
+#pragma unroll
+            for (int h = 0; h < 16; ++h) {
+                if (2 * h + 1 > j) {
+                    const double2 l = ld_shared_d2(col + h);
+                    if (2 * h > j) x[2 * h] = fma(-x[j], l.x, x[2 * h]);
+                    x[2 * h + 1] = fma(-x[j], l.y, x[2 * h + 1]);
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+            if (live && 32 * C + i < nbk) Ar[(long long)(32 * C + i) * lda] = x[i];
+    }
+}
+
 template <class T, bool UP>
 cudaError_t launch_trsm_panel(T* A, long long lda, int k0, int nbk, int n, const int* dinfo, cudaStream_t s)
 {
@@ -365,6 +458,16 @@ cudaError_t launch_trsm_panel(T* A, long long lda, int k0, int nbk, int n, const
         const double md = (double)m, b = nbk;
         ProfScope ps(PK_TRSM_PANEL, s, md * b * b, sizeof(T) * (2.0 * md * b + b * (b + 1) / 2));
         k_trsm_panel_rows<<<(unsigned)ceil_div(m, TRR_NT), TRR_NT, TRR_SMEM, s>>>(A, lda, k0, nbk, n, dinfo);
+        note_launches(1);
+        return cudaGetLastError();
+    }
+    if constexpr (std::is_same<T, double>::value && !UP) {
+        const long long m = (long long)n - k0 - nbk;
+        if (m <= 0) return cudaSuccess;
+        if (cudaError_t e = smem_optin(k_trsm_panel_rows_f64, TRD_SMEM); e != cudaSuccess) return e;
+        const double md = (double)m, b = nbk;
+        ProfScope ps(PK_TRSM_PANEL, s, md * b * b, sizeof(T) * (2.0 * md * b + b * (b + 1) / 2));
+        k_trsm_panel_rows_f64<<<(unsigned)ceil_div(m, TRD_NT), TRD_NT, TRD_SMEM, s>>>(A, lda, 0, k0, nbk, n, dinfo);
         note_launches(1);
         return cudaGetLastError();
     }
@@ -412,7 +515,7 @@ static cudaError_t potrf_enqueue(T* A, long long lda, int n, int G, int* dinfo, 
     constexpr int NB = potrf_nb<T>();
     constexpr int NQ = NB / 32;
     constexpr int PR = sizeof(T) >= 16 ? 4 : 8;
-    const size_t diag_smem = (size_t)NB * (NB + 1) * sizeof(T);
+    const size_t diag_smem = (size_t)NB * diag_block_ld<T>(NB) * sizeof(T);
     const size_t panel_smem = (size_t)(NQ * 32) * (NQ * 32 + 1) * sizeof(T);
     if (cudaError_t e = smem_optin(k_potrf_diag<T, UP>, diag_smem); e != cudaSuccess) return e;
     if (cudaError_t e = smem_optin(k_trsm_panel<T, UP, NQ, PR>, panel_smem); e != cudaSuccess) return e;
@@ -420,16 +523,23 @@ static cudaError_t potrf_enqueue(T* A, long long lda, int n, int G, int* dinfo, 
     LookaheadRes& L = lookahead_res();
     cudaStream_t hi = L.hi;
 
+    cudaError_t panel_err = cudaSuccess;
     auto diag_and_panel = [&](int k0, cudaStream_t s) {
         const int nbk = n - k0 < NB ? n - k0 : NB;
         const double b = nbk;
         {
             ProfScope ps(PK_POTRF_DIAG, s, cf * b * b * b / 3.0, sizeof(T) * b * (b + 1));
-            k_potrf_diag<T, UP><<<1, 256, (size_t)nbk * (nbk + 1) * sizeof(T), s>>>(A, lda, k0, nbk, dinfo);
+            k_potrf_diag<T, UP><<<1, 256, (size_t)nbk * diag_block_ld<T>(nbk) * sizeof(T), s>>>(A, lda, 0, k0, nbk,
+                                                                                              dinfo);
         }
         note_launches(1);
         const long long m = (long long)n - k0 - nbk;
         if (m <= 0) return;
+        if constexpr ((std::is_same<T, double>::value || std::is_same<T, float>::value) && !UP) {
+            const cudaError_t pe = launch_trsm_panel<T, UP>(A, lda, k0, nbk, n, dinfo, s);  // one thread per row
+            if (pe != cudaSuccess && panel_err == cudaSuccess) panel_err = pe;
+            return;
+        }
         const double md = (double)m;
         {
             ProfScope ps(PK_TRSM_PANEL, s, cf * md * b * b, sizeof(T) * (2.0 * md * b + b * (b + 1) / 2));
@@ -489,6 +599,7 @@ static cudaError_t potrf_enqueue(T* A, long long lda, int n, int G, int* dinfo, 
     // join
     cudaEventRecord(L.panel, hi);
     cudaStreamWaitEvent(st, L.panel, 0);
+    if (panel_err != cudaSuccess) return panel_err;
     return cudaGetLastError();
 }
 
@@ -500,6 +611,165 @@ static cudaError_t potrf_typed(char uplo, int n, int G, void* A, long long lda, 
 }
 
 }  // namespace ddlak
+
+// ---------------------------------------------------------------------------
+// L L^T x = b for a batch of factored equal-order FP64 matrices (lower, order
+// <= 1024, one right-hand side each), one CTA per matrix with x in shared
+// memory; log det = 2 sum log l_ii on the way.  Forward, by 32-row blocks: warp
+// 0 solves the block (lane i owns row i; x_j = x_j / l_jj, then broadcast),
+// every thread updates its rows below with the block's 32 columns (coalesced
+// column reads).  Backward, by 32-row blocks from the end: each warp forms the
+// dot products of some of the block's columns with the solved x below
+// (coalesced, warp sums), then warp 0 solves the transposed block from a
+// shared copy.  A matrix with info != 0 keeps b and gets log det = NaN.
+// ---------------------------------------------------------------------------
+constexpr int PB_NT = 256, PB_NMAX = 1024;
+
+__global__ void __launch_bounds__(PB_NT) k_potrs_batched_f64(int n, const double* __restrict__ Lg, long long lda,
+                                                             long long astride, double* __restrict__ Bg,
+                                                             long long bstride, const int* __restrict__ info,
+                                                             double* __restrict__ logdet)
+{
+    __shared__ double x[PB_NMAX];
+    __shared__ double blk[32][33];
+    __shared__ double s_ld;
+    const int m = blockIdx.x, t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    if (info[m] != 0) {
+        if (t == 0 && logdet) logdet[m] = __longlong_as_double(0x7ff8000000000000LL);
+        return;
+    }
+    const double* L = Lg + (long long)m * astride;
+    double* B = Bg + (long long)m * bstride;
+    for (int i = t; i < n; i += PB_NT) x[i] = B[i];
+    double ld = 0.0;  // warp 0: sum of log l_ii over the rows its lanes own
+    __syncthreads();
+    for (int b0 = 0; b0 < n; b0 += 32) {
+        const int w = n - b0 < 32 ? n - b0 : 32;
+        if (warp == 0) {
+            double xi = lane < w ? x[b0 + lane] : 0.0;
+            for (int j = 0; j < w; ++j) {
+                if (lane == j) {
+                    const double d = L[(b0 + j) + (long long)(b0 + j) * lda];
+                    xi = xi / d;
+                    ld += log(d);
+                }
+                const double xj = __shfl_sync(0xffffffffu, xi, j);
+                if (lane > j && lane < w) xi = fma(-L[(b0 + lane) + (long long)(b0 + j) * lda], xj, xi);
+            }
+            if (lane < w) x[b0 + lane] = xi;
+        }
+        __syncthreads();
+        for (int r = b0 + 32 + t; r < n; r += PB_NT) {
+            double acc = x[r];
+            const double* lr = L + r + (long long)b0 * lda;
+            for (int j = 0; j < w; ++j) acc = fma(-lr[(long long)j * lda], x[b0 + j], acc);
+            x[r] = acc;
+        }
+        __syncthreads();
+    }
+    if (warp == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ld += __shfl_xor_sync(0xffffffffu, ld, o);
+        if (lane == 0) s_ld = 2.0 * ld;
+    }
+    for (int b0 = ((n - 1) / 32) * 32; b0 >= 0; b0 -= 32) {
+        const int w = n - b0 < 32 ? n - b0 : 32;
+        // x_i -= sum_{r >= b0 + 32} l(r, b0 + i) x_r for the block's columns i
+        for (int i = warp; i < w; i += PB_NT / 32) {
+            const double* lc = L + (long long)(b0 + i) * lda;
+            double acc = 0.0;
+            for (int r = b0 + 32 + lane; r < n; r += 32) acc = fma(lc[r], x[r], acc);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) x[b0 + i] -= acc;
+        }
+        if (warp == 1)  // the block itself, for the transposed solve
+            for (int c = 0; c < w; ++c) blk[lane][c] = lane < w ? L[(b0 + lane) + (long long)(b0 + c) * lda] : 0.0;
+        __syncthreads();
+        if (warp == 0) {
+            double xi = lane < w ? x[b0 + lane] : 0.0;
+            for (int j = w - 1; j >= 0; --j) {
+                if (lane == j) xi = xi / blk[j][j];
+                const double xj = __shfl_sync(0xffffffffu, xi, j);
+                if (lane < j) xi = fma(-blk[j][lane], xj, xi);
+            }
+            if (lane < w) x[b0 + lane] = xi;
+        }
+        __syncthreads();
+    }
+    for (int i = t; i < n; i += PB_NT) B[i] = x[i];
+    if (t == 0 && logdet) logdet[m] = s_ld;
+}
+
+// A batch of equal-order FP64 matrices (lower), right-looking by block columns
+// of 128, each step one launch per kernel over the whole batch: the diagonal
+// blocks (one CTA per matrix), the panels (row-per-thread solve, grid.y =
+// matrix) and the trailing updates (TMA DMMA tiles, grid.y = matrix).  The
+// same operations as the single-matrix factorization without look-ahead.
+extern "C" int ddlak_potrf_batched_f64(int batch, int n, void* A_, long long lda, long long astride, int* dinfo,
+                                       void* stream)
+{
+    using namespace ddlak;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    double* A = static_cast<double*>(A_);
+    if (batch < 0 || n < 0 || (batch > 0 && (!A || !dinfo || lda < n || astride < lda * (long long)n)))
+        return (int)cudaErrorInvalidValue;
+    if (batch == 0) return 0;
+    if (batch > 65535 || (lda & 1) || (astride & 1) || (reinterpret_cast<uintptr_t>(A) & 15))
+        return (int)cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(dinfo, 0, sizeof(int) * (size_t)batch, st);
+    if (e != cudaSuccess || n == 0) return (int)e;
+    constexpr int NB = 128;
+    const size_t diag_smem = (size_t)NB * diag_block_ld<double>(NB) * sizeof(double);
+    if ((e = smem_optin(k_potrf_diag<double, false>, diag_smem)) != cudaSuccess) return (int)e;
+    if ((e = smem_optin(k_trsm_panel_rows_f64, TRD_SMEM)) != cudaSuccess) return (int)e;
+    const double nb3 = (double)batch;
+    for (int k0 = 0; k0 < n; k0 += NB) {
+        const int nbk = n - k0 < NB ? n - k0 : NB;
+        const double b = nbk;
+        {
+            ProfScope ps(PK_POTRF_DIAG, st, nb3 * b * b * b / 3.0, nb3 * 8.0 * b * (b + 1));
+            k_potrf_diag<double, false><<<(unsigned)batch, 256, (size_t)nbk * diag_block_ld<double>(nbk) * 8, st>>>(
+                A, lda, astride, k0, nbk, dinfo);
+        }
+        note_launches(1);
+        const long long m = (long long)n - k0 - nbk;
+        if (m <= 0) break;
+        {
+            const double md = (double)m;
+            ProfScope ps(PK_TRSM_PANEL, st, nb3 * md * b * b, nb3 * 8.0 * (2.0 * md * b + b * (b + 1) / 2));
+            k_trsm_panel_rows_f64<<<dim3((unsigned)ceil_div(m, TRD_NT), (unsigned)batch), TRD_NT, TRD_SMEM, st>>>(
+                A, lda, astride, k0, nbk, n, dinfo);
+        }
+        note_launches(1);
+        {
+            const double md = (double)m;
+            ProfScope ps(PK_SYRK_UPDATE, st, nb3 * md * (md + 1) * b, nb3 * 8.0 * (md * (md + 1) + md * b));
+            if (!launch_dmma_tma_batched(A, lda, astride, batch, k0, nbk, n, (long long)k0 + nbk, dinfo, st, &e))
+                return (int)cudaErrorInvalidValue;
+            if (e != cudaSuccess) return (int)e;
+        }
+        note_launches(1);
+    }
+    return (int)cudaGetLastError();
+}
+
+extern "C" int ddlak_potrs_batched_f64(int batch, int n, const void* L, long long lda, long long astride, void* B,
+                                       long long bstride, const int* dinfo, double* logdet, void* stream)
+{
+    using namespace ddlak;
+    if (batch < 0 || n < 0 || n > PB_NMAX) return (int)cudaErrorInvalidValue;
+    if (batch == 0 || n == 0) return 0;
+    if (!L || !B || !dinfo || lda < n || astride < lda * (long long)n || bstride < n)
+        return (int)cudaErrorInvalidValue;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const double nn = n;
+    ProfScope ps(PK_POTRS_FUSED, st, 2.0 * batch * nn * nn, 8.0 * batch * nn * (nn + 1));
+    k_potrs_batched_f64<<<(unsigned)batch, PB_NT, 0, st>>>(n, static_cast<const double*>(L), lda, astride,
+                                                         static_cast<double*>(B), bstride, dinfo, logdet);
+    note_launches(1);
+    return (int)cudaGetLastError();
+}
 
 extern "C" int ddlak_potrf_grouped(char type, char uplo, int group, int n, void* A, long long lda, int* dinfo,
                                    void* stream)

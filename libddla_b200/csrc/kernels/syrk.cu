@@ -193,10 +193,14 @@ __global__ void __launch_bounds__(256, 1) k_syrk_dmma(double* __restrict__ A, lo
 // columns as two 132 x 32 FP64 boxes (the 4 extra rows pad the leading dimension
 // of the shared tile to 132, which keeps the fragment reads conflict free; rows
 // past n arrive as zeros), so no thread spends issue slots on per-element copies.
-// 3 stages of 66 KB.  A stage's arrival wait is bounded: if it gives up, the CTA
-// records it in g_dmma_status, writes NaN into its tile (the factorization then
-// stops at that column block with a failed pivot) and waits, bounded, for its
-// copies still in flight before it exits.
+// 3 stages of 66 KB.  No CTA barrier per stage: each warp releases a stage on
+// its `empty` mbarrier when done with it, and the loading thread refills the
+// stage of chunk c - 1 (long released by the other warps) after its own chunk c,
+// so the warps drift freely and the DMMA pipe is not drained once per chunk.
+// Every wait is bounded: if one gives up, the CTA records it in g_dmma_status,
+// writes NaN into its tile (the factorization then stops at that column block
+// with a failed pivot) and waits, bounded, for its copies still in flight
+// before it exits.
 // ---------------------------------------------------------------------------
 constexpr int DT_BK = 32, DT_LDS = 132, DT_NS = 3;
 constexpr int DT_BOX = DT_BK * DT_LDS;                                  // doubles per operand box
@@ -205,12 +209,17 @@ constexpr size_t DT_SMEM = (size_t)DT_NS * 2 * DT_BOX_BYTES + 128;      // + ali
 
 __device__ int g_dmma_status;
 
+template <bool BATCH>  // BATCH: blockIdx.y is the matrix of a batch (3-D map, matrices astride apart)
 __global__ void __launch_bounds__(256, 1) k_syrk_dmma_tma(const __grid_constant__ CUtensorMap amap,
-                                                          double* __restrict__ A, long long lda, int k0, int nbk,
-                                                          int n, long long t0, int cols, const int* __restrict__ info)
+                                                          double* __restrict__ A, long long lda, long long astride,
+                                                          int k0, int nbk, int n, long long t0, int cols,
+                                                          const int* __restrict__ info)
 {
     extern __shared__ __align__(128) unsigned char dt_raw[];
-    __shared__ __align__(8) uint64_t full[DT_NS];
+    __shared__ __align__(8) uint64_t full[DT_NS], empty[DT_NS];
+    const int z = BATCH ? (int)blockIdx.y : 0;
+    A += (long long)z * astride;
+    info += z;
     if (*(volatile const int*)info != 0) return;
     int I, J;
     if (cols == 0) {
@@ -233,11 +242,19 @@ __global__ void __launch_bounds__(256, 1) k_syrk_dmma_tma(const __grid_constant_
         const int s = c % DT_NS;
         double* st = sm + (size_t)s * 2 * DT_BOX;
         tc::mbar_expect_tx(&full[s], 2 * DT_BOX_BYTES);
-        tc::tma_load_2d(st, &amap, &full[s], (int)ri, k0 + c * DT_BK);
-        tc::tma_load_2d(st + DT_BOX, &amap, &full[s], (int)rj, k0 + c * DT_BK);
+        if (BATCH) {
+            tc::tma_load_3d(st, &amap, &full[s], (int)ri, k0 + c * DT_BK, z);
+            tc::tma_load_3d(st + DT_BOX, &amap, &full[s], (int)rj, k0 + c * DT_BK, z);
+        } else {
+            tc::tma_load_2d(st, &amap, &full[s], (int)ri, k0 + c * DT_BK);
+            tc::tma_load_2d(st + DT_BOX, &amap, &full[s], (int)rj, k0 + c * DT_BK);
+        }
     };
     if (threadIdx.x == 0) {
-        for (int s = 0; s < DT_NS; ++s) tc::mbar_init(&full[s], 1);
+        for (int s = 0; s < DT_NS; ++s) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 256 / 32);  // one arrival per warp
+        }
         tc::mbar_fence_init();
         tc::prefetch_tmap(&amap);
         for (int c = 0; c < DT_NS && c < nchunks; ++c) issue(c);
@@ -251,11 +268,13 @@ __global__ void __launch_bounds__(256, 1) k_syrk_dmma_tma(const __grid_constant_
         for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
 
     bool ok = true;
-    int consumed = 0;
+    int consumed = 0, issued = nchunks < DT_NS ? nchunks : DT_NS;  // issued: thread 0's count
     for (int c = 0; c < nchunks; ++c) {
         const int s = c % DT_NS;
-        ok = __syncthreads_and(tc::mbar_wait(&full[s], (uint32_t)((c / DT_NS) & 1), &g_dmma_status, 0x41));
-        if (!ok) break;
+        if (!tc::mbar_wait(&full[s], (uint32_t)((c / DT_NS) & 1), &g_dmma_status, 0x41)) {
+            ok = false;
+            break;
+        }
         consumed = c + 1;
         const double* As = sm + (size_t)s * 2 * DT_BOX;
         const double* Bs = As + DT_BOX;
@@ -271,13 +290,23 @@ __global__ void __launch_bounds__(256, 1) k_syrk_dmma_tma(const __grid_constant_
 #pragma unroll
                 for (int b = 0; b < 4; ++b) dmma2(acc[a][b], acc[a + 1][b], af[a], af[a + 1], bf[b]);
         }
-        __syncthreads();  // stage s is free again
-        if (threadIdx.x == 0 && c + DT_NS < nchunks) issue(c + DT_NS);
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&empty[s]);  // this warp is done with stage s
+        if (threadIdx.x == 0 && c >= 1 && c - 1 + DT_NS < nchunks) {
+            const int cp = c - 1;  // refill chunk cp's stage with chunk cp + NS
+            if (!tc::mbar_wait(&empty[cp % DT_NS], (uint32_t)((cp / DT_NS) & 1), &g_dmma_status, 0x44)) {
+                ok = false;
+                break;
+            }
+            issue(cp + DT_NS);
+            issued = cp + DT_NS + 1;
+        }
     }
+    ok = __syncthreads_and(ok);
     if (!ok) {
-        // copies issued for chunks consumed .. min(consumed + NS, nchunks) - 1 may still be in flight
+        // copies issued for chunks consumed .. issued - 1 may still be in flight
         if (threadIdx.x == 0) {
-            for (int c = consumed; c < nchunks && c < consumed + DT_NS; ++c)
+            for (int c = consumed; c < issued; ++c)
                 (void)tc::mbar_wait(&full[c % DT_NS], (uint32_t)((c / DT_NS) & 1), &g_dmma_status, 0x42);
         }
         __syncthreads();
@@ -332,13 +361,42 @@ bool launch_dmma_tma(double* A, long long lda, int k0, int nbk, int n, long long
     if (!tc::encode_colmajor_2d(&amap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, A, n, n, lda, DT_LDS, DT_BK,
                                 CU_TENSOR_MAP_SWIZZLE_NONE))
         return false;
-    if ((*err = smem_optin(k_syrk_dmma_tma, DT_SMEM)) != cudaSuccess) return true;
+    if ((*err = smem_optin(k_syrk_dmma_tma<false>, DT_SMEM)) != cudaSuccess) return true;
     const long long t = ceil_div(m, DM_BM);
     const long long grid = cols == 0 ? t * (t + 1) / 2 : t * ceil_div(cols, DM_BM);
-    k_syrk_dmma_tma<<<(unsigned)grid, 256, DT_SMEM, st>>>(amap, A, lda, k0, nbk, n, t0, cols, dinfo);
+    k_syrk_dmma_tma<false><<<(unsigned)grid, 256, DT_SMEM, st>>>(amap, A, lda, 0, k0, nbk, n, t0, cols, dinfo);
     *err = cudaGetLastError();
     return true;
 }
+
+}  // namespace
+
+// The same over a batch of equal-order matrices (blockIdx.y = matrix, astride
+// elements apart, info per matrix): the lower triangle from row / column t0
+// (cols == 0).  False (nothing launched) when the TMA conditions do not hold.
+bool launch_dmma_tma_batched(double* A, long long lda, long long astride, int batch, int k0, int nbk, int n,
+                             long long t0, const int* dinfo, cudaStream_t st, cudaError_t* err)
+{
+    if ((lda & 1) || (astride & 1) || (reinterpret_cast<uintptr_t>(A) & 15) || (t0 & 1) || nbk % DT_BK != 0 ||
+        nbk <= 0 || batch < 1 || batch > 65535)
+        return false;
+    const long long m = (long long)n - t0;
+    if (m <= 0) {
+        *err = cudaSuccess;
+        return true;
+    }
+    CUtensorMap amap;
+    if (!tc::encode_colmajor_3d(&amap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, A, n, n, lda, batch, astride, DT_LDS, DT_BK))
+        return false;
+    if ((*err = smem_optin(k_syrk_dmma_tma<true>, DT_SMEM)) != cudaSuccess) return true;
+    const long long t = ceil_div(m, DM_BM);
+    const dim3 grid((unsigned)(t * (t + 1) / 2), (unsigned)batch);
+    k_syrk_dmma_tma<true><<<grid, 256, DT_SMEM, st>>>(amap, A, lda, astride, k0, nbk, n, t0, 0, dinfo);
+    *err = cudaGetLastError();
+    return true;
+}
+
+namespace {
 
 // ---------------------------------------------------------------------------
 // Complex double (lower storage) on the FP64 tensor cores.  With K interleaved

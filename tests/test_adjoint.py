@@ -44,7 +44,7 @@ def se_kernel(X, theta):
 
 
 @pytest.mark.parametrize("dtype", ["float64", "float32"])
-@pytest.mark.parametrize("n", [1, 17, 64, 100, 256, 1024])
+@pytest.mark.parametrize("n", [1, 17, 64, 100, 256, 512, 1024])
 def test_chol_nll_loss_and_gradient_vs_torch(n, dtype):
     torch = _t()
     dt = getattr(torch, dtype)
@@ -160,16 +160,17 @@ def test_large_order_single_problem():
     assert ((th.grad - th2.grad).abs().max() / th2.grad.abs().max()) < 1e-8
 
 
-def test_not_positive_definite_raises():
+@pytest.mark.parametrize("n", [50, 600])
+def test_not_positive_definite_raises(n):
     torch = _t()
-    A, y = spd(3, 50, torch.float64, 3)
+    A, y = spd(3, n, torch.float64, 3)
     A[1, 10, 10] = -5.0
     with pytest.raises(RuntimeError, match="matrix 1"):
         _ag().chol_nll(A, y)
 
 
-@pytest.mark.parametrize("n,batch", [(1, 3), (15, 2), (17, 5), (33, 1), (100, 4), (255, 2), (512, 1), (1000, 3),
-                                     (1024, 2)])
+@pytest.mark.parametrize("n,batch", [(1, 3), (15, 2), (17, 5), (33, 1), (64, 2), (65, 3), (100, 4), (129, 2),
+                                     (255, 2), (512, 1), (640, 2), (1000, 3), (1024, 2)])
 @pytest.mark.parametrize("dtype", ["float64", "float32"])
 def test_trtri_batched_inverse(n, batch, dtype):
     """ddlak_trtri_batched (W = L^-1, the lower triangle) against the inverse
