@@ -445,11 +445,11 @@ int gp_build_t(int batch, int n, int d, const void* X, long long xstride, const 
 //           upper block W(o.., o+h..), which the result does not use;
 //   step 2: W21 = -W22 T (W22 lower: k <= i), written to W(o+h.., o..).
 // 64 x 64 tiles, 4 warps of 32 x 32, k in chunks of 32 staged by cp.async
-// (3 stages); shared rows padded to 68 / 36 doubles so that the fragment reads
+// (double-buffered, three CTAs per SM); shared rows padded to 68 / 36 doubles so that the fragment reads
 // are conflict free.  The strictly upper triangles of W are read nowhere
 // (masked) and are overwritten as scratch.
 // ---------------------------------------------------------------------------
-constexpr int TL_BK = 32, TL_NS = 3, TL_LDK = 68, TL_LDJ = 36;
+constexpr int TL_BK = 32, TL_NS = 2, TL_LDK = 68, TL_LDJ = 36;  // 2 stages: 72 KB, 3 CTAs per SM
 constexpr int TL_ASZ = TL_BK * TL_LDK;  // A slice [k][i]
 constexpr int TL_BSZ = 64 * TL_LDJ;     // B slice [j][k] (step 1) or [k][j] (step 2, 32 x 68 fits)
 constexpr size_t TL_SMEM = (size_t)TL_NS * (TL_ASZ + TL_BSZ) * sizeof(double);
@@ -617,15 +617,17 @@ int trtri_t(int batch, int n, const void* L, long long ldl, long long lstride, v
 
 // ---------------------------------------------------------------------------
 // The FP64 contraction (not DIRECT) on the FP64 tensor cores: the same tiles
-// and epilogues, C(i, j) = sum_k W(k, i) W(k, j) by DMMA (mma.sync m8n8k4 f64,
+// and epilogues, C(i, j) = sum_k W(k, i) W(k, j) by DMMA (mma.sync m16n8k4 f64,
 // 8 warps of 64 x 32).  Operand slices arrive by TMA from the batch of W seen as
 // a 3-D tensor: per stage the columns i0 .. i0+127 and j0 .. j0+127 over 32 k,
 // as boxes of 36 k (the 4 extra pad the shared rows to 36 doubles, which keeps
-// the fragment reads conflict free) x 128 columns, 3 stages.  W's strictly upper
-// triangle is not written by the inversion, so the chunks that reach it (k <
-// i0 + 128) are masked in shared memory.  A stage's arrival wait is bounded: if
-// it gives up the tile's result is NaN (the gradient comes back NaN) after a
-// bounded wait for the copies still in flight.
+// the fragment reads conflict free) x 128 columns, 3 stages; each warp releases
+// a stage on its `empty` mbarrier, with no CTA barrier per chunk.  W's strictly
+// upper triangle is unspecified after the inversion (the recursive one keeps
+// scratch there), so in the chunks that reach it (k < i0 + 128) the fragments
+// are masked as they are read.  Every wait is bounded: if one gives up the
+// tile's result is NaN (the gradient comes back NaN) after a bounded wait for
+// the copies still in flight.
 // ---------------------------------------------------------------------------
 constexpr int AD_BK = 32, AD_LDK = 36, AD_NS = 3;
 constexpr int AD_BOX = CT_TILE * AD_LDK;
@@ -633,13 +635,6 @@ constexpr unsigned AD_BOX_BYTES = AD_BOX * 8u;  // 36864
 constexpr size_t AD_SMEM = (size_t)AD_NS * 2 * AD_BOX_BYTES + 128;
 
 __device__ int g_adjoint_status;
-
-__device__ __forceinline__ void dmma_f64(double& d0, double& d1, double a, double b)
-{
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
-                 : "+d"(d0), "+d"(d1)
-                 : "d"(a), "d"(b));
-}
 
 template <int MODE>
 __global__ void __launch_bounds__(CT_NT, 1)
@@ -649,9 +644,11 @@ __global__ void __launch_bounds__(CT_NT, 1)
                             double* __restrict__ G, long long ldg, long long gstride)
 {
     extern __shared__ __align__(128) unsigned char ad_raw[];
-    __shared__ __align__(8) uint64_t full[AD_NS];
+    __shared__ __align__(8) uint64_t full[AD_NS], empty[AD_NS];
     __shared__ double red[3][CT_NT / 32];
-    const int m = blockIdx.y, tile = blockIdx.x;
+    // blockIdx.x = matrix, blockIdx.y = tile: the grid runs every matrix's longest tiles
+    // (smallest i0, the most k) first
+    const int m = blockIdx.x, tile = blockIdx.y;
     int ti, tj;
     tile_of_lower(tile, ti, tj);
     const int i0 = ti * CT_TILE, j0 = tj * CT_TILE;
@@ -668,7 +665,10 @@ __global__ void __launch_bounds__(CT_NT, 1)
         tc::tma_load_3d(st + AD_BOX, &wmap, &full[s], kbeg + c * AD_BK, j0, m);
     };
     if (t == 0) {
-        for (int s = 0; s < AD_NS; ++s) tc::mbar_init(&full[s], 1);
+        for (int s = 0; s < AD_NS; ++s) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], CT_NT / 32);  // one arrival per warp
+        }
         tc::mbar_fence_init();
         tc::prefetch_tmap(&wmap);
         for (int c = 0; c < AD_NS && c < nch; ++c) issue(c);
@@ -680,43 +680,59 @@ __global__ void __launch_bounds__(CT_NT, 1)
 #pragma unroll
         for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
     bool ok = true;
-    int consumed = 0;
+    int consumed = 0, issued = nch < AD_NS ? nch : AD_NS;  // issued: thread 0's count
     for (int c = 0; c < nch; ++c) {
         const int s = c % AD_NS;
-        ok = __syncthreads_and(tc::mbar_wait(&full[s], (uint32_t)((c / AD_NS) & 1), &g_adjoint_status, 0x61));
-        if (!ok) break;
-        consumed = c + 1;
-        double* Wi = sm + (size_t)s * 2 * AD_BOX;
-        double* Wj = Wi + AD_BOX;
-        const int k0 = kbeg + c * AD_BK;
-        if (k0 < i0 + CT_TILE) {
-            // zero W(k, col) for k < col (the unwritten upper triangle) in this chunk
-            for (int e = t; e < CT_TILE * AD_BK; e += CT_NT) {
-                const int cl = e / AD_BK, kl = e % AD_BK;
-                if (k0 + kl < i0 + cl) Wi[cl * AD_LDK + kl] = 0.0;
-                if (ti == tj && k0 + kl < j0 + cl) Wj[cl * AD_LDK + kl] = 0.0;
-            }
-            tc::fence_proxy_async_smem();
-            __syncthreads();
+        if (!tc::mbar_wait(&full[s], (uint32_t)((c / AD_NS) & 1), &g_adjoint_status, 0x61)) {
+            ok = false;
+            break;
         }
+        consumed = c + 1;
+        const double* Wi = sm + (size_t)s * 2 * AD_BOX;
+        const double* Wj = Wi + AD_BOX;
+        const int k0 = kbeg + c * AD_BK;
+        // W(k, col) = 0 for k < col (the strictly upper triangle, which the inversion
+        // leaves unspecified): applied to the fragments of the chunks that reach it
+        const bool mask_i = k0 < i0 + CT_TILE, mask_j = mask_i && ti == tj;
 #pragma unroll
         for (int kk = 0; kk < AD_BK; kk += 4) {
+            const int k = k0 + kk + q;
             double af[8], bf[4];
 #pragma unroll
-            for (int a = 0; a < 8; ++a) af[a] = Wi[(wm * 64 + a * 8 + g) * AD_LDK + kk + q];
+            for (int a = 0; a < 8; ++a) {
+                const int cl = wm * 64 + a * 8 + g;
+                const double v = Wi[cl * AD_LDK + kk + q];
+                af[a] = (mask_i && k < i0 + cl) ? 0.0 : v;
+            }
 #pragma unroll
-            for (int b = 0; b < 4; ++b) bf[b] = Wj[(wn * 32 + b * 8 + g) * AD_LDK + kk + q];
+            for (int b = 0; b < 4; ++b) {
+                const int cl = wn * 32 + b * 8 + g;
+                const double v = Wj[cl * AD_LDK + kk + q];
+                bf[b] = (mask_j && k < j0 + cl) ? 0.0 : v;
+            }
+            // rows a*8+g and (a+1)*8+g as one m16n8k4 product: the same accumulators as two m8n8k4
 #pragma unroll
-            for (int a = 0; a < 8; ++a)
+            for (int a = 0; a < 8; a += 2)
 #pragma unroll
-                for (int b = 0; b < 4; ++b) dmma_f64(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+                for (int b = 0; b < 4; ++b) tl_mma(acc[a][b], acc[a + 1][b], af[a], af[a + 1], bf[b]);
         }
-        __syncthreads();
-        if (t == 0 && c + AD_NS < nch) issue(c + AD_NS);
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&empty[s]);  // this warp is done with stage s
+        if (t == 0 && c >= 1 && c - 1 + AD_NS < nch) {
+            const int cp = c - 1;  // refill chunk cp's stage with chunk cp + NS
+            if (!tc::mbar_wait(&empty[cp % AD_NS], (uint32_t)((cp / AD_NS) & 1), &g_adjoint_status, 0x63)) {
+                ok = false;
+                break;
+            }
+            issue(cp + AD_NS);
+            issued = cp + AD_NS + 1;
+        }
     }
+    ok = __syncthreads_and(ok);
     if (!ok) {
+        // copies issued for chunks consumed .. issued - 1 may still be in flight
         if (t == 0)
-            for (int c = consumed; c < nch && c < consumed + AD_NS; ++c)
+            for (int c = consumed; c < issued; ++c)
                 (void)tc::mbar_wait(&full[c % AD_NS], (uint32_t)((c / AD_NS) & 1), &g_adjoint_status, 0x62);
         __syncthreads();
         const double nan = __longlong_as_double(0x7ff8000000000000LL);
@@ -744,34 +760,40 @@ __global__ void __launch_bounds__(CT_NT, 1)
                     }
                 }
     } else {
+        // the tile into shared memory (the operand stages are free: every chunk was consumed and
+        // the barrier above passed), then one rolled loop over its entries, so that the
+        // exponential's code is not replicated for every fragment entry
+        constexpr int CLD = CT_TILE + 1;
+        double* cs = sm;
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+#pragma unroll
+                for (int e = 0; e < 2; ++e)
+                    cs[(wm * 64 + a * 8 + g) * CLD + wn * 32 + b * 8 + 2 * q + e] = acc[a][b][e];
+        __syncthreads();
         const double* th = theta + (long long)m * tstride;
         const double l = th[0], sf2 = th[1];
         const double inv2l2 = 0.5 / (l * l), invl3 = 1.0 / (l * l * l);
         const double* x = X + m * xstride;
         double g0 = 0.0, g1 = 0.0, g2 = 0.0;
-#pragma unroll
-        for (int a = 0; a < 8; ++a) {
-            const int i = row_of(a);
-            if (i >= n) continue;
-            const double ai = al[i];
-#pragma unroll
-            for (int b = 0; b < 4; ++b)
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const int j = col_of(b, e);
-                    if (j > i) continue;
-                    const double ab = 0.5 * (acc[a][b][e] - ai * al[j]);
-                    const double w = i == j ? 1.0 : 2.0;
-                    double r2 = 0.0;
-                    for (int cc = 0; cc < d; ++cc) {
-                        const double dx = x[(long long)i * d + cc] - x[(long long)j * d + cc];
-                        r2 += dx * dx;
-                    }
-                    const double ex = exp(-r2 * inv2l2);
-                    g0 += w * ab * sf2 * ex * r2 * invl3;  // dA/dl
-                    g1 += w * ab * ex;                     // dA/dsigma_f^2
-                    if (i == j) g2 += ab;                  // dA/dsigma^2
-                }
+#pragma unroll 1
+        for (int e = t; e < CT_TILE * CT_TILE; e += CT_NT) {
+            const int il = e / CT_TILE, jl = e % CT_TILE;
+            const int i = i0 + il, j = j0 + jl;
+            if (i >= n || j > i) continue;
+            const double ab = 0.5 * (cs[il * CLD + jl] - al[i] * al[j]);
+            const double w = i == j ? 1.0 : 2.0;
+            double r2 = 0.0;
+            for (int cc = 0; cc < d; ++cc) {
+                const double dx = x[(long long)i * d + cc] - x[(long long)j * d + cc];
+                r2 += dx * dx;
+            }
+            const double ex = exp(-r2 * inv2l2);
+            g0 += w * ab * sf2 * ex * r2 * invl3;  // dA/dl
+            g1 += w * ab * ex;                     // dA/dsigma_f^2
+            if (i == j) g2 += ab;                  // dA/dsigma^2
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -788,7 +810,7 @@ __global__ void __launch_bounds__(CT_NT, 1)
         if (t < 3) {
             double sum = 0.0;
             for (int w = 0; w < CT_NT / 32; ++w) sum += red[t][w];
-            partial[((long long)m * gridDim.x + tile) * 3 + t] = sum;
+            partial[((long long)m * gridDim.y + tile) * 3 + t] = sum;
         }
     }
 }
@@ -806,7 +828,8 @@ bool contract_dmma(int mode, int batch, int n, const double* W, long long ldw, l
         return false;
     const int nt = (n + CT_TILE - 1) / CT_TILE;
     const int ntiles = nt * (nt + 1) / 2;
-    dim3 grid(ntiles, batch);
+    if (ntiles > 65535) return false;
+    dim3 grid(batch, ntiles);
     if (mode == 0) {
         if ((*err = smem_optin(k_adjoint_contract_dmma<0>, AD_SMEM)) != cudaSuccess) return true;
         k_adjoint_contract_dmma<0><<<grid, CT_NT, AD_SMEM, st>>>(wmap, n, alpha, astride, X, d, xstride, theta,

@@ -372,10 +372,11 @@ bool launch_dmma_tma(double* A, long long lda, int k0, int nbk, int n, long long
 }  // namespace
 
 // The same over a batch of equal-order matrices (blockIdx.y = matrix, astride
-// elements apart, info per matrix): the lower triangle from row / column t0
-// (cols == 0).  False (nothing launched) when the TMA conditions do not hold.
+// elements apart, info per matrix): the region from row / column t0, all of it
+// (cols == 0) or its first cols columns.  False (nothing launched) when the TMA
+// conditions do not hold.
 bool launch_dmma_tma_batched(double* A, long long lda, long long astride, int batch, int k0, int nbk, int n,
-                             long long t0, const int* dinfo, cudaStream_t st, cudaError_t* err)
+                             long long t0, int cols, const int* dinfo, cudaStream_t st, cudaError_t* err)
 {
     if ((lda & 1) || (astride & 1) || (reinterpret_cast<uintptr_t>(A) & 15) || (t0 & 1) || nbk % DT_BK != 0 ||
         nbk <= 0 || batch < 1 || batch > 65535)
@@ -390,8 +391,8 @@ bool launch_dmma_tma_batched(double* A, long long lda, long long astride, int ba
         return false;
     if ((*err = smem_optin(k_syrk_dmma_tma<true>, DT_SMEM)) != cudaSuccess) return true;
     const long long t = ceil_div(m, DM_BM);
-    const dim3 grid((unsigned)(t * (t + 1) / 2), (unsigned)batch);
-    k_syrk_dmma_tma<true><<<grid, 256, DT_SMEM, st>>>(amap, A, lda, astride, k0, nbk, n, t0, 0, dinfo);
+    const dim3 grid((unsigned)(cols == 0 ? t * (t + 1) / 2 : t * ceil_div(cols, DM_BM)), (unsigned)batch);
+    k_syrk_dmma_tma<true><<<grid, 256, DT_SMEM, st>>>(amap, A, lda, astride, k0, nbk, n, t0, cols, dinfo);
     *err = cudaGetLastError();
     return true;
 }
