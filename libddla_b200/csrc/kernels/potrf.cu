@@ -645,16 +645,23 @@ __global__ void __launch_bounds__(PB_NT) k_potrs_batched_f64(int n, const double
     __syncthreads();
     for (int b0 = 0; b0 < n; b0 += 32) {
         const int w = n - b0 < 32 ? n - b0 : 32;
+        // the block's lower triangle into shared memory first (all warps, coalesced), so that
+        // warp 0's chain reads no global memory
+        for (int e = t; e < 32 * 32; e += PB_NT) {
+            const int r = e & 31, c = e >> 5;
+            blk[r][c] = (r < w && c <= r) ? L[(b0 + r) + (long long)(b0 + c) * lda] : 0.0;
+        }
+        __syncthreads();
         if (warp == 0) {
             double xi = lane < w ? x[b0 + lane] : 0.0;
             for (int j = 0; j < w; ++j) {
                 if (lane == j) {
-                    const double d = L[(b0 + j) + (long long)(b0 + j) * lda];
+                    const double d = blk[j][j];
                     xi = xi / d;
                     ld += log(d);
                 }
                 const double xj = __shfl_sync(0xffffffffu, xi, j);
-                if (lane > j && lane < w) xi = fma(-L[(b0 + lane) + (long long)(b0 + j) * lda], xj, xi);
+                if (lane > j && lane < w) xi = fma(-blk[lane][j], xj, xi);
             }
             if (lane < w) x[b0 + lane] = xi;
         }
@@ -683,8 +690,10 @@ __global__ void __launch_bounds__(PB_NT) k_potrs_batched_f64(int n, const double
             for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
             if (lane == 0) x[b0 + i] -= acc;
         }
-        if (warp == 1)  // the block itself, for the transposed solve
-            for (int c = 0; c < w; ++c) blk[lane][c] = lane < w ? L[(b0 + lane) + (long long)(b0 + c) * lda] : 0.0;
+        for (int e = t; e < 32 * 32; e += PB_NT) {  // the block itself, for the transposed solve
+            const int r = e & 31, c = e >> 5;
+            blk[r][c] = (r < w && c <= r) ? L[(b0 + r) + (long long)(b0 + c) * lda] : 0.0;
+        }
         __syncthreads();
         if (warp == 0) {
             double xi = lane < w ? x[b0 + lane] : 0.0;
@@ -701,11 +710,13 @@ __global__ void __launch_bounds__(PB_NT) k_potrs_batched_f64(int n, const double
     if (t == 0 && logdet) logdet[m] = s_ld;
 }
 
-// A batch of equal-order FP64 matrices (lower), right-looking by block columns
-// of 128, each step one launch per kernel over the whole batch: the diagonal
-// blocks (one CTA per matrix), the panels (row-per-thread solve, grid.y =
-// matrix) and the trailing updates (TMA DMMA tiles, grid.y = matrix).  The
-// same operations as the single-matrix factorization without look-ahead.
+// A batch of equal-order FP64 matrices (lower), right-looking by super-steps of
+// two block columns of 128, each step one launch per kernel over the whole
+// batch: the diagonal blocks (one CTA per matrix), the panels (row-per-thread
+// solve, grid.y = matrix) and the updates (TMA DMMA tiles, grid.y = matrix).
+// In a super-step, block column 1 first takes block column 0's update of its own
+// 128 columns, and the rest of the trailing matrix is updated once with K = 256,
+// so the trailing matrix is read and written once per 256 columns.
 extern "C" int ddlak_potrf_batched_f64(int batch, int n, void* A_, long long lda, long long astride, int* dinfo,
                                        void* stream)
 {
@@ -719,12 +730,12 @@ extern "C" int ddlak_potrf_batched_f64(int batch, int n, void* A_, long long lda
         return (int)cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(dinfo, 0, sizeof(int) * (size_t)batch, st);
     if (e != cudaSuccess || n == 0) return (int)e;
-    constexpr int NB = 128;
+    constexpr int NB = 128, G = 2;
     const size_t diag_smem = (size_t)NB * diag_block_ld<double>(NB) * sizeof(double);
     if ((e = smem_optin(k_potrf_diag<double, false>, diag_smem)) != cudaSuccess) return (int)e;
     if ((e = smem_optin(k_trsm_panel_rows_f64, TRD_SMEM)) != cudaSuccess) return (int)e;
     const double nb3 = (double)batch;
-    for (int k0 = 0; k0 < n; k0 += NB) {
+    auto diag_and_panel = [&](int k0) -> cudaError_t {
         const int nbk = n - k0 < NB ? n - k0 : NB;
         const double b = nbk;
         {
@@ -734,22 +745,38 @@ extern "C" int ddlak_potrf_batched_f64(int batch, int n, void* A_, long long lda
         }
         note_launches(1);
         const long long m = (long long)n - k0 - nbk;
-        if (m <= 0) break;
-        {
+        if (m > 0) {
             const double md = (double)m;
             ProfScope ps(PK_TRSM_PANEL, st, nb3 * md * b * b, nb3 * 8.0 * (2.0 * md * b + b * (b + 1) / 2));
             k_trsm_panel_rows_f64<<<dim3((unsigned)ceil_div(m, TRD_NT), (unsigned)batch), TRD_NT, TRD_SMEM, st>>>(
                 A, lda, astride, k0, nbk, n, dinfo);
+            note_launches(1);
         }
+        return cudaGetLastError();
+    };
+    // C -= L(:, k0 : k0 + kw) L(:, k0 : k0 + kw)^T on the region from t0 (all of it, or cols columns)
+    auto update = [&](int k0, int kw, long long t0, int cols) -> cudaError_t {
+        const double md = (double)(n - t0), b = kw;
+        const double cw = cols ? (double)cols : md;
+        const double fl = cols ? 2.0 * b * (md * cw - cw * (cw - 1) / 2) : md * (md + 1) * b;
+        ProfScope ps(PK_SYRK_UPDATE, st, nb3 * fl, nb3 * 8.0 * ((cols ? 2.0 * md * cw : md * (md + 1)) + md * b));
+        cudaError_t ue = cudaSuccess;
+        if (!launch_dmma_tma_batched(A, lda, astride, batch, k0, kw, n, t0, cols, dinfo, st, &ue))
+            return cudaErrorInvalidValue;
         note_launches(1);
-        {
-            const double md = (double)m;
-            ProfScope ps(PK_SYRK_UPDATE, st, nb3 * md * (md + 1) * b, nb3 * 8.0 * (md * (md + 1) + md * b));
-            if (!launch_dmma_tma_batched(A, lda, astride, batch, k0, nbk, n, (long long)k0 + nbk, dinfo, st, &e))
-                return (int)cudaErrorInvalidValue;
-            if (e != cudaSuccess) return (int)e;
-        }
-        note_launches(1);
+        return ue;
+    };
+    for (int k0 = 0; k0 < n; k0 += G * NB) {
+        if ((e = diag_and_panel(k0)) != cudaSuccess) return (int)e;
+        const int k1 = k0 + NB;
+        if (k1 >= n) break;
+        // block column 1 of the super-step: block column 0's update of its own columns, then its factor
+        const int c1 = n - k1 < NB ? n - k1 : NB;
+        if ((e = update(k0, NB, k1, c1)) != cudaSuccess) return (int)e;
+        if ((e = diag_and_panel(k1)) != cudaSuccess) return (int)e;
+        const long long t0 = (long long)k0 + G * NB;
+        if (t0 >= n) break;
+        if ((e = update(k0, G * NB, t0, 0)) != cudaSuccess) return (int)e;
     }
     return (int)cudaGetLastError();
 }
