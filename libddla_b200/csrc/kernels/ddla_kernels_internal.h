@@ -24,11 +24,6 @@ cudaError_t launch_trsm_panel(T* A, long long lda, int k0, int nbk, int n, const
 bool launch_dmma_tma_batched(double* A, long long lda, long long astride, int batch, int k0, int nbk, int n,
                              long long t0, int cols, const int* dinfo, cudaStream_t st, cudaError_t* err);
 
-// The mixed factorization's FP32 panel (lower) as A21 W11^T with W11 = L11^-1
-// computed into inv (128 x 128 floats of scratch), potrf.cu.
-cudaError_t launch_trsm_panel_inv(float* A, long long lda, int k0, int nbk, int n, float* inv, const int* dinfo,
-                                  cudaStream_t s);
-
 template <class T, bool UP>
 cudaError_t trailing_update_simt(T* A, long long lda, int k0, int nbk, int n, long long t0, int cols,
                                  const int* dinfo, cudaStream_t st);

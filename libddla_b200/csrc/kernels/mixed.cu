@@ -252,14 +252,17 @@ __global__ void __launch_bounds__(128, 3) k_mixed_update(const __grid_constant__
 
     if (threadIdx.x == 0) {
         tc::prefetch_tmap(&pmap);
+        // the panel is read by every tile of its row and column: keep it in L2 ahead of the
+        // W tiles, which stream through once (evict_first on their load and store)
+        const uint64_t keep = tc::l2_policy_evict_last();
         for (int kb = 0; kb < nkb; ++kb) {
             const int s = kb % MU_STAGES;
             if (kb >= MU_STAGES && !tc::mbar_wait(&empty[s], ((kb / MU_STAGES) - 1) & 1, status, MU_ERR_EMPTY)) break;
             unsigned char* sa = base + (size_t)s * 2 * MU_TILE_BYTES;
             tc::mbar_expect_tx(&full[s], 2 * MU_TILE_BYTES);
             const int x = kb * (TF32 ? 32 : 64);
-            tc::tma_load_2d(sa, &pmap, &full[s], x, (int)(ri - pr0));
-            tc::tma_load_2d(sa + MU_TILE_BYTES, &pmap, &full[s], x, (int)(rj - pr0));
+            tc::tma_load_2d_hint(sa, &pmap, &full[s], x, (int)(ri - pr0), keep);
+            tc::tma_load_2d_hint(sa + MU_TILE_BYTES, &pmap, &full[s], x, (int)(rj - pr0), keep);
         }
     } else if (threadIdx.x == 32) {
         constexpr uint32_t idesc = tc::idesc_m128_n128<TF32>();
@@ -293,7 +296,7 @@ __global__ void __launch_bounds__(128, 3) k_mixed_update(const __grid_constant__
     if (__syncthreads_and(ok)) {
         if (threadIdx.x == 0) {
             tc::mbar_expect_tx(&cbar, 128 * 128 * 4);
-            tc::tma_load_2d(ct, &wmap, &cbar, (int)ri, (int)rj);
+            tc::tma_load_2d_hint(ct, &wmap, &cbar, (int)ri, (int)rj, tc::l2_policy_evict_first());
         }
         ok = tc::mbar_wait(&cbar, 0, status, MU_ERR_CTILE);
         ok = __all_sync(0xffffffffu, ok);
@@ -309,7 +312,7 @@ __global__ void __launch_bounds__(128, 3) k_mixed_update(const __grid_constant__
             tc::fence_proxy_async_smem();
         }
         if (__syncthreads_and(ok) && threadIdx.x == 0) {
-            tc::tma_store_2d(&wmap, ct, (int)ri, (int)rj);
+            tc::tma_store_2d_hint(&wmap, ct, (int)ri, (int)rj, tc::l2_policy_evict_first());
             tc::tma_store_wait_read();
         }
     }
