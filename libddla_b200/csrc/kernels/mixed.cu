@@ -325,6 +325,136 @@ __global__ void __launch_bounds__(128, 3) k_mixed_update(const __grid_constant__
 }
 
 // ---------------------------------------------------------------------------
+// The same update over the whole region from t0 by pairs of tiles (I, 2P) and
+// (I, 2P + 1) of one tile row: one 128 x 256 MMA accumulator (TMEM columns
+// 0..255), the A rows loaded once for both tiles, so each C tile costs 3/4 of
+// the operand bytes of the single-tile kernel; two CTAs per SM (96 KB of
+// operand stages each).  The epilogue runs the two C tiles one after the other
+// through the freed stages; a pair whose second tile lies above the diagonal
+// computes it (the MMA is 256 wide) but neither loads nor stores it.
+// ---------------------------------------------------------------------------
+constexpr int MP_STAGES = 2;
+constexpr int MP_STAGE_BYTES = 3 * MU_TILE_BYTES;  // A (128 rows) + B (256 rows) of 128 bytes
+constexpr size_t MP_SMEM = (size_t)MP_STAGES * MP_STAGE_BYTES + 1024;
+
+// first pair of tile row I: rows 0..I-1 hold floor(i / 2) + 1 pairs each
+__host__ __device__ __forceinline__ long long pair_start(long long I)
+{
+    return (I & 1) ? ((I + 1) / 2) * ((I + 1) / 2) : (I / 2) * (I / 2 + 1);
+}
+__device__ __forceinline__ void pair_of(long long b, int& I, int& P)
+{
+    long long i = (long long)(2.0 * sqrt((double)b)) - 1;
+    if (i < 0) i = 0;
+    while (pair_start(i + 1) <= b) ++i;
+    while (i > 0 && pair_start(i) > b) --i;
+    I = (int)i;
+    P = (int)(b - pair_start(i));
+}
+
+template <bool TF32>
+__global__ void __launch_bounds__(128, 2) k_mixed_update_pair(const __grid_constant__ CUtensorMap pmap,
+                                                              const __grid_constant__ CUtensorMap wmap, int n,
+                                                              long long t0, long long pr0, int nkb,
+                                                              const int* __restrict__ info, int* __restrict__ status)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[MP_STAGES], empty[MP_STAGES], done, cbar;
+    __shared__ uint32_t s_tmem;
+    if (*(volatile const int*)info != 0) return;
+    int I, P;
+    pair_of(blockIdx.x, I, P);
+    const long long ri = t0 + (long long)I * 128, rj = t0 + (long long)P * 256;
+    const int halves = (2 * P + 1 <= I) ? 2 : 1;  // the second tile of the pair lies on or below the diagonal
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < MP_STAGES; ++s) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        tc::mbar_init(&done, 1);
+        tc::mbar_init(&cbar, 1);
+        tc::mbar_fence_init();
+    }
+    if (warp == 0) tc::tmem_alloc(&s_tmem, 256);
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = s_tmem;
+
+    if (threadIdx.x == 0) {
+        tc::prefetch_tmap(&pmap);
+        const uint64_t keep = tc::l2_policy_evict_last();
+        for (int kb = 0; kb < nkb; ++kb) {
+            const int s = kb % MP_STAGES;
+            if (kb >= MP_STAGES && !tc::mbar_wait(&empty[s], ((kb / MP_STAGES) - 1) & 1, status, MU_ERR_EMPTY)) break;
+            unsigned char* sa = base + (size_t)s * MP_STAGE_BYTES;
+            tc::mbar_expect_tx(&full[s], MP_STAGE_BYTES);
+            const int x = kb * (TF32 ? 32 : 64);
+            tc::tma_load_2d_hint(sa, &pmap, &full[s], x, (int)(ri - pr0), keep);
+            tc::tma_load_2d_hint(sa + MU_TILE_BYTES, &pmap, &full[s], x, (int)(rj - pr0), keep);
+            tc::tma_load_2d_hint(sa + 2 * MU_TILE_BYTES, &pmap, &full[s], x, (int)(rj + 128 - pr0), keep);
+        }
+    } else if (threadIdx.x == 32) {
+        constexpr uint32_t idesc = tc::idesc_m128_n256<TF32>();
+        bool ok = true;
+        for (int kb = 0; kb < nkb && ok; ++kb) {
+            const int s = kb % MP_STAGES;
+            ok = tc::mbar_wait(&full[s], (kb / MP_STAGES) & 1, status, MU_ERR_FULL);
+            if (!ok) break;
+            tc::tc_fence_after();
+            const unsigned char* sa = base + (size_t)s * MP_STAGE_BYTES;
+            const uint64_t ad = tc::smem_desc_sw128(sa), bd = tc::smem_desc_sw128(sa + MU_TILE_BYTES);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)  // four K steps of 32 bytes per 128-byte row
+                tc::umma<TF32>(tmem, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0 ? 1u : 0u);
+            tc::umma_commit(&empty[s]);
+        }
+        tc::umma_commit(&done);
+    }
+    __syncwarp();
+
+    // epilogue: the two C tiles in turn through the freed stages (64 KB each)
+    bool ok = tc::mbar_wait(&done, 0, status, MU_ERR_DONE);
+    ok = __all_sync(0xffffffffu, ok);
+    tc::tc_fence_after();
+    float* ct = reinterpret_cast<float*>(base);  // [128 cols][128 rows]
+    const uint64_t stream_once = tc::l2_policy_evict_first();
+    for (int h = 0; h < halves; ++h) {
+        if (!__syncthreads_and(ok)) break;
+        if (threadIdx.x == 0) {
+            if (h > 0) tc::tma_store_wait_read();  // the first tile's store has left the buffer
+            tc::mbar_expect_tx(&cbar, 128 * 128 * 4);
+            tc::tma_load_2d_hint(ct, &wmap, &cbar, (int)ri, (int)(rj + 128 * h), stream_once);
+        }
+        ok = tc::mbar_wait(&cbar, (uint32_t)h, status, MU_ERR_CTILE);
+        ok = __all_sync(0xffffffffu, ok);
+        if (ok) {
+            const int r = 32 * warp + lane;
+#pragma unroll 1
+            for (int c = 0; c < 4; ++c) {
+                float v[32];
+                tc::tmem_ld_32x32b_x32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(128 * h + 32 * c), v);
+#pragma unroll
+                for (int e = 0; e < 32; ++e) ct[(32 * c + e) * 128 + r] -= v[e];
+            }
+            tc::fence_proxy_async_smem();
+        }
+        if (__syncthreads_and(ok) && threadIdx.x == 0)
+            tc::tma_store_2d_hint(&wmap, ct, (int)ri, (int)(rj + 128 * h), stream_once);
+    }
+    if (threadIdx.x == 0) tc::tma_store_wait_read();
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, 256);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // R = B - A X for symmetric A stored in its lower triangle (FP64), NC (8 or 16)
 // right-hand sides per chunk (grid.y).  Every lower tile A(I, J), I >= J, is
 // read from HBM once and used twice: A(I,J) X(J) goes to R(I) and A(I,J)^T X(I)
@@ -881,6 +1011,14 @@ cudaError_t mixed_update(float* W, long long ldw, int n, long long t0, long long
     const double md = (double)m, cw = cols ? (double)cols : md;
     const double fl = cols ? 2.0 * nbk * (md * cw - cw * (cw - 1) / 2) : md * (md + 1) * nbk;
     ProfScope ps(PK_MIXED_UPDATE, st, fl, 4.0 * (cols ? 2.0 * md * cw : md * (md + 1)));
+    if (cols == 0 && t >= 4) {
+        // the whole trailing region by pairs of tiles sharing their A rows
+        if (cudaError_t e = smem_optin(k_mixed_update_pair<TF32>, MP_SMEM); e != cudaSuccess) return e;
+        k_mixed_update_pair<TF32><<<(unsigned)pair_start(t), 128, MP_SMEM, st>>>(map, wmap, n, t0, pr0, nkb, dinfo,
+                                                                                 status);
+        note_launches(1);
+        return cudaGetLastError();
+    }
     k_mixed_update<TF32><<<(unsigned)grid, 128, MU_SMEM, st>>>(map, wmap, W, ldw, n, t0, pr0, cols, nkb, dinfo,
                                                                status);
     note_launches(1);

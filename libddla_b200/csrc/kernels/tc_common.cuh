@@ -263,6 +263,12 @@ __host__ __device__ constexpr uint32_t idesc_m128_n128()
 {
     return (1u << 4) | ((TF32 ? 2u : 1u) << 7) | ((TF32 ? 2u : 1u) << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
 }
+// the same with N = 256 (B: 256 rows; the accumulator takes 256 TMEM columns)
+template <bool TF32>
+__host__ __device__ constexpr uint32_t idesc_m128_n256()
+{
+    return (1u << 4) | ((TF32 ? 2u : 1u) << 7) | ((TF32 ? 2u : 1u) << 10) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+}
 
 }  // namespace tc
 }  // namespace ddlak
