@@ -25,6 +25,7 @@
 #include "ddla_kernels_internal.h"
 #include "diag_factor.cuh"
 #include "profile.h"
+#include "tc_common.cuh"
 
 namespace ddlak {
 
@@ -358,8 +359,9 @@ __global__ void __launch_bounds__(TRR_NT) k_trsm_panel_rows(float* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// The FP64 panel (lower storage, nbk <= 128): one thread per row, in four
-// chunks of 32 columns so that 32 of the row's values are live in registers.
+// The FP64 panel (lower storage, nbk <= 128): L11 staged in shared memory by TMA
+// (ten 32 x 32 boxes, one mbarrier) when lda is even, then one thread per row, in
+// four chunks of 32 columns so that 32 of the row's values are live in registers.
 // Chunk C: x = row[32C : 32C + 32]; x -= x_J L11[32C.., 32J..]^T for the
 // chunks J < C (their solved values re-read from the row this thread already
 // wrote); then x is solved against the diagonal block (x_j *= 1 / l_jj,
@@ -380,26 +382,57 @@ __device__ __forceinline__ double2 ld_shared_d2(const double2* p)
     return v;
 }
 
-__global__ void __launch_bounds__(TRD_NT) k_trsm_panel_rows_f64(double* __restrict__ A, long long lda,
+// TMA_DIMS: 0 = L11 staged by plain loads (any lda, any nbk); 2 = by ten 32 x 32 TMA
+// boxes from a 2-D map over A; 3 = the same from a 3-D map over a batch (z = matrix).
+// The TMA forms need nbk = 128: they load whole boxes, so the diagonal blocks'
+// upper halves come in unmasked (the solve reads only entries below the diagonal).
+__device__ int g_trsm_status;  // a TMA wait that gave up (never expected): the panel is NaN-poisoned
+
+template <int TMA_DIMS>
+__global__ void __launch_bounds__(TRD_NT) k_trsm_panel_rows_f64(const __grid_constant__ CUtensorMap amap,
+                                                                double* __restrict__ A, long long lda,
                                                                 long long astride, int k0, int nbk, int n,
                                                                 const int* __restrict__ info)
 {
     // block (C, J), J <= C, at trd_smem + (C (C + 1) / 2 + J) * 1024, element [j * 32 + i]
-    // = L(k0 + 32 C + i, k0 + 32 J + j), zero above the diagonal and past nbk
-    extern __shared__ __align__(16) double trd_smem[];
+    // = L(k0 + 32 C + i, k0 + 32 J + j) (zero above the diagonal and past nbk when staged by loads)
+    extern __shared__ __align__(128) double trd_smem[];
     __shared__ double rinv[128];
+    __shared__ __align__(8) uint64_t l11_bar;
     A += (long long)blockIdx.y * astride;  // blockIdx.y: the matrix of a batch
     info += blockIdx.y;
     if (*(volatile const int*)info != 0) return;
-    const double* Ad = A + k0 + (long long)k0 * lda;
-    for (int idx = threadIdx.x; idx < 10 * 1024; idx += TRD_NT) {
-        const int b = idx >> 10, e = idx & 1023, j = e >> 5, i = e & 31;
-        const int C = b >= 6 ? 3 : b >= 3 ? 2 : b >= 1 ? 1 : 0;
-        const int J = b - C * (C + 1) / 2;
-        const int r = 32 * C + i, c = 32 * J + j;
-        trd_smem[idx] = (r < nbk && c < nbk && r >= c) ? Ad[r + (long long)c * lda] : 0.0;
+    bool staged = true;
+    if constexpr (TMA_DIMS == 0) {
+        const double* Ad = A + k0 + (long long)k0 * lda;
+        for (int idx = threadIdx.x; idx < 10 * 1024; idx += TRD_NT) {
+            const int b = idx >> 10, e = idx & 1023, j = e >> 5, i = e & 31;
+            const int C = b >= 6 ? 3 : b >= 3 ? 2 : b >= 1 ? 1 : 0;
+            const int J = b - C * (C + 1) / 2;
+            const int r = 32 * C + i, c = 32 * J + j;
+            trd_smem[idx] = (r < nbk && c < nbk && r >= c) ? Ad[r + (long long)c * lda] : 0.0;
+        }
+        __syncthreads();
+    } else {
+        if (threadIdx.x == 0) {
+            tc::mbar_init(&l11_bar, 1);
+            tc::mbar_fence_init();
+            tc::prefetch_tmap(&amap);
+            tc::mbar_expect_tx(&l11_bar, 10 * 32 * 32 * 8);
+            for (int C = 0, b = 0; C < 4; ++C)
+                for (int J = 0; J <= C; ++J, ++b) {
+                    if constexpr (TMA_DIMS == 2)
+                        tc::tma_load_2d(trd_smem + b * 1024, &amap, &l11_bar, k0 + 32 * C, k0 + 32 * J);
+                    else
+                        tc::tma_load_3d(trd_smem + b * 1024, &amap, &l11_bar, k0 + 32 * C, k0 + 32 * J,
+                                        (int)blockIdx.y);
+                }
+        }
+        __syncthreads();
+        staged = __syncthreads_and(tc::mbar_wait(&l11_bar, 0, &g_trsm_status, 0x51));
+        if (!staged && threadIdx.x == 0)  // give the copies a second bounded chance to land before the exit
+            (void)tc::mbar_wait(&l11_bar, 0, &g_trsm_status, 0x52);
     }
-    __syncthreads();
     {
         const int t = threadIdx.x, C = t >> 5, i = t & 31;
         rinv[t] = t < nbk ? 1.0 / trd_smem[(C * (C + 1) / 2 + C) * 1024 + i * 32 + i] : 0.0;
@@ -408,6 +441,11 @@ __global__ void __launch_bounds__(TRD_NT) k_trsm_panel_rows_f64(double* __restri
     const long long row = (long long)k0 + nbk + (long long)blockIdx.x * TRD_NT + threadIdx.x;
     const bool live = row < n;
     double* Ar = A + (live ? row : (long long)k0) + (long long)k0 * lda;
+    if (!staged) {  // L11 never arrived: poison the rows (the next diagonal block reports a NaN pivot)
+        if (live)
+            for (int c = 0; c < nbk; ++c) Ar[(long long)c * lda] = __longlong_as_double(0x7ff8000000000000LL);
+        return;
+    }
     const int nch = (nbk + 31) >> 5;
     for (int C = 0; C < nch; ++C) {
         double x[32];
@@ -464,10 +502,19 @@ cudaError_t launch_trsm_panel(T* A, long long lda, int k0, int nbk, int n, const
     if constexpr (std::is_same<T, double>::value && !UP) {
         const long long m = (long long)n - k0 - nbk;
         if (m <= 0) return cudaSuccess;
-        if (cudaError_t e = smem_optin(k_trsm_panel_rows_f64, TRD_SMEM); e != cudaSuccess) return e;
         const double md = (double)m, b = nbk;
         ProfScope ps(PK_TRSM_PANEL, s, md * b * b, sizeof(T) * (2.0 * md * b + b * (b + 1) / 2));
-        k_trsm_panel_rows_f64<<<(unsigned)ceil_div(m, TRD_NT), TRD_NT, TRD_SMEM, s>>>(A, lda, 0, k0, nbk, n, dinfo);
+        const unsigned grid = (unsigned)ceil_div(m, TRD_NT);
+        CUtensorMap amap{};
+        if (nbk == 128 && !(lda & 1) &&
+            tc::encode_colmajor_2d(&amap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, A, n, n, lda, 32, 32,
+                                   CU_TENSOR_MAP_SWIZZLE_NONE)) {
+            if (cudaError_t e = smem_optin(k_trsm_panel_rows_f64<2>, TRD_SMEM); e != cudaSuccess) return e;
+            k_trsm_panel_rows_f64<2><<<grid, TRD_NT, TRD_SMEM, s>>>(amap, A, lda, 0, k0, nbk, n, dinfo);
+        } else {
+            if (cudaError_t e = smem_optin(k_trsm_panel_rows_f64<0>, TRD_SMEM); e != cudaSuccess) return e;
+            k_trsm_panel_rows_f64<0><<<grid, TRD_NT, TRD_SMEM, s>>>(amap, A, lda, 0, k0, nbk, n, dinfo);
+        }
         note_launches(1);
         return cudaGetLastError();
     }
@@ -733,7 +780,12 @@ extern "C" int ddlak_potrf_batched_f64(int batch, int n, void* A_, long long lda
     constexpr int NB = 128, G = 2;
     const size_t diag_smem = (size_t)NB * diag_block_ld<double>(NB) * sizeof(double);
     if ((e = smem_optin(k_potrf_diag<double, false>, diag_smem)) != cudaSuccess) return (int)e;
-    if ((e = smem_optin(k_trsm_panel_rows_f64, TRD_SMEM)) != cudaSuccess) return (int)e;
+    if ((e = smem_optin(k_trsm_panel_rows_f64<3>, TRD_SMEM)) != cudaSuccess) return (int)e;
+    if ((e = smem_optin(k_trsm_panel_rows_f64<0>, TRD_SMEM)) != cudaSuccess) return (int)e;
+    // L11 of every matrix by TMA boxes of 32 x 32 (lda and astride even, A 16-byte aligned: checked above)
+    CUtensorMap amap{};
+    const bool tma = tc::encode_colmajor_3d(&amap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, A, n, n, lda, batch, astride,
+                                            32, 32);
     const double nb3 = (double)batch;
     auto diag_and_panel = [&](int k0) -> cudaError_t {
         const int nbk = n - k0 < NB ? n - k0 : NB;
@@ -748,8 +800,11 @@ extern "C" int ddlak_potrf_batched_f64(int batch, int n, void* A_, long long lda
         if (m > 0) {
             const double md = (double)m;
             ProfScope ps(PK_TRSM_PANEL, st, nb3 * md * b * b, nb3 * 8.0 * (2.0 * md * b + b * (b + 1) / 2));
-            k_trsm_panel_rows_f64<<<dim3((unsigned)ceil_div(m, TRD_NT), (unsigned)batch), TRD_NT, TRD_SMEM, st>>>(
-                A, lda, astride, k0, nbk, n, dinfo);
+            const dim3 grid((unsigned)ceil_div(m, TRD_NT), (unsigned)batch);
+            if (tma && nbk == 128)
+                k_trsm_panel_rows_f64<3><<<grid, TRD_NT, TRD_SMEM, st>>>(amap, A, lda, astride, k0, nbk, n, dinfo);
+            else
+                k_trsm_panel_rows_f64<0><<<grid, TRD_NT, TRD_SMEM, st>>>(amap, A, lda, astride, k0, nbk, n, dinfo);
             note_launches(1);
         }
         return cudaGetLastError();
