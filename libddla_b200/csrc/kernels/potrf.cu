@@ -290,32 +290,58 @@ __device__ __forceinline__ void trr_solve64(float (&x)[64], const float* l11, co
     }
 }
 
-__global__ void __launch_bounds__(TRR_NT) k_trsm_panel_rows(float* __restrict__ A, long long lda, int k0, int nbk,
+__device__ int g_trsm_status;  // a TMA wait that gave up (never expected): the panel is NaN-poisoned
+
+// TMA: L11 staged by one 128 x 128 TMA box (nbk = 128; the solve reads only entries
+// below the diagonal, so the block's upper half comes in unmasked); otherwise by loads.
+template <bool TMA>
+__global__ void __launch_bounds__(TRR_NT) k_trsm_panel_rows(const __grid_constant__ CUtensorMap amap,
+                                                            float* __restrict__ A, long long lda, int k0, int nbk,
                                                             int n, const int* __restrict__ info)
 {
-    extern __shared__ __align__(16) float trr_smem[];
-    float* l11 = trr_smem;               // l11[j * 128 + k] = L(k0 + k, k0 + j), zero for k < j or k >= nbk
+    extern __shared__ __align__(128) float trr_smem[];
+    float* l11 = trr_smem;               // l11[j * 128 + k] = L(k0 + k, k0 + j) (zero for k < j or k >= nbk by loads)
     float* xs = trr_smem + 128 * 128;    // xs[j * TRR_NT + t]: thread t's solved first half
     __shared__ float rinv[128];
+    __shared__ __align__(8) uint64_t l11_bar;
     if (*(volatile const int*)info != 0) return;
-    const float* Ad = A + k0 + (long long)k0 * lda;
-    for (int idx = threadIdx.x; idx < 128 * 32; idx += TRR_NT) {
-        const int j = idx >> 5, k4 = (idx & 31) * 4;
-        float v[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int k = k4 + e;
-            v[e] = (j < nbk && k < nbk && k >= j) ? Ad[k + (long long)j * lda] : 0.f;
+    bool staged = true;
+    if constexpr (TMA) {
+        if (threadIdx.x == 0) {
+            tc::mbar_init(&l11_bar, 1);
+            tc::mbar_fence_init();
+            tc::prefetch_tmap(&amap);
+            tc::mbar_expect_tx(&l11_bar, 128 * 128 * 4);
+            tc::tma_load_2d(l11, &amap, &l11_bar, k0, k0);
         }
-        *reinterpret_cast<float4*>(&l11[j * 128 + k4]) = make_float4(v[0], v[1], v[2], v[3]);
+        __syncthreads();
+        staged = __syncthreads_and(tc::mbar_wait(&l11_bar, 0, &g_trsm_status, 0x53));
+        if (!staged && threadIdx.x == 0) (void)tc::mbar_wait(&l11_bar, 0, &g_trsm_status, 0x54);
+    } else {
+        const float* Ad = A + k0 + (long long)k0 * lda;
+        for (int idx = threadIdx.x; idx < 128 * 32; idx += TRR_NT) {
+            const int j = idx >> 5, k4 = (idx & 31) * 4;
+            float v[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int k = k4 + e;
+                v[e] = (j < nbk && k < nbk && k >= j) ? Ad[k + (long long)j * lda] : 0.f;
+            }
+            *reinterpret_cast<float4*>(&l11[j * 128 + k4]) = make_float4(v[0], v[1], v[2], v[3]);
+        }
+        __syncthreads();
     }
-    __syncthreads();
     rinv[threadIdx.x] = threadIdx.x < nbk ? 1.f / l11[threadIdx.x * 129] : 0.f;
     __syncthreads();
     const int t = threadIdx.x;
     const long long row = (long long)k0 + nbk + (long long)blockIdx.x * TRR_NT + t;
     const bool live = row < n;
     float* Ar = A + (live ? row : (long long)k0) + (long long)k0 * lda;
+    if (!staged) {  // L11 never arrived: poison the rows (the next diagonal block reports a NaN pivot)
+        if (live)
+            for (int c = 0; c < nbk; ++c) Ar[(long long)c * lda] = __int_as_float(0x7fc00000);
+        return;
+    }
     float x[64];
 #pragma unroll
     for (int c = 0; c < 64; ++c) x[c] = (live && c < nbk) ? Ar[(long long)c * lda] : 0.f;
@@ -386,7 +412,6 @@ __device__ __forceinline__ double2 ld_shared_d2(const double2* p)
 // boxes from a 2-D map over A; 3 = the same from a 3-D map over a batch (z = matrix).
 // The TMA forms need nbk = 128: they load whole boxes, so the diagonal blocks'
 // upper halves come in unmasked (the solve reads only entries below the diagonal).
-__device__ int g_trsm_status;  // a TMA wait that gave up (never expected): the panel is NaN-poisoned
 
 template <int TMA_DIMS>
 __global__ void __launch_bounds__(TRD_NT) k_trsm_panel_rows_f64(const __grid_constant__ CUtensorMap amap,
@@ -492,10 +517,19 @@ cudaError_t launch_trsm_panel(T* A, long long lda, int k0, int nbk, int n, const
     if constexpr (std::is_same<T, float>::value && !UP) {
         const long long m = (long long)n - k0 - nbk;
         if (m <= 0) return cudaSuccess;
-        if (cudaError_t e = smem_optin(k_trsm_panel_rows, TRR_SMEM); e != cudaSuccess) return e;
         const double md = (double)m, b = nbk;
         ProfScope ps(PK_TRSM_PANEL, s, md * b * b, sizeof(T) * (2.0 * md * b + b * (b + 1) / 2));
-        k_trsm_panel_rows<<<(unsigned)ceil_div(m, TRR_NT), TRR_NT, TRR_SMEM, s>>>(A, lda, k0, nbk, n, dinfo);
+        const unsigned grid = (unsigned)ceil_div(m, TRR_NT);
+        CUtensorMap amap{};
+        if (nbk == 128 && (lda % 4) == 0 &&
+            tc::encode_colmajor_2d(&amap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, A, n, n, lda, 128, 128,
+                                   CU_TENSOR_MAP_SWIZZLE_NONE)) {
+            if (cudaError_t e = smem_optin(k_trsm_panel_rows<true>, TRR_SMEM); e != cudaSuccess) return e;
+            k_trsm_panel_rows<true><<<grid, TRR_NT, TRR_SMEM, s>>>(amap, A, lda, k0, nbk, n, dinfo);
+        } else {
+            if (cudaError_t e = smem_optin(k_trsm_panel_rows<false>, TRR_SMEM); e != cudaSuccess) return e;
+            k_trsm_panel_rows<false><<<grid, TRR_NT, TRR_SMEM, s>>>(amap, A, lda, k0, nbk, n, dinfo);
+        }
         note_launches(1);
         return cudaGetLastError();
     }
