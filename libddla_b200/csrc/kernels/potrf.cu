@@ -342,45 +342,46 @@ __global__ void __launch_bounds__(TRR_NT) k_trsm_panel_rows(const __grid_constan
             for (int c = 0; c < nbk; ++c) Ar[(long long)c * lda] = __int_as_float(0x7fc00000);
         return;
     }
-    float x[64];
+    // the two 64-column halves through one rolled loop, so that the unrolled solve exists once
+    // in the instruction stream (the kernel is bound by instruction fetch, not arithmetic)
+#pragma unroll 1
+    for (int half = 0; half < 2; ++half) {
+        const int c0 = 64 * half;
+        if (c0 >= nbk) break;  // uniform
+        float x[64];
+        {
+            const float* p = Ar + (long long)c0 * lda;
 #pragma unroll
-    for (int c = 0; c < 64; ++c) x[c] = (live && c < nbk) ? Ar[(long long)c * lda] : 0.f;
-    trr_solve64(x, l11, rinv, 0);
-    {
-        // the row's addresses are recomputed here rather than kept live through the solve
-        float* p = Ar;
-        long long ld = lda;
-        asm volatile("" : "+l"(p), "+l"(ld));
-#pragma unroll
-        for (int c = 0; c < 64; ++c) {
-            if (live && c < nbk) p[(long long)c * ld] = x[c];
-            xs[c * TRR_NT + t] = x[c];
+            for (int c = 0; c < 64; ++c) x[c] = (live && c0 + c < nbk) ? p[(long long)c * lda] : 0.f;
         }
-    }
-    if (nbk <= 64) return;  // uniform: no barrier follows
-#pragma unroll
-    for (int c = 0; c < 64; ++c) x[c] = (live && 64 + c < nbk) ? Ar[(long long)(64 + c) * lda] : 0.f;
+        if (half == 1) {
+            // x -= x1 L11[64:128, 0:64]^T, x1 = this thread's solved first half
 #pragma unroll 4
-    for (int j = 0; j < 64; ++j) {
-        const float xj = xs[j * TRR_NT + t];
-        const float4* col = reinterpret_cast<const float4*>(&l11[j * 128 + 64]);
+            for (int j = 0; j < 64; ++j) {
+                const float xj = xs[j * TRR_NT + t];
+                const float4* col = reinterpret_cast<const float4*>(&l11[j * 128 + 64]);
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            const float4 l = ld_shared_f4(col + q);
-            x[4 * q + 0] = fmaf(-xj, l.x, x[4 * q + 0]);
-            x[4 * q + 1] = fmaf(-xj, l.y, x[4 * q + 1]);
-            x[4 * q + 2] = fmaf(-xj, l.z, x[4 * q + 2]);
-            x[4 * q + 3] = fmaf(-xj, l.w, x[4 * q + 3]);
+                for (int q = 0; q < 16; ++q) {
+                    const float4 l = ld_shared_f4(col + q);
+                    x[4 * q + 0] = fmaf(-xj, l.x, x[4 * q + 0]);
+                    x[4 * q + 1] = fmaf(-xj, l.y, x[4 * q + 1]);
+                    x[4 * q + 2] = fmaf(-xj, l.z, x[4 * q + 2]);
+                    x[4 * q + 3] = fmaf(-xj, l.w, x[4 * q + 3]);
+                }
+            }
         }
-    }
-    trr_solve64(x, l11, rinv, 64);
-    {
-        float* p = Ar;
-        long long ld = lda;
-        asm volatile("" : "+l"(p), "+l"(ld));
+        trr_solve64(x, l11, rinv, c0);
+        {
+            // the row's addresses are recomputed here rather than kept live through the solve
+            float* p = Ar + (long long)c0 * lda;
+            long long ld = lda;
+            asm volatile("" : "+l"(p), "+l"(ld));
 #pragma unroll
-        for (int c = 0; c < 64; ++c)
-            if (live && 64 + c < nbk) p[(long long)(64 + c) * ld] = x[c];
+            for (int c = 0; c < 64; ++c) {
+                if (live && c0 + c < nbk) p[(long long)c * ld] = x[c];
+                if (half == 0) xs[c * TRR_NT + t] = x[c];
+            }
+        }
     }
 }
 
