@@ -279,6 +279,20 @@ __host__ __device__ constexpr int diag_block_ld(int nbk)
 // longer waits for the whole trailing update.  Every entry receives the same
 // operations as in the unpipelined order, so the factor is unchanged.  Full
 // panels take the compile-time-width forms of the chain and the row solve.
+// The partial-panel forms (a block whose order is not a multiple of 32: only the last
+// block of a factorization) out of line, so that the full-panel code the kernel runs
+// for every other block stays compact in the instruction cache.
+static __device__ __noinline__ void panel_diag_f64_partial(double* s, int ld, int c0, int w, int lane,
+                                                    double (*colbuf)[diagf::PW], double* s_inv, double* s_rs,
+                                                    int* s_fail)
+{
+    diagf::panel_diag<double>(s, ld, c0, w, lane, colbuf, s_inv, s_rs, s_fail);
+}
+static __device__ __noinline__ void panel_row_f64_partial(double* s, int ld, int c0, int r, int jd, const double* s_rs)
+{
+    diagf::panel_row_f64(s, ld, c0, r, jd, s_rs);
+}
+
 __device__ __forceinline__ int factor_block_smem_f64(double* s, int ld, int nbk)
 {
     using namespace diagf;
@@ -291,7 +305,7 @@ __device__ __forceinline__ int factor_block_smem_f64(double* s, int ld, int nbk)
     __syncthreads();
     auto chain = [&](int c, int w) {  // warp 0
         if (w == PW) panel_diag<double, PW>(s, ld, c, PW, lane, colbuf, s_inv, s_rs, &s_fail);
-        else panel_diag<double>(s, ld, c, w, lane, colbuf, s_inv, s_rs, &s_fail);
+        else panel_diag_f64_partial(s, ld, c, w, lane, colbuf, s_inv, s_rs, &s_fail);
     };
     if (warp == 0) chain(0, nbk < PW ? nbk : PW);
     __syncthreads();
@@ -303,7 +317,7 @@ __device__ __forceinline__ int factor_block_smem_f64(double* s, int ld, int nbk)
         if (jd == PW) {
             for (int r = c1 + t; r < nbk; r += blockDim.x) panel_row_f64<PW>(s, ld, c0, r, PW, s_rs);
         } else {
-            for (int r = c1 + t; r < nbk; r += blockDim.x) panel_row_f64(s, ld, c0, r, jd, s_rs);
+            for (int r = c1 + t; r < nbk; r += blockDim.x) panel_row_f64_partial(s, ld, c0, r, jd, s_rs);
         }
         __syncthreads();
         if (fail || c1 >= nbk) break;
