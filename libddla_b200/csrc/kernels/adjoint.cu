@@ -437,7 +437,7 @@ int gp_build_t(int batch, int n, int d, const void* X, long long xstride, const 
 
 // ---------------------------------------------------------------------------
 // Recursive FP64 inversion, bottom-up: the 64 x 64 diagonal blocks by
-// k_trtri_batched, then for h = 64, 128, ... each pair of inverted h-blocks
+// k_trtri_leaf64, then for h = 64, 128, ... each pair of inverted h-blocks
 // (o = 2 p h) is joined by
 //   W21 = -W22 (L21 W11),  L21 = L(o+h.., o..), W11 = W(o.., o..), W22 = W(o+h.., o+h..),
 // two batched products on the FP64 tensor cores (mma.sync m16n8k4):
@@ -566,20 +566,51 @@ __global__ void __launch_bounds__(128) k_trtri_level(int n, int h, const double*
             }
 }
 
+// The recursion's 64 x 64 leaves, four per CTA: thread j of a leaf's 64 computes
+// column j of its inverse by substitution, w_j = 1 / l_jj and
+// w_i = -(sum_{j <= k < i} l_ik w_k) / l_ii, with the column in registers and L
+// read through the L1 cache (the 64 threads of a leaf read the same entry at each
+// step).  Leaf g = blockIdx.x * 4 + threadIdx.x / 64 is block sub = g % nsub of
+// matrix g / nsub; its order is 64, or `last` for the final block of a matrix
+// whose order is not a multiple of 64.
+constexpr int TLF = 64;
+__global__ void __launch_bounds__(256) k_trtri_leaf64(long long nleaf, int nsub, int n, const double* __restrict__ Lg,
+                                                      long long ldl, long long lstride, double* __restrict__ Wg,
+                                                      long long ldw, long long wstride)
+{
+    const long long g = (long long)blockIdx.x * 4 + (threadIdx.x >> 6);
+    if (g >= nleaf) return;
+    const long long m = g / nsub;
+    const int sub = (int)(g % nsub);
+    const int o = sub * TLF, nb = n - o < TLF ? n - o : TLF;
+    const int j = threadIdx.x & 63;
+    const double* L = Lg + m * lstride + o + (long long)o * ldl;
+    double* W = Wg + m * wstride + o + (long long)o * ldw;
+    double w[TLF];
+#pragma unroll
+    for (int i = 0; i < TLF; ++i) {
+        double acc = 0.0;
+        const bool row = i < nb;
+#pragma unroll
+        for (int k = 0; k < i; ++k)
+            if (row && k >= j) acc = fma(__ldg(&L[i + (long long)k * ldl]), w[k], acc);
+        const double lii = row ? __ldg(&L[i + (long long)i * ldl]) : 1.0;
+        w[i] = (i < j || !row) ? 0.0 : (i == j ? 1.0 / lii : -acc / lii);
+    }
+    if (j < nb)
+#pragma unroll
+        for (int i = 0; i < TLF; ++i)
+            if (i >= j && i < nb) W[i + (long long)j * ldw] = w[i];
+}
+
 int trtri_recursive_f64(int batch, int n, const double* L, long long ldl, long long lstride, double* W, long long ldw,
                         long long wstride, cudaStream_t st)
 {
-    constexpr int LEAF = 64;
-    const int full = n / LEAF, last = n - full * LEAF;
-    if (full > 0) {
-        k_trtri_batched<double><<<dim3((unsigned)((long long)batch * full), 1), TR_NT, 0, st>>>(
-            LEAF, L, ldl, lstride, W, ldw, wstride, full, LEAF * (ldl + 1), LEAF * (ldw + 1));
-        note_launches(1);
-    }
-    if (last > 0) {
-        const long long off_l = (long long)full * LEAF * (ldl + 1), off_w = (long long)full * LEAF * (ldw + 1);
-        k_trtri_batched<double><<<dim3((unsigned)batch, 1), TR_NT, 0, st>>>(last, L + off_l, ldl, lstride, W + off_w,
-                                                                            ldw, wstride, 1, 0, 0);
+    constexpr int LEAF = TLF;
+    {
+        const int nsub = (n + LEAF - 1) / LEAF;
+        const long long nleaf = (long long)batch * nsub;
+        k_trtri_leaf64<<<(unsigned)((nleaf + 3) / 4), 256, 0, st>>>(nleaf, nsub, n, L, ldl, lstride, W, ldw, wstride);
         note_launches(1);
     }
     if (cudaError_t e = cudaGetLastError(); e != cudaSuccess) return (int)e;
