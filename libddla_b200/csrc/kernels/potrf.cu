@@ -793,12 +793,16 @@ __global__ void __launch_bounds__(PB_NT) k_potrs_batched_f64(int n, const double
 }
 
 // A batch of equal-order FP64 matrices (lower), right-looking by super-steps of
-// two block columns of 128, each step one launch per kernel over the whole
-// batch: the diagonal blocks (one CTA per matrix), the panels (row-per-thread
-// solve, grid.y = matrix) and the updates (TMA DMMA tiles, grid.y = matrix).
-// In a super-step, block column 1 first takes block column 0's update of its own
-// 128 columns, and the rest of the trailing matrix is updated once with K = 256,
-// so the trailing matrix is read and written once per 256 columns.
+// G block columns of 128, each step one launch per kernel over the whole batch:
+// the diagonal blocks (one CTA per matrix), the panels (row-per-thread solve,
+// grid.y = matrix) and the updates (TMA DMMA tiles, grid.y = matrix).  In a
+// super-step, block column g first takes the update of its own 128 columns by
+// block columns 0 .. g-1 (K = 128 g), and the rest of the trailing matrix is
+// updated once with K = 128 G, so the trailing matrix is read and written once
+// per 128 G columns and the update tiles run long K.
+#ifndef BATCHED_POTRF_GROUP
+#define BATCHED_POTRF_GROUP 4
+#endif
 extern "C" int ddlak_potrf_batched_f64(int batch, int n, void* A_, long long lda, long long astride, int* dinfo,
                                        void* stream)
 {
@@ -812,7 +816,7 @@ extern "C" int ddlak_potrf_batched_f64(int batch, int n, void* A_, long long lda
         return (int)cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(dinfo, 0, sizeof(int) * (size_t)batch, st);
     if (e != cudaSuccess || n == 0) return (int)e;
-    constexpr int NB = 128, G = 2;
+    constexpr int NB = 128, G = BATCHED_POTRF_GROUP;
     const size_t diag_smem = (size_t)NB * diag_block_ld<double>(NB) * sizeof(double);
     if ((e = smem_optin(k_potrf_diag<double, false>, diag_smem)) != cudaSuccess) return (int)e;
     if ((e = smem_optin(k_trsm_panel_rows_f64<3>, TRD_SMEM)) != cudaSuccess) return (int)e;
@@ -858,12 +862,15 @@ extern "C" int ddlak_potrf_batched_f64(int batch, int n, void* A_, long long lda
     };
     for (int k0 = 0; k0 < n; k0 += G * NB) {
         if ((e = diag_and_panel(k0)) != cudaSuccess) return (int)e;
-        const int k1 = k0 + NB;
-        if (k1 >= n) break;
-        // block column 1 of the super-step: block column 0's update of its own columns, then its factor
-        const int c1 = n - k1 < NB ? n - k1 : NB;
-        if ((e = update(k0, NB, k1, c1)) != cudaSuccess) return (int)e;
-        if ((e = diag_and_panel(k1)) != cudaSuccess) return (int)e;
+        // block column g of the super-step: the update of its own columns by block columns
+        // 0 .. g-1 of the super-step (left-looking, K = 128 g), then its factor
+        for (int g = 1; g < G; ++g) {
+            const int kg = k0 + g * NB;
+            if (kg >= n) break;
+            const int cg = n - kg < NB ? n - kg : NB;
+            if ((e = update(k0, g * NB, kg, cg)) != cudaSuccess) return (int)e;
+            if ((e = diag_and_panel(kg)) != cudaSuccess) return (int)e;
+        }
         const long long t0 = (long long)k0 + G * NB;
         if (t0 >= n) break;
         if ((e = update(k0, G * NB, t0, 0)) != cudaSuccess) return (int)e;
