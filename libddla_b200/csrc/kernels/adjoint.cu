@@ -660,48 +660,79 @@ int trtri_t(int batch, int n, const void* L, long long ldl, long long lstride, v
 // tile's result is NaN (the gradient comes back NaN) after a bounded wait for
 // the copies still in flight.
 // ---------------------------------------------------------------------------
-constexpr int AD_BK = 32, AD_LDK = 36, AD_NS = 3;
+constexpr int AD_BK = 32, AD_LDK = 36;
 constexpr int AD_BOX = CT_TILE * AD_LDK;
 constexpr unsigned AD_BOX_BYTES = AD_BOX * 8u;  // 36864
-constexpr size_t AD_SMEM = (size_t)AD_NS * 2 * AD_BOX_BYTES + 128;
+// TNC: the tile's column count.  128: 128 x 128 tiles, 8 warps, 3 stages, one CTA per SM
+// (registers); 64: 128 x 64 tiles, 4 warps, 2 stages, two CTAs per SM, so that one CTA's
+// prologue and epilogue run under the other's MMAs.  The warp tile is 64 x 32 in both.
+#ifndef AD_CONTRACT_TNC
+#define AD_CONTRACT_TNC 64
+#endif
+template <int TNC> struct AdShape {
+    static constexpr int NT = 2 * TNC, NS = TNC == 128 ? 3 : 2, WN = TNC / 32;
+    static constexpr int BOXJ = TNC * AD_LDK;
+    static constexpr unsigned STAGE_BYTES = (unsigned)(AD_BOX + BOXJ) * 8u;
+    static constexpr size_t SMEM = (size_t)NS * STAGE_BYTES + 128;
+};
+
+// tile t of the lower part, 128 x TNC tiles: (ti, tj) with tj <= ti (TNC = 128) or
+// tj <= 2 ti + 1 (TNC = 64, row ti holding 2 ti + 2 tiles)
+template <int TNC>
+__device__ __forceinline__ void ad_tile(int t, int& ti, int& tj)
+{
+    if constexpr (TNC == 128) {
+        tile_of_lower(t, ti, tj);
+    } else {
+        int i = (int)((sqrtf(4.f * t + 1.f) - 1.f) * 0.5f);
+        while ((i + 1) * (i + 2) <= t) ++i;
+        while (i > 0 && i * (i + 1) > t) --i;
+        ti = i;
+        tj = t - i * (i + 1);
+    }
+}
 
 __device__ int g_adjoint_status;
 
-template <int MODE>
-__global__ void __launch_bounds__(CT_NT, 1)
-    k_adjoint_contract_dmma(const __grid_constant__ CUtensorMap wmap, int n, const double* __restrict__ alpha_g,
+template <int MODE, int TNC>
+__global__ void __launch_bounds__(AdShape<TNC>::NT, TNC == 128 ? 1 : 2)
+    k_adjoint_contract_dmma(const __grid_constant__ CUtensorMap wmap, const __grid_constant__ CUtensorMap wmapj,
+                            int n, const double* __restrict__ alpha_g,
                             long long astride, const double* __restrict__ X, int d, long long xstride,
                             const double* __restrict__ theta, int tstride, double* __restrict__ partial,
                             double* __restrict__ G, long long ldg, long long gstride)
 {
+    using SH = AdShape<TNC>;
+    constexpr int AD_NS = SH::NS, NW = SH::NT / 32;
     extern __shared__ __align__(128) unsigned char ad_raw[];
     __shared__ __align__(8) uint64_t full[AD_NS], empty[AD_NS];
-    __shared__ double red[3][CT_NT / 32];
+    __shared__ double red[3][NW];
     // blockIdx.x = matrix, blockIdx.y = tile: the grid runs every matrix's longest tiles
     // (smallest i0, the most k) first
     const int m = blockIdx.x, tile = blockIdx.y;
     int ti, tj;
-    tile_of_lower(tile, ti, tj);
-    const int i0 = ti * CT_TILE, j0 = tj * CT_TILE;
+    ad_tile<TNC>(tile, ti, tj);
+    const int i0 = ti * CT_TILE, j0 = tj * TNC;
     double* sm = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(ad_raw) + 127) & ~uintptr_t(127));
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-    const int wm = warp >> 2, wn = warp & 3;
+    const int wm = warp / SH::WN, wn = warp % SH::WN;
     const int g = lane >> 2, q = lane & 3;
     const int kbeg = i0, nch = (n - kbeg + AD_BK - 1) / AD_BK;
     auto issue = [&](int c) {
         const int s = c % AD_NS;
-        double* st = sm + (size_t)s * 2 * AD_BOX;
-        tc::mbar_expect_tx(&full[s], 2 * AD_BOX_BYTES);
+        double* st = sm + (size_t)s * (AD_BOX + SH::BOXJ);
+        tc::mbar_expect_tx(&full[s], SH::STAGE_BYTES);
         tc::tma_load_3d(st, &wmap, &full[s], kbeg + c * AD_BK, i0, m);
-        tc::tma_load_3d(st + AD_BOX, &wmap, &full[s], kbeg + c * AD_BK, j0, m);
+        tc::tma_load_3d(st + AD_BOX, &wmapj, &full[s], kbeg + c * AD_BK, j0, m);
     };
     if (t == 0) {
         for (int s = 0; s < AD_NS; ++s) {
             tc::mbar_init(&full[s], 1);
-            tc::mbar_init(&empty[s], CT_NT / 32);  // one arrival per warp
+            tc::mbar_init(&empty[s], NW);  // one arrival per warp
         }
         tc::mbar_fence_init();
         tc::prefetch_tmap(&wmap);
+        tc::prefetch_tmap(&wmapj);
         for (int c = 0; c < AD_NS && c < nch; ++c) issue(c);
     }
     __syncthreads();
@@ -719,33 +750,50 @@ __global__ void __launch_bounds__(CT_NT, 1)
             break;
         }
         consumed = c + 1;
-        const double* Wi = sm + (size_t)s * 2 * AD_BOX;
+        const double* Wi = sm + (size_t)s * (AD_BOX + SH::BOXJ);
         const double* Wj = Wi + AD_BOX;
         const int k0 = kbeg + c * AD_BK;
         // W(k, col) = 0 for k < col (the strictly upper triangle, which the inversion
         // leaves unspecified): applied to the fragments of the chunks that reach it
-        const bool mask_i = k0 < i0 + CT_TILE, mask_j = mask_i && ti == tj;
+        const bool mask_i = k0 < i0 + CT_TILE, mask_j = k0 < j0 + TNC;
+        if (mask_i || mask_j) {
 #pragma unroll
-        for (int kk = 0; kk < AD_BK; kk += 4) {
-            const int k = k0 + kk + q;
-            double af[8], bf[4];
+            for (int kk = 0; kk < AD_BK; kk += 4) {
+                const int k = k0 + kk + q;
+                double af[8], bf[4];
 #pragma unroll
-            for (int a = 0; a < 8; ++a) {
-                const int cl = wm * 64 + a * 8 + g;
-                const double v = Wi[cl * AD_LDK + kk + q];
-                af[a] = (mask_i && k < i0 + cl) ? 0.0 : v;
+                for (int a = 0; a < 8; ++a) {
+                    const int cl = wm * 64 + a * 8 + g;
+                    const double v = Wi[cl * AD_LDK + kk + q];
+                    af[a] = (mask_i && k < i0 + cl) ? 0.0 : v;
+                }
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const int cl = wn * 32 + b * 8 + g;
+                    const double v = Wj[cl * AD_LDK + kk + q];
+                    bf[b] = (mask_j && k < j0 + cl) ? 0.0 : v;
+                }
+                // rows a*8+g and (a+1)*8+g as one m16n8k4 product: the same accumulators as two m8n8k4
+#pragma unroll
+                for (int a = 0; a < 8; a += 2)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) tl_mma(acc[a][b], acc[a + 1][b], af[a], af[a + 1], bf[b]);
             }
+        } else {
+            // the chunks clear of the triangle (all but the first few of a tile): the fragments
+            // go from shared memory straight into the MMAs
 #pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const int cl = wn * 32 + b * 8 + g;
-                const double v = Wj[cl * AD_LDK + kk + q];
-                bf[b] = (mask_j && k < j0 + cl) ? 0.0 : v;
+            for (int kk = 0; kk < AD_BK; kk += 4) {
+                double af[8], bf[4];
+#pragma unroll
+                for (int a = 0; a < 8; ++a) af[a] = Wi[(wm * 64 + a * 8 + g) * AD_LDK + kk + q];
+#pragma unroll
+                for (int b = 0; b < 4; ++b) bf[b] = Wj[(wn * 32 + b * 8 + g) * AD_LDK + kk + q];
+#pragma unroll
+                for (int a = 0; a < 8; a += 2)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) tl_mma(acc[a][b], acc[a + 1][b], af[a], af[a + 1], bf[b]);
             }
-            // rows a*8+g and (a+1)*8+g as one m16n8k4 product: the same accumulators as two m8n8k4
-#pragma unroll
-            for (int a = 0; a < 8; a += 2)
-#pragma unroll
-                for (int b = 0; b < 4; ++b) tl_mma(acc[a][b], acc[a + 1][b], af[a], af[a + 1], bf[b]);
         }
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(&empty[s]);  // this warp is done with stage s
@@ -794,7 +842,7 @@ __global__ void __launch_bounds__(CT_NT, 1)
         // the tile into shared memory (the operand stages are free: every chunk was consumed and
         // the barrier above passed), then one rolled loop over its entries, so that the
         // exponential's code is not replicated for every fragment entry
-        constexpr int CLD = CT_TILE + 1;
+        constexpr int CLD = TNC + 1;
         double* cs = sm;
 #pragma unroll
         for (int a = 0; a < 8; ++a)
@@ -810,8 +858,8 @@ __global__ void __launch_bounds__(CT_NT, 1)
         const double* x = X + m * xstride;
         double g0 = 0.0, g1 = 0.0, g2 = 0.0;
 #pragma unroll 1
-        for (int e = t; e < CT_TILE * CT_TILE; e += CT_NT) {
-            const int il = e / CT_TILE, jl = e % CT_TILE;
+        for (int e = t; e < CT_TILE * TNC; e += SH::NT) {
+            const int il = e / TNC, jl = e % TNC;
             const int i = i0 + il, j = j0 + jl;
             if (i >= n || j > i) continue;
             const double ab = 0.5 * (cs[il * CLD + jl] - al[i] * al[j]);
@@ -840,7 +888,7 @@ __global__ void __launch_bounds__(CT_NT, 1)
         __syncthreads();
         if (t < 3) {
             double sum = 0.0;
-            for (int w = 0; w < CT_NT / 32; ++w) sum += red[t][w];
+            for (int w = 0; w < NW; ++w) sum += red[t][w];
             partial[((long long)m * gridDim.y + tile) * 3 + t] = sum;
         }
     }
@@ -853,24 +901,28 @@ bool contract_dmma(int mode, int batch, int n, const double* W, long long ldw, l
                    double* partial, double* grad, double* G, long long ldg, long long gstride, cudaStream_t st,
                    cudaError_t* err)
 {
-    CUtensorMap wmap;
+    constexpr int TNC = AD_CONTRACT_TNC;
+    using SH = AdShape<TNC>;
+    CUtensorMap wmap, wmapj;
     if (!tc::encode_colmajor_3d(&wmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, W, n, n, ldw, batch, wstride, AD_LDK,
-                                CT_TILE))
+                                CT_TILE) ||
+        !tc::encode_colmajor_3d(&wmapj, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, W, n, n, ldw, batch, wstride, AD_LDK,
+                                TNC))
         return false;
     const int nt = (n + CT_TILE - 1) / CT_TILE;
-    const int ntiles = nt * (nt + 1) / 2;
+    const int ntiles = TNC == 64 ? nt * (nt + 1) : nt * (nt + 1) / 2;  // 64 columns: row ti holds 2 ti + 2 tiles
     if (ntiles > 65535) return false;
     dim3 grid(batch, ntiles);
     if (mode == 0) {
-        if ((*err = smem_optin(k_adjoint_contract_dmma<0>, AD_SMEM)) != cudaSuccess) return true;
-        k_adjoint_contract_dmma<0><<<grid, CT_NT, AD_SMEM, st>>>(wmap, n, alpha, astride, X, d, xstride, theta,
-                                                                 tstride, partial, nullptr, 0, 0);
+        if ((*err = smem_optin(k_adjoint_contract_dmma<0, TNC>, SH::SMEM)) != cudaSuccess) return true;
+        k_adjoint_contract_dmma<0, TNC><<<grid, SH::NT, SH::SMEM, st>>>(wmap, wmapj, n, alpha, astride, X, d, xstride,
+                                                                        theta, tstride, partial, nullptr, 0, 0);
         k_adjoint_reduce<<<batch, 32, 0, st>>>(ntiles, partial, grad);
         note_launches(2);
     } else {
-        if ((*err = smem_optin(k_adjoint_contract_dmma<1>, AD_SMEM)) != cudaSuccess) return true;
-        k_adjoint_contract_dmma<1><<<grid, CT_NT, AD_SMEM, st>>>(wmap, n, alpha, astride, nullptr, 0, 0, nullptr, 0,
-                                                                 nullptr, G, ldg, gstride);
+        if ((*err = smem_optin(k_adjoint_contract_dmma<1, TNC>, SH::SMEM)) != cudaSuccess) return true;
+        k_adjoint_contract_dmma<1, TNC><<<grid, SH::NT, SH::SMEM, st>>>(wmap, wmapj, n, alpha, astride, nullptr, 0, 0,
+                                                                        nullptr, 0, nullptr, G, ldg, gstride);
         note_launches(1);
     }
     *err = cudaGetLastError();
@@ -941,8 +993,10 @@ extern "C" int ddlak_trtri_batched(char type, int batch, int n, const void* L, l
 
 extern "C" unsigned long long ddlak_adjoint_partial_bytes(int batch, int n)
 {
+    // three partial sums per tile: the FP64 contraction's 128 x 64 tiles, nt (nt + 1) per
+    // matrix (the register-tiled form uses nt (nt + 1) / 2 of 128 x 128)
     const unsigned long long nt = (unsigned long long)(n + ddlak::CT_TILE - 1) / ddlak::CT_TILE;
-    return sizeof(double) * 3ull * (unsigned long long)batch * (nt * (nt + 1) / 2);
+    return sizeof(double) * 3ull * (unsigned long long)batch * (nt * (nt + 1));
 }
 
 extern "C" int ddlak_batched_dot(char type, int batch, int n, const void* x, long long xstride, const void* y,
