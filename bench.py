@@ -958,7 +958,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     dom = head["kernels"].get("mixed_update", {})
     gbs = dom["bytes"] / (dom["ms"] * 1e-3) / 1e9 if dom.get("ms") else None
     hbm = peaks.get("hbm_gbs") or 6650.0
-    roof = {"bound": "hbm", "kernel": "k_mixed_update_pair / k_mixed_update (tcgen05 trailing update, FP32 W read-modify-write)",
+    roof = {"bound": "hbm", "kernel": "k_mixed_update_cta2 / k_mixed_update_pair / k_mixed_update (tcgen05 trailing update, FP32 W read-modify-write)",
             "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm if gbs else None,
             # DRAM bytes per launch: the measured bytes per 128 x 128 tile times the tiles an average launch updates
             "traffic": (traffic["k_mixed_update"]["bytes_per_tile"] * (dom["bytes"] / dom["launches"]) /

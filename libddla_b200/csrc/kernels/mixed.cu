@@ -455,6 +455,146 @@ __global__ void __launch_bounds__(128, 2) k_mixed_update_pair(const __grid_const
 }
 
 // ---------------------------------------------------------------------------
+// The same update over the whole region from t0 by 256 x 256 blocks (I2, J2),
+// J2 <= I2, on CTA pairs: a cluster of two CTAs runs one 256 x 256 MMA
+// (tcgen05 cta_group::2).  CTA v of the pair loads rows
+// 128 v .. 128 v + 127 of the block's A rows and of its B rows, holds the
+// 128 x 256 accumulator of its A rows in its own TMEM and writes their C tiles.
+// Each C tile costs half the operand bytes of the single-tile kernel, and with
+// 256 TMEM columns and 96 KB of stages per CTA two CTAs share an SM, so one
+// CTA's C-tile epilogue runs under the other's MMAs.  Both CTAs always run the
+// whole protocol (no early exit on a failed pivot): the leader counts the
+// peer's operand bytes on its own barriers and the MMA completions arrive on
+// both CTAs' barriers, so neither may leave while the other can still signal it.
+// ---------------------------------------------------------------------------
+constexpr long long MC_MIN_TILES = 32;  // smaller regions keep the pair kernel (more CTAs)
+
+// block b of the lower triangle of 256-blocks, row by row: rows 0..I2-1 hold I2 (I2 + 1) / 2
+__host__ __device__ __forceinline__ void block256_of(long long b, int& I2, int& J2)
+{
+    long long i = (long long)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
+    while (i > 0 && i * (i + 1) / 2 > b) --i;
+    while ((i + 1) * (i + 2) / 2 <= b) ++i;
+    I2 = (int)i;
+    J2 = (int)(b - i * (i + 1) / 2);
+}
+
+constexpr int MC_STAGES = 3;
+constexpr int MC_STAGE_BYTES = 2 * MU_TILE_BYTES;  // this CTA's 128 A rows + 128 B rows of 128 bytes
+constexpr size_t MC_SMEM = (size_t)MC_STAGES * MC_STAGE_BYTES + 1024;
+static_assert(MC_STAGES * MC_STAGE_BYTES >= 128 * 128 * 4, "the stages hold one FP32 C tile");
+
+template <bool TF32>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(128, 2)
+    k_mixed_update_cta2(const __grid_constant__ CUtensorMap pmap, const __grid_constant__ CUtensorMap wmap,
+                        long long t0, long long pr0, int t, int nkb, int* __restrict__ status)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[MC_STAGES], empty[MC_STAGES], done, cbar;
+    __shared__ uint32_t s_tmem;
+    const uint32_t v = tc::cluster_ctarank();  // 0: the leader, which issues the MMAs
+    int I2, J2;
+    block256_of((long long)(blockIdx.x >> 1), I2, J2);
+    const long long rowt = 2LL * I2 + v;  // this CTA's tile row
+    const long long ri = t0 + rowt * 128, rj = t0 + (long long)J2 * 256;
+    // its C tiles (rowt, 2 J2) and (rowt, 2 J2 + 1) where they lie on or below the diagonal
+    const int halves = rowt >= t ? 0 : (2LL * J2 + 1 <= rowt ? 2 : 1);
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < MC_STAGES; ++s) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        tc::mbar_init(&done, 1);
+        tc::mbar_init(&cbar, 1);
+        tc::mbar_fence_init();
+    }
+    if (warp == 0) tc::tmem_alloc_pair(&s_tmem, 256);
+    tc::tc_fence_before();
+    tc::cluster_sync();  // both CTAs' barriers initialised and their TMEM allocated
+    tc::tc_fence_after();
+    const uint32_t tmem = s_tmem;
+
+    if (threadIdx.x == 0) {
+        tc::prefetch_tmap(&pmap);
+        const uint64_t keep = tc::l2_policy_evict_last();
+        bool ok = true;
+        int issued = 0;
+        for (int kb = 0; kb < nkb; ++kb) {
+            const int s = kb % MC_STAGES;
+            if (kb >= MC_STAGES && !(ok = tc::mbar_wait(&empty[s], ((kb / MC_STAGES) - 1) & 1, status, MU_ERR_EMPTY)))
+                break;
+            unsigned char* sa = base + (size_t)s * MC_STAGE_BYTES;
+            const uint32_t fb = tc::mapa_shared(tc::smem_u32(&full[s]), 0);
+            if (v == 0) tc::mbar_expect_tx(&full[s], 2 * MC_STAGE_BYTES);  // both CTAs' bytes
+            const int x = kb * (TF32 ? 32 : 64);
+            tc::tma_load_2d_pair(sa, &pmap, fb, x, (int)(ri - pr0), keep);
+            tc::tma_load_2d_pair(sa + MU_TILE_BYTES, &pmap, fb, x, (int)(rj + 128 * v - pr0), keep);
+            issued = kb + 1;
+        }
+        // every release of this CTA's stages has arrived before it may leave
+        for (int kb = issued > MC_STAGES ? issued - MC_STAGES : 0; ok && kb < issued; ++kb)
+            ok = tc::mbar_wait(&empty[kb % MC_STAGES], (kb / MC_STAGES) & 1, status, MU_ERR_EMPTY);
+    } else if (threadIdx.x == 32 && v == 0) {
+        constexpr uint32_t idesc = tc::idesc_m256_n256<TF32>();
+        bool ok = true;
+        for (int kb = 0; kb < nkb && ok; ++kb) {
+            const int s = kb % MC_STAGES;
+            ok = tc::mbar_wait(&full[s], (kb / MC_STAGES) & 1, status, MU_ERR_FULL);
+            if (!ok) break;
+            tc::tc_fence_after();
+            const unsigned char* sa = base + (size_t)s * MC_STAGE_BYTES;
+            const uint64_t ad = tc::smem_desc_sw128(sa), bd = tc::smem_desc_sw128(sa + MU_TILE_BYTES);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)  // four K steps of 32 bytes per 128-byte row
+                tc::umma_pair<TF32>(tmem, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0 ? 1u : 0u);
+            tc::umma_commit_pair(&empty[s]);
+        }
+        tc::umma_commit_pair(&done);
+    }
+    __syncwarp();
+
+    // epilogue: this CTA's C tiles in turn through its freed stages (64 KB each)
+    bool ok = tc::mbar_wait(&done, 0, status, MU_ERR_DONE);
+    ok = __all_sync(0xffffffffu, ok);
+    tc::tc_fence_after();
+    float* ct = reinterpret_cast<float*>(base);  // [128 cols][128 rows]
+    const uint64_t stream_once = tc::l2_policy_evict_first();
+    for (int h = 0; h < halves; ++h) {
+        if (!__syncthreads_and(ok)) break;
+        if (threadIdx.x == 0) {
+            if (h > 0) tc::tma_store_wait_read();  // the first tile's store has left the buffer
+            tc::mbar_expect_tx(&cbar, 128 * 128 * 4);
+            tc::tma_load_2d_hint(ct, &wmap, &cbar, (int)ri, (int)(rj + 128 * h), stream_once);
+        }
+        ok = tc::mbar_wait(&cbar, (uint32_t)h, status, MU_ERR_CTILE);
+        ok = __all_sync(0xffffffffu, ok);
+        if (ok) {
+            const int r = 32 * warp + lane;
+#pragma unroll 1
+            for (int c = 0; c < 4; ++c) {
+                float vv[32];
+                tc::tmem_ld_32x32b_x32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(128 * h + 32 * c), vv);
+#pragma unroll
+                for (int e = 0; e < 32; ++e) ct[(32 * c + e) * 128 + r] -= vv[e];
+            }
+            tc::fence_proxy_async_smem();
+        }
+        if (__syncthreads_and(ok) && threadIdx.x == 0)
+            tc::tma_store_2d_hint(&wmap, ct, (int)ri, (int)(rj + 128 * h), stream_once);
+    }
+    if (threadIdx.x == 0) tc::tma_store_wait_read();
+    tc::tc_fence_before();
+    tc::cluster_sync();  // neither CTA frees TMEM or leaves while the pair is still working
+    if (warp == 0) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc_pair(tmem, 256);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // R = B - A X for symmetric A stored in its lower triangle (FP64), NC (8 or 16)
 // right-hand sides per chunk (grid.y).  Every lower tile A(I, J), I >= J, is
 // read from HBM once and used twice: A(I,J) X(J) goes to R(I) and A(I,J)^T X(I)
@@ -1011,6 +1151,15 @@ cudaError_t mixed_update(float* W, long long ldw, int n, long long t0, long long
     const double md = (double)m, cw = cols ? (double)cols : md;
     const double fl = cols ? 2.0 * nbk * (md * cw - cw * (cw - 1) / 2) : md * (md + 1) * nbk;
     ProfScope ps(PK_MIXED_UPDATE, st, fl, 4.0 * (cols ? 2.0 * md * cw : md * (md + 1)));
+    if (cols == 0 && t >= MC_MIN_TILES) {
+        // the whole trailing region by 256 x 256 blocks, one per CTA pair
+        if (cudaError_t e = smem_optin(k_mixed_update_cta2<TF32>, MC_SMEM); e != cudaSuccess) return e;
+        const long long t2 = (t + 1) / 2;
+        k_mixed_update_cta2<TF32><<<(unsigned)(t2 * (t2 + 1)), 128, MC_SMEM, st>>>(map, wmap, t0, pr0, (int)t, nkb,
+                                                                                    status);
+        note_launches(1);
+        return cudaGetLastError();
+    }
     if (cols == 0 && t >= 4) {
         // the whole trailing region by pairs of tiles sharing their A rows
         if (cudaError_t e = smem_optin(k_mixed_update_pair<TF32>, MP_SMEM); e != cudaSuccess) return e;

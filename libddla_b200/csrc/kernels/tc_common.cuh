@@ -1,6 +1,8 @@
 // sm_100a primitives used by the tensor-core kernels: mbarriers with bounded
-// waits, TMA tile loads (no cluster multicast anywhere), tcgen05 MMA / TMEM
-// management, and the shared-memory / instruction descriptors of UMMA.
+// waits, TMA tile loads (no load with cluster multicast anywhere), tcgen05 MMA /
+// TMEM management for one CTA and for a CTA pair (cta_group::2, whose MMA
+// completion arrives on both CTAs' mbarriers), and the shared-memory /
+// instruction descriptors of UMMA.
 //
 // Descriptor layouts follow the PTX ISA "tcgen05 matrix descriptors" and
 // "instruction descriptor" tables for kind::f16 / kind::tf32:
@@ -10,7 +12,7 @@
 //   instruction descriptor: D format [4,6) (1 = F32), A format [7,10) and
 //     B format [10,13) (1 = BF16 for kind::f16, 2 = TF32 for kind::tf32),
 //     negate A/B [13]/[14], A/B major [15]/[16] (0 = K-major), N >> 3 [17,23),
-//     M >> 4 [24,29).
+//     M >> 4 [24,29) (M = 256 for a CTA pair).
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -268,6 +270,85 @@ template <bool TF32>
 __host__ __device__ constexpr uint32_t idesc_m128_n256()
 {
     return (1u << 4) | ((TF32 ? 2u : 1u) << 7) | ((TF32 ? 2u : 1u) << 10) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+}
+// M = 256 across a CTA pair (cta_group::2), N = 256
+template <bool TF32>
+__host__ __device__ constexpr uint32_t idesc_m256_n256()
+{
+    return (1u << 4) | ((TF32 ? 2u : 1u) << 7) | ((TF32 ? 2u : 1u) << 10) | ((256u >> 3) << 17) | ((256u >> 4) << 24);
+}
+
+// ---- CTA pairs (a cluster of two CTAs sharing one tcgen05 MMA) -------------------
+__device__ __forceinline__ uint32_t cluster_ctarank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+// every thread of every CTA of the cluster
+__device__ __forceinline__ void cluster_sync()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// shared::cluster address of the variable at shared::cta address `a` in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t mapa_shared(uint32_t a, uint32_t rank)
+{
+    uint32_t d;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(rank));
+    return d;
+}
+// TMA load into this CTA's shared memory whose completion is counted on the
+// mbarrier at shared::cluster address `bar` (the pair leader's); no multicast
+__device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, uint32_t bar, int x, int y,
+                                                 uint64_t policy)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], "
+        "[%1, {%3, %4}], [%2], %5;" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y), "l"(policy)
+        : "memory");
+}
+// TMEM allocation of a CTA pair: the same warp of both CTAs
+__device__ __forceinline__ void tmem_alloc_pair(uint32_t* dst_smem, uint32_t ncols)
+{
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc_pair(uint32_t taddr, uint32_t ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+// D[tmem of both CTAs] (+)= A * B^T, 256 x N: A rows 0..127 and B rows 0..N/2-1 from
+// the leader's shared memory, the other halves from the same offsets in the peer's
+template <bool TF32>
+__device__ __forceinline__ void umma_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t acc)
+{
+    if (TF32) {
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+            : "memory");
+    } else {
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+            : "memory");
+    }
+}
+// Arrive on the mbarrier at the same offset in both CTAs of the pair once every
+// pair MMA issued so far by this thread has completed (an arrival, not a load).
+__device__ __forceinline__ void umma_commit_pair(uint64_t* bar)
+{
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            smem_u32(bar)),
+        "h"((uint16_t)0x3)
+        : "memory");
 }
 
 }  // namespace tc

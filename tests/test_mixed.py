@@ -72,10 +72,11 @@ def test_symm_residual_matches_numpy(handle, n, nrhs, pad):
 
 
 @pytest.mark.parametrize("precision,tol", [("B", 3e-2), ("T", 4e-3)])
-@pytest.mark.parametrize("n", [128, 300, 1111, 2048, 5000])
+@pytest.mark.parametrize("n", [128, 300, 1111, 2048, 4700, 5000])
 def test_tensor_core_factorization(handle, precision, tol, n):
     """ddlak_potrf_mixed: backward error of the FP32 factor at the level of the operand rounding
-    (n=5000: its first trailing updates take the multi-tile kernel, 4 tiles per CTA)."""
+    (n=4700 and 5000: their first trailing updates run on CTA pairs, 256 x 256 blocks; at 4700
+    the first one covers 33 tile rows, so the last pair's second CTA holds rows past the end)."""
     rng = np.random.default_rng(7 + n)
     A = _spd(rng, n)
     ldw = (n + 3) // 4 * 4
@@ -101,6 +102,35 @@ def test_tensor_core_factorization(handle, precision, tol, n):
         assert err < tol, err
         Lref = np.linalg.cholesky(A)
         assert np.max(np.abs(L - Lref)) / np.max(np.abs(Lref)) < 10 * tol
+    finally:
+        for p in (dW, P0, P1, dI):
+            handle.free(p)
+
+
+@pytest.mark.parametrize("precision", ["B", "T"])
+def test_tensor_core_factorization_failed_pivot_on_cta_pairs(handle, precision):
+    """A failed pivot in the first block column at n=4700: the trailing updates that follow
+    run on CTA pairs, which take no early exit, over the failed factor; the order of the
+    failed minor comes back and no pipeline wait gives up."""
+    n = 4700
+    ldw = (n + 3) // 4 * 4
+    W = np.zeros((ldw, n), dtype=np.float32, order="F")
+    W[np.arange(n), np.arange(n)] = 2.0
+    W[100, 100] = -1.0
+    vp, i, ll, c = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_char
+    pb = _k("ddlak_mixed_panel_bytes", i)
+    pb.restype = ctypes.c_ulonglong
+    f = _k("ddlak_potrf_mixed", c, i, vp, ll, vp, vp, vp, vp, vp)
+    dW = _dev(handle, W)
+    P0, P1 = handle.malloc(pb(n)), handle.malloc(pb(n))
+    dI = handle.malloc(256)
+    try:
+        assert f(precision.encode(), n, dW, ldw, P0, P1, dI, dI + 4, _stream(handle)) == 0
+        out = np.zeros(2, dtype=np.int32)
+        handle.memcpy(out.ctypes.data, dI, 8)
+        handle.synchronize()
+        assert out[1] == 0, "tensor-core pipeline wait gave up"
+        assert out[0] == 101
     finally:
         for p in (dW, P0, P1, dI):
             handle.free(p)
