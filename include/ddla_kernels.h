@@ -174,6 +174,15 @@ int ddlak_diag_logsum_grid(char type, int n, const void* A, long long lld, int l
  * (enough for any group up to DDLAK_MIXED_MAX_GROUP). */
 unsigned long long ddlak_mixed_panel_bytes(int n);
 
+/* Host-side view of the factorization's update of a whole trailing region of t
+ * tile rows (tiles of 128) (no device work): *kind = 2 when it runs by 256 x 256
+ * blocks on CTA pairs, 1 by pairs of tiles of one tile row, 0 by single tiles,
+ * and *ctas the size of its grid.  For kinds 1 and 2, CTA c decoded to the C tiles
+ * it writes: tile row *row, tile columns *col0 .. *col0 + *ntiles - 1.  For tests
+ * of the launch's coverage of the lower triangle. */
+int ddlak_mixed_update_grid(int t, int* kind, long long* ctas);
+int ddlak_mixed_update_cta_tiles(int t, long long c, long long* row, long long* col0, int* ntiles);
+
 /* W = fl32(A) on the lower triangle (diagonal times diag_scale, a relative
  * shift), colsum[j] = sum_i |A(i,j)| of the full symmetric A, *anrm = max_j
  * colsum[j] (= ||A||_inf), all on the stream.  ldw must be a multiple of 4. */

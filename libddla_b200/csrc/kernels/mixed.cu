@@ -342,7 +342,7 @@ __host__ __device__ __forceinline__ long long pair_start(long long I)
 {
     return (I & 1) ? ((I + 1) / 2) * ((I + 1) / 2) : (I / 2) * (I / 2 + 1);
 }
-__device__ __forceinline__ void pair_of(long long b, int& I, int& P)
+__host__ __device__ __forceinline__ void pair_of(long long b, int& I, int& P)
 {
     long long i = (long long)(2.0 * sqrt((double)b)) - 1;
     if (i < 0) i = 0;
@@ -350,6 +350,20 @@ __device__ __forceinline__ void pair_of(long long b, int& I, int& P)
     while (i > 0 && pair_start(i) > b) --i;
     I = (int)i;
     P = (int)(b - pair_start(i));
+}
+
+// The C tiles one CTA of a whole-region update writes: tile row `row`, tile
+// columns col0 .. col0 + ntiles - 1 (128-wide tiles from the region's start).
+struct UpdateTiles {
+    long long row, col0;
+    int ntiles;
+};
+// pair CTA b: tiles (I, 2P) and, when it lies on or below the diagonal, (I, 2P + 1)
+__host__ __device__ __forceinline__ UpdateTiles pair_tiles(long long b)
+{
+    int I, P;
+    pair_of(b, I, P);
+    return {I, 2LL * P, (2 * P + 1 <= I) ? 2 : 1};
 }
 
 template <bool TF32>
@@ -362,10 +376,9 @@ __global__ void __launch_bounds__(128, 2) k_mixed_update_pair(const __grid_const
     __shared__ __align__(8) uint64_t full[MP_STAGES], empty[MP_STAGES], done, cbar;
     __shared__ uint32_t s_tmem;
     if (*(volatile const int*)info != 0) return;
-    int I, P;
-    pair_of(blockIdx.x, I, P);
-    const long long ri = t0 + (long long)I * 128, rj = t0 + (long long)P * 256;
-    const int halves = (2 * P + 1 <= I) ? 2 : 1;  // the second tile of the pair lies on or below the diagonal
+    const UpdateTiles tl = pair_tiles(blockIdx.x);
+    const long long ri = t0 + tl.row * 128, rj = t0 + tl.col0 * 128;
+    const int halves = tl.ntiles;
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -478,6 +491,25 @@ __host__ __device__ __forceinline__ void block256_of(long long b, int& I2, int& 
     I2 = (int)i;
     J2 = (int)(b - i * (i + 1) / 2);
 }
+// CTA c of the CTA-pair update over t tile rows: block c / 2, rows 128 (c mod 2)
+// .. of it (c mod 2 is the CTA's rank in its cluster); its tiles (row, 2 J2) and
+// (row, 2 J2 + 1) where they lie on or below the diagonal, none past the last row
+// the form of a whole-region update over t tile rows: 2 CTA pairs, 1 tile pairs,
+// 0 single tiles; *ctas its grid
+inline int region_update_kind(long long t, long long* ctas)
+{
+    const long long t2 = (t + 1) / 2;
+    const int kind = t >= MC_MIN_TILES ? 2 : (t >= 4 ? 1 : 0);
+    *ctas = kind == 2 ? t2 * (t2 + 1) : (kind == 1 ? pair_start(t) : t * (t + 1) / 2);
+    return kind;
+}
+__host__ __device__ __forceinline__ UpdateTiles cta2_tiles(long long c, long long t)
+{
+    int I2, J2;
+    block256_of(c >> 1, I2, J2);
+    const long long row = 2LL * I2 + (c & 1);
+    return {row, 2LL * J2, row >= t ? 0 : (2LL * J2 + 1 <= row ? 2 : 1)};
+}
 
 constexpr int MC_STAGES = 3;
 constexpr int MC_STAGE_BYTES = 2 * MU_TILE_BYTES;  // this CTA's 128 A rows + 128 B rows of 128 bytes
@@ -493,12 +525,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(128, 2)
     __shared__ __align__(8) uint64_t full[MC_STAGES], empty[MC_STAGES], done, cbar;
     __shared__ uint32_t s_tmem;
     const uint32_t v = tc::cluster_ctarank();  // 0: the leader, which issues the MMAs
-    int I2, J2;
-    block256_of((long long)(blockIdx.x >> 1), I2, J2);
-    const long long rowt = 2LL * I2 + v;  // this CTA's tile row
-    const long long ri = t0 + rowt * 128, rj = t0 + (long long)J2 * 256;
-    // its C tiles (rowt, 2 J2) and (rowt, 2 J2 + 1) where they lie on or below the diagonal
-    const int halves = rowt >= t ? 0 : (2LL * J2 + 1 <= rowt ? 2 : 1);
+    const UpdateTiles tl = cta2_tiles(blockIdx.x, t);  // blockIdx.x mod 2 == v (clusters of 2 along x)
+    const long long ri = t0 + tl.row * 128, rj = t0 + tl.col0 * 128;
+    const int halves = tl.ntiles;
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -1146,25 +1175,23 @@ cudaError_t mixed_update(float* W, long long ldw, int n, long long t0, long long
     CUtensorMap wmap;
     if (!encode_w_map(&wmap, W, n, ldw)) return cudaErrorInvalidValue;
     const long long t = ceil_div(m, 128);
-    const long long grid = cols == 0 ? t * (t + 1) / 2 : t * ceil_div(cols, 128);
+    long long grid = t * ceil_div(cols, 128);
+    const int kind = cols == 0 ? region_update_kind(t, &grid) : 0;
     const int nkb = nbk / (TF32 ? 32 : 64);
     const double md = (double)m, cw = cols ? (double)cols : md;
     const double fl = cols ? 2.0 * nbk * (md * cw - cw * (cw - 1) / 2) : md * (md + 1) * nbk;
     ProfScope ps(PK_MIXED_UPDATE, st, fl, 4.0 * (cols ? 2.0 * md * cw : md * (md + 1)));
-    if (cols == 0 && t >= MC_MIN_TILES) {
+    if (kind == 2) {
         // the whole trailing region by 256 x 256 blocks, one per CTA pair
         if (cudaError_t e = smem_optin(k_mixed_update_cta2<TF32>, MC_SMEM); e != cudaSuccess) return e;
-        const long long t2 = (t + 1) / 2;
-        k_mixed_update_cta2<TF32><<<(unsigned)(t2 * (t2 + 1)), 128, MC_SMEM, st>>>(map, wmap, t0, pr0, (int)t, nkb,
-                                                                                    status);
+        k_mixed_update_cta2<TF32><<<(unsigned)grid, 128, MC_SMEM, st>>>(map, wmap, t0, pr0, (int)t, nkb, status);
         note_launches(1);
         return cudaGetLastError();
     }
-    if (cols == 0 && t >= 4) {
+    if (kind == 1) {
         // the whole trailing region by pairs of tiles sharing their A rows
         if (cudaError_t e = smem_optin(k_mixed_update_pair<TF32>, MP_SMEM); e != cudaSuccess) return e;
-        k_mixed_update_pair<TF32><<<(unsigned)pair_start(t), 128, MP_SMEM, st>>>(map, wmap, n, t0, pr0, nkb, dinfo,
-                                                                                 status);
+        k_mixed_update_pair<TF32><<<(unsigned)grid, 128, MP_SMEM, st>>>(map, wmap, n, t0, pr0, nkb, dinfo, status);
         note_launches(1);
         return cudaGetLastError();
     }
@@ -1418,6 +1445,28 @@ extern "C" unsigned long long ddlak_mixed_panel_bytes(int n)
     const unsigned long long rows = (unsigned long long)(n > 0 ? n : 0);
     const unsigned long long G = DDLAK_MIXED_MAX_GROUP;
     return (rows * G * ddlak::MX_NB * 4 + 255) / 256 * 256 + (rows * (G - 1) * ddlak::MX_NB * 4 + 255) / 256 * 256;
+}
+
+extern "C" int ddlak_mixed_update_grid(int t, int* kind, long long* ctas)
+{
+    using namespace ddlak;
+    if (t < 1 || !kind || !ctas) return (int)cudaErrorInvalidValue;
+    *kind = region_update_kind(t, ctas);
+    return 0;
+}
+
+extern "C" int ddlak_mixed_update_cta_tiles(int t, long long c, long long* row, long long* col0, int* ntiles)
+{
+    using namespace ddlak;
+    int kind = 0;
+    long long ctas = 0;
+    if (ddlak_mixed_update_grid(t, &kind, &ctas) != 0 || kind == 0 || c < 0 || c >= ctas || !row || !col0 || !ntiles)
+        return (int)cudaErrorInvalidValue;
+    const UpdateTiles tl = kind == 2 ? cta2_tiles(c, t) : pair_tiles(c);
+    *row = tl.row;
+    *col0 = tl.col0;
+    *ntiles = tl.ntiles;
+    return 0;
 }
 
 extern "C" int ddlak_convert_lower(int n, const void* A, long long lda, void* W, long long ldw, double diag_scale,
