@@ -91,16 +91,62 @@ def traffic_summary() -> dict:
 # clocks sampling during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
+    """SM clock and clock-event reasons of one GPU, sampled while the timed region runs.
+
+    NVML is read in-process every 20 ms from a thread (reads only; no setting of the
+    GPU is touched), so a timed region of a few hundred milliseconds still gets a
+    dozen samples.  Where NVML cannot be opened, ``nvidia-smi -lms 200`` is read
+    instead.  The torch device is matched to its NVML handle by UUID, so the index
+    is right under CUDA_VISIBLE_DEVICES too.
+    """
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASON_BITS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+                   ("sw_power_cap", 0x4))
+    PERIOD_S = 0.02
 
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
         self.lines = []
+        self.samples = []  # (sm MHz, reason bitmask) from NVML
+        self.max_mhz = None
+        self._nvml = None
+        self._stop = threading.Event()
+        self._t = None
+
+    def _nvml_handle(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        self._nvml = pynvml
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            return pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.dev)
+
+    def _poll_nvml(self, h):
+        nv = self._nvml
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self._stop.is_set():
+            try:
+                self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), int(get_reasons(h))))
+            except Exception:
+                break
+            self._stop.wait(self.PERIOD_S)
 
     def __enter__(self):
+        try:
+            h = self._nvml_handle()
+            self.max_mhz = float(self._nvml.nvmlDeviceGetMaxClockInfo(h, self._nvml.NVML_CLOCK_SM))
+            self._t = threading.Thread(target=self._poll_nvml, args=(h,), daemon=True)
+            self._t.start()
+            return self
+        except Exception:
+            self._nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -116,6 +162,13 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        if self._nvml is not None:
+            self._stop.set()
+            self._t.join(timeout=5)
+            try:
+                self._nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -124,8 +177,13 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self) -> dict:
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, mx, reasons = [], self.max_mhz, set()
+        for mhz, bits in self.samples:
+            sm.append(mhz)
+            for name, bit in self.REASON_BITS:
+                if bits & bit:
+                    reasons.add(name)
+        names = [name for name, _ in self.REASON_BITS]
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
@@ -139,7 +197,7 @@ class ClockSampler:
                 if val.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvml" if self.samples else "nvidia-smi"}
 
 
 # ---------------------------------------------------------------------------

@@ -46,3 +46,27 @@ def test_reference_arm_other_ranks_are_silent():
     r = _run({"WORLD_SIZE": "2", "RANK": "1", "LOCAL_RANK": "1"})
     assert r.returncode == 0, r.stderr[-2000:]
     assert not [l for l in r.stdout.splitlines() if l.startswith("{")]
+
+
+def test_clock_summary_decodes_reasons_and_median():
+    """The clock record of the timed region: NVML reason bits map to the names the
+    timing rules use (hw_slowdown 0x8, hw_thermal_slowdown 0x40, sw_thermal_slowdown
+    0x20, sw_power_cap 0x4), and the SM clock reported is the median of the samples."""
+    import pynvml
+
+    import bench
+
+    assert dict(bench.ClockSampler.REASON_BITS) == {
+        "hw_slowdown": pynvml.nvmlClocksThrottleReasonHwSlowdown,
+        "hw_thermal_slowdown": pynvml.nvmlClocksThrottleReasonHwThermalSlowdown,
+        "sw_thermal_slowdown": pynvml.nvmlClocksThrottleReasonSwThermalSlowdown,
+        "sw_power_cap": pynvml.nvmlClocksThrottleReasonSwPowerCap,
+    }
+    c = bench.ClockSampler(0)
+    c.samples = [(1965.0, 0x0), (1890.0, 0x4), (1920.0, 0x4 | 0x1)]
+    c.max_mhz = 1965.0
+    s = c.summary()
+    assert s["sm_mhz"] == 1920.0 and s["sm_max_mhz"] == 1965.0 and s["samples"] == 3
+    assert s["reasons"] == ["sw_power_cap"] and s["source"] == "nvml"
+    c.samples = [(1400.0, 0x40 | 0x8)]
+    assert bench.ClockSampler.summary(c)["reasons"] == ["hw_slowdown", "hw_thermal_slowdown"]
